@@ -1,0 +1,1397 @@
+// bfx batched relaxation engines for B200 (sm_100a).
+//
+// One launch relaxes any number of batches (planned query groups of 1, 8,
+// 16 or 32 lanes, one query per lane) over the resident graph:
+//   * frontier push  -- the reference's BatchedFrontierPushEngine
+//                       (src/hip/batched_frontier_push.hip.cpp:710-906),
+//   * Jacobi pull    -- BatchedJacobiPullEngine (src/hip/batched_jacobi.hip.cpp:466-694),
+//   * dense chaotic  -- BatchedDenseChaoticPushEngine
+//                       (src/hip/batched_dense_chaotic_push.hip.cpp:392-600).
+// All three converge to the same labels: every label is the minimum over
+// admitted paths of the left-folded float sum (float + is monotone), and the
+// packed 64-bit label keeps the smallest stable edge id among tight
+// in-edges.  The schedule is ours:
+//   * labels live in compact union-tile storage per batch (vertex-major,
+//     lanes contiguous), addressed through a dense per-tile {lane mask,
+//     compact bias} table that doubles as the run admission test
+//     (mask[src tile] & mask[dst tile], src/device_layout.cpp:762), so no run
+//     masks are materialised;
+//   * edges are 16-byte records {endpoint, weight bits, eid+1, endpoint tile}
+//     read with 128-bit non-coherent loads;
+//   * a frontier vertex is processed by one warp that flattens (edge, active
+//     lane) pairs over its 32 threads; improvements use a non-returning
+//     64-bit min after a coherent pre-read, success bits are OR-combined per
+//     edge with shuffles and queue claims are warp-aggregated;
+//   * persistent mode runs all rounds of all batches in one cooperative
+//     launch with a grid barrier whose waits time out; host-poll modes run
+//     CUDA-graph-captured chunks of rounds.
+#include "bfx.h"
+#include "bfx_internal.hpp"
+#include "device_common.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace bfx {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string& message) { g_last_error = message; }
+
+#define BFX_CUDA(call)                                                                          \
+  do {                                                                                          \
+    cudaError_t err_ = (call);                                                                  \
+    if (err_ != cudaSuccess) {                                                                  \
+      throw ::bfx::Error(err_ == cudaErrorMemoryAllocation ? BFX_ERR_OUT_OF_MEMORY : BFX_ERR_CUDA, \
+                         std::string(#call) + ": " + cudaGetErrorString(err_));                \
+    }                                                                                           \
+  } while (0)
+
+using dev::u32;
+using dev::u64;
+
+// ---------------------------------------------------------------------------
+// Device structures
+// ---------------------------------------------------------------------------
+
+struct DGraph {
+  u32 V, E, T, reserved;
+  const u32* owner;    // [V]
+  const u32* csr_off;  // [V+1]
+  const uint4* csr;    // [E] {dst, weight bits, eid+1, dst tile}
+  const u32* csc_off;  // [V+1]
+  const uint4* csc;    // [E] {src, weight bits, eid+1, src tile}
+};
+
+struct DBatch {
+  u32 W, shift, valid, U;
+  u32 src_count, tgt_count, range_count, reserved;
+  u64* dist[2];        // [U*W] labels (slot 1 only for Jacobi)
+  u32* mask[2];        // [U] pending lane masks (frontier)
+  u32* queue[2];       // [U] frontier vertices (global ids)
+  u32* c2g;            // [U] compact -> global vertex
+  uint2* tiles;        // [T] {lane mask, compact bias}
+  const u32* src_off;  // [W+1]
+  const u32* src;
+  const u32* tgt_off;  // [W+1]
+  const u32* tgt;
+  const uint4* ranges;    // [R] {tile, begin, end, lane mask}
+  const u32* range_off;   // [R+1] compact offsets
+};
+
+struct DCtl {
+  u32 count[3];    // frontier sizes, rotating by round
+  u32 changed[3];  // Jacobi/dense: lanes whose distance changed, rotating
+  u32 rounds;      // rounds executed with work
+  u32 missing;     // finalize: lanes with an unreached target
+  u32 active;      // finalize: lanes still pending at the stop
+  u32 error_bits;
+};
+
+struct DRun {
+  dev::GridSync sync;
+  u32 round;       // next round (host-poll modes)
+  u32 done;        // all batches stopped
+  u32 stop;        // launch-wide stop reason
+  u32 abort;       // device failure seen
+  u64 max_rounds;
+  u64 launches;
+};
+
+constexpr u32 kMaxBatchesPerLaunch = 4096;
+constexpr u64 kBarrierTimeoutNs = 2000000000ull;  // 2 s per barrier wait
+
+struct LaunchParams {
+  DGraph g;
+  const DBatch* batches;
+  DCtl* ctl;
+  DRun* run;
+  const u32* unit_base;  // [nb+1] prefix of U (init / finalize)
+  u32 nb;
+  u32 engine;
+  u32 per_lane;
+  u32 reserved;
+  u64 max_rounds;
+};
+
+// ---------------------------------------------------------------------------
+// Small device helpers
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ u32 lane_id() { return threadIdx.x & 31u; }
+
+// Largest b with prefix[b] <= x (prefix strictly covering [0, prefix[nb])).
+__device__ __forceinline__ u32 find_batch(const u32* prefix, u32 nb, u32 x) {
+  u32 lo = 0, hi = nb;
+  while (hi - lo > 1u) {
+    const u32 mid = (lo + hi) >> 1;
+    if (prefix[mid] <= x) {
+      lo = mid;
+    } else {
+      hi = mid;
+    }
+  }
+  return lo;
+}
+
+__device__ __forceinline__ u32 lane_of_position(const u32* offsets, u32 W, u32 pos) {
+  u32 lo = 0, hi = W;
+  while (hi - lo > 1u) {
+    const u32 mid = (lo + hi) >> 1;
+    if (offsets[mid] <= pos) {
+      lo = mid;
+    } else {
+      hi = mid;
+    }
+  }
+  return lo;
+}
+
+// Block-wide exclusive scan of per-batch values into smem prefix[0..nb].
+template <typename F>
+__device__ void block_prefix(u32* prefix, u32 nb, F value) {
+  __shared__ u32 s_warp[33];
+  const u32 per = (nb + blockDim.x - 1) / blockDim.x;
+  const u32 begin = threadIdx.x * per;
+  u32 local = 0;
+  for (u32 i = 0; i < per; ++i) {
+    const u32 b = begin + i;
+    if (b < nb) local += value(b);
+  }
+  // inclusive warp scan
+  u32 x = local;
+  for (u32 o = 1; o < 32; o <<= 1) {
+    const u32 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane_id() >= o) x += y;
+  }
+  const u32 warp = threadIdx.x >> 5;
+  if (lane_id() == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    u32 acc = 0;
+    const u32 nw = blockDim.x >> 5;
+    for (u32 w = 0; w < nw; ++w) {
+      const u32 t = s_warp[w];
+      s_warp[w] = acc;
+      acc += t;
+    }
+    s_warp[32] = acc;
+  }
+  __syncthreads();
+  u32 run = s_warp[warp] + x - local;
+  for (u32 i = 0; i < per; ++i) {
+    const u32 b = begin + i;
+    if (b < nb) {
+      prefix[b] = run;
+      run += value(b);
+    }
+  }
+  if (threadIdx.x == 0) prefix[nb] = s_warp[32];
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Initialisation and seeding
+// ---------------------------------------------------------------------------
+
+// Grid-stride over all union vertices of all batches: compact->global map,
+// +inf labels, clear masks; over tile tables: {mask, bias} for union tiles.
+__global__ void init_kernel(LaunchParams p) {
+  const u64 tid = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+  const u32 total_units = p.unit_base[p.nb];
+  for (u64 u = tid; u < total_units; u += stride) {
+    const u32 b = find_batch(p.unit_base, p.nb, static_cast<u32>(u));
+    const DBatch& B = p.batches[b];
+    const u32 cv = static_cast<u32>(u) - p.unit_base[b];
+    // range containing cv
+    u32 lo = 0, hi = B.range_count;
+    while (hi - lo > 1u) {
+      const u32 mid = (lo + hi) >> 1;
+      if (B.range_off[mid] <= cv) lo = mid; else hi = mid;
+    }
+    const uint4 r = B.ranges[lo];
+    B.c2g[cv] = r.y + (cv - B.range_off[lo]);
+    B.mask[0][cv] = 0u;
+    B.mask[1][cv] = 0u;
+    for (u32 l = 0; l < B.W; ++l) {
+      B.dist[0][(static_cast<u64>(cv) << B.shift) + l] = dev::kUnreached;
+      if (p.engine == BFX_ENGINE_JACOBI_PULL) B.dist[1][(static_cast<u64>(cv) << B.shift) + l] = dev::kUnreached;
+    }
+  }
+  // Tile tables: clear every tile then write union tiles (a second pass in
+  // the same kernel would race; clearing is done by the host-side memset).
+  for (u32 b = 0; b < p.nb; ++b) {
+    const DBatch& B = p.batches[b];
+    for (u64 i = tid; i < B.range_count; i += stride) {
+      const uint4 r = B.ranges[i];
+      B.tiles[r.x] = make_uint2(r.w, r.y - B.range_off[i]);
+    }
+  }
+  if (tid < p.nb) {
+    DCtl& c = p.ctl[tid];
+    c.count[0] = c.count[1] = c.count[2] = 0u;
+    c.changed[0] = p.batches[tid].valid;
+    c.changed[1] = c.changed[2] = 0u;
+    c.rounds = 0u;
+    c.missing = 0u;
+    c.active = 0u;
+    c.error_bits = 0u;
+  }
+  if (tid == 0) {
+    p.run->sync.arrive = 0u;
+    p.run->sync.generation = 0u;
+    p.run->sync.abort = 0u;
+    p.run->round = 0u;
+    p.run->done = 0u;
+    p.run->stop = 0u;
+    p.run->abort = 0u;
+  }
+}
+
+// Sources: label (0, 0) in every lane that owns them; frontier engines also
+// mark the lane bit and enqueue the vertex once (src/hip/batched_frontier_push.hip.cpp:495-559).
+__global__ void seed_kernel(LaunchParams p, const u32* src_base) {
+  const u64 tid = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+  const u32 total = src_base[p.nb];
+  for (u64 i = tid; i < total; i += stride) {
+    const u32 b = find_batch(src_base, p.nb, static_cast<u32>(i));
+    const DBatch& B = p.batches[b];
+    const u32 pos = static_cast<u32>(i) - src_base[b];
+    const u32 lane = lane_of_position(B.src_off, B.W, pos);
+    const u32 v = B.src[pos];
+    const uint2 t = B.tiles[p.g.owner[v]];
+    if (((t.x >> lane) & 1u) == 0u) {
+      atomicOr(&p.ctl[b].error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
+      continue;
+    }
+    const u32 cv = v - t.y;
+    B.dist[0][(static_cast<u64>(cv) << B.shift) + lane] = dev::kSourceWord;
+    if (p.engine == BFX_ENGINE_JACOBI_PULL) B.dist[1][(static_cast<u64>(cv) << B.shift) + lane] = dev::kSourceWord;
+    if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
+      const u32 old = atomicOr(&B.mask[0][cv], 1u << lane);
+      if (old == 0u) {
+        const u32 slot = atomicAdd(&p.ctl[b].count[0], 1u);
+        if (slot < B.U) {
+          B.queue[0][slot] = v;
+        } else {
+          atomicOr(&p.ctl[b].error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Frontier push: one warp per (batch, vertex) queue entry.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void frontier_entry(const LaunchParams& p, const DBatch& B, DCtl& C, u32 v, u32 rd,
+                                               u32 widx) {
+  const u32 lane = lane_id();
+  const u32 st = __ldg(p.g.owner + v);
+  const uint2 sti = B.tiles[st];
+  const u32 cv = v - sti.y;
+  u32 m = 0;
+  if (lane == 0) m = atomicExch(&B.mask[rd][cv], 0u);
+  m = __shfl_sync(0xFFFFFFFFu, m, 0) & sti.x;
+  if (m == 0u) return;
+  const u32 k = __popc(m);
+  const u32 s = k <= 1u ? 0u : 32u - __clz(k - 1u);  // group = 2^s lanes per edge
+  const u32 kp = 1u << s;
+  const u32 slot = lane >> s;
+  const u32 j = lane & (kp - 1u);
+  const u32 G = 32u >> s;  // edges per warp iteration
+  const bool has_lane = j < k;
+  u32 ql = 0, src_bits = dev::kInfBits;
+  if (has_lane) {
+    u32 mm = m;
+    for (u32 t = 0; t < j; ++t) mm &= mm - 1u;  // drop the j lowest active lanes
+    ql = __ffs(mm) - 1u;
+    src_bits = dev::hi(dev::ld_cg(B.dist[0] + ((static_cast<u64>(cv) << B.shift) + ql)));
+  }
+  u32* const mask_w = B.mask[rd ^ 1u];
+  u32* const queue_w = B.queue[rd ^ 1u];
+  const u32 rb = __ldg(p.g.csr_off + v), re = __ldg(p.g.csr_off + v + 1);
+  for (u32 base = rb; base < re; base += G) {
+    const u32 e = base + slot;
+    u32 bits = 0u, cdst = 0u, dstv = 0u;
+    if (e < re && has_lane) {
+      const uint4 rec = __ldg(p.g.csr + e);
+      const uint2 dt = B.tiles[rec.w];
+      cdst = rec.x - dt.y;
+      dstv = rec.x;
+      if (((dt.x >> ql) & 1u) && src_bits != dev::kInfBits) {
+        const u64 cand = dev::candidate(src_bits, rec.y, rec.z);
+        u64* const target = B.dist[0] + ((static_cast<u64>(cdst) << B.shift) + ql);
+        const u64 cur = dev::ld_cg(target);
+        if (cand < cur) {
+          dev::red_min(target, cand);
+          if (dev::hi(cand) < dev::hi(cur)) bits = 1u << ql;
+        }
+      }
+    }
+    for (u32 o = 1; o < kp; o <<= 1) bits |= __shfl_xor_sync(0xFFFFFFFFu, bits, o);
+    bool claim = false;
+    if (j == 0u && bits != 0u) {
+      const u32 old = atomicOr(mask_w + cdst, bits);
+      claim = old == 0u;
+    }
+    const u32 cm = __ballot_sync(0xFFFFFFFFu, claim);
+    if (cm != 0u) {
+      const u32 leader = __ffs(cm) - 1u;
+      u32 pos = 0;
+      if (lane == leader) pos = atomicAdd(&C.count[widx], static_cast<u32>(__popc(cm)));
+      pos = __shfl_sync(0xFFFFFFFFu, pos, static_cast<int>(leader));
+      if (claim) {
+        const u32 at = pos + __popc(cm & ((1u << lane) - 1u));
+        if (at < B.U) {
+          queue_w[at] = dstv;
+        } else {
+          atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Jacobi pull: lane = query lane, 32/W destination vertices per warp.
+// d_next[v,l] = min(d[v,l], min over admitted in-edges of d[u,l] + w).
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void jacobi_item(const LaunchParams& p, const DBatch& B, DCtl& C, u32 item, u32 r,
+                                            u32 widx) {
+  const u32 lane = lane_id();
+  const u32 sub = lane >> B.shift;
+  const u32 ql = lane & (B.W - 1u);
+  const u32 vpw = 32u >> B.shift;
+  const u32 cv = item * vpw + sub;
+  const u64* const dr = B.dist[r & 1u];
+  u64* const dw = B.dist[(r & 1u) ^ 1u];
+  u32 changed = 0u;
+  if (cv < B.U) {
+    const u32 v = B.c2g[cv];
+    const uint2 vt = B.tiles[__ldg(p.g.owner + v)];
+    const u64 idx = (static_cast<u64>(cv) << B.shift) + ql;
+    const u64 old = dev::ld_cg(dr + idx);
+    u64 best = old;
+    if ((vt.x >> ql) & 1u) {
+      const u32 cb = __ldg(p.g.csc_off + v), ce = __ldg(p.g.csc_off + v + 1);
+      for (u32 e = cb; e < ce; ++e) {
+        const uint4 rec = __ldg(p.g.csc + e);
+        const uint2 su = B.tiles[rec.w];
+        if ((su.x >> ql) & 1u) {
+          const u32 sb = dev::hi(dev::ld_cg(dr + ((static_cast<u64>(rec.x - su.y) << B.shift) + ql)));
+          if (sb != dev::kInfBits) {
+            const u64 cand = dev::candidate(sb, rec.y, rec.z);
+            best = cand < best ? cand : best;
+          }
+        }
+      }
+      if (dev::hi(best) != dev::hi(old)) changed = 1u << ql;
+    }
+    dw[idx] = best;
+  }
+  const u32 any = __reduce_or_sync(0xFFFFFFFFu, changed);
+  if (lane == 0 && any != 0u && (dev::ld_cg(&C.changed[widx]) & any) != any) atomicOr(&C.changed[widx], any);
+}
+
+// ---------------------------------------------------------------------------
+// Dense chaotic push: every admitted (source vertex, lane) pushes all of its
+// admitted out-edges in place each round.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void dense_item(const LaunchParams& p, const DBatch& B, DCtl& C, u32 item, u32 exec,
+                                           u32 widx) {
+  const u32 lane = lane_id();
+  const u32 sub = lane >> B.shift;
+  const u32 ql = lane & (B.W - 1u);
+  const u32 vpw = 32u >> B.shift;
+  const u32 cu = item * vpw + sub;
+  u32 changed = 0u;
+  if (cu < B.U) {
+    const u32 u = B.c2g[cu];
+    const uint2 ut = B.tiles[__ldg(p.g.owner + u)];
+    if (((ut.x & exec) >> ql) & 1u) {
+      const u32 sb = dev::hi(dev::ld_cg(B.dist[0] + ((static_cast<u64>(cu) << B.shift) + ql)));
+      if (sb != dev::kInfBits) {
+        const u32 rb = __ldg(p.g.csr_off + u), re = __ldg(p.g.csr_off + u + 1);
+        for (u32 e = rb; e < re; ++e) {
+          const uint4 rec = __ldg(p.g.csr + e);
+          const uint2 dt = B.tiles[rec.w];
+          if ((dt.x >> ql) & 1u) {
+            const u64 cand = dev::candidate(sb, rec.y, rec.z);
+            u64* const target = B.dist[0] + ((static_cast<u64>(rec.x - dt.y) << B.shift) + ql);
+            const u64 cur = dev::ld_cg(target);
+            if (cand < cur) {
+              dev::red_min(target, cand);
+              if (dev::hi(cand) < dev::hi(cur)) changed = 1u << ql;
+            }
+          }
+        }
+      }
+    }
+  }
+  const u32 any = __reduce_or_sync(0xFFFFFFFFu, changed);
+  if (lane == 0 && any != 0u && (dev::ld_cg(&C.changed[widx]) & any) != any) atomicOr(&C.changed[widx], any);
+}
+
+// ---------------------------------------------------------------------------
+// One round over every batch.  Returns false when the launch must stop.
+// Called by every block of the grid; `prefix` is dynamic shared memory of
+// nb+1 words.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ u32 batch_exec(const LaunchParams& p, u32 b, u32 ridx) {
+  const u32 ch = dev::ld_cg(&p.ctl[b].changed[ridx]);
+  if (p.engine == BFX_ENGINE_JACOBI_PULL) return ch != 0u ? p.batches[b].valid : 0u;
+  return p.per_lane ? ch : (ch != 0u ? p.batches[b].valid : 0u);
+}
+
+__device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
+  const u32 ridx = r % 3u, widx = (r + 1u) % 3u;
+  if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
+    block_prefix(prefix, p.nb, [&](u32 b) { return min(dev::ld_cg(&p.ctl[b].count[ridx]), p.batches[b].U); });
+  } else {
+    block_prefix(prefix, p.nb, [&](u32 b) {
+      const DBatch& B = p.batches[b];
+      return batch_exec(p, b, ridx) != 0u ? (((B.U << B.shift) + 31u) >> 5) : 0u;
+    });
+  }
+  return prefix[p.nb];
+}
+
+__device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix) {
+  const u32 ridx = r % 3u, widx = (r + 1u) % 3u;
+  const u32 total = prefix[p.nb];
+  const u32 warps_per_block = blockDim.x >> 5;
+  const u32 gw = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
+  const u32 nw = gridDim.x * warps_per_block;
+  for (u32 w = gw; w < total; w += nw) {
+    const u32 b = find_batch(prefix, p.nb, w);
+    const DBatch& B = p.batches[b];
+    DCtl& C = p.ctl[b];
+    const u32 item = w - prefix[b];
+    if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
+      const u32 v = dev::ld_cg(B.queue[r & 1u] + item);
+      frontier_entry(p, B, C, v, r & 1u, widx);
+    } else if (p.engine == BFX_ENGINE_JACOBI_PULL) {
+      jacobi_item(p, B, C, item, r, widx);
+    } else {
+      dense_item(p, B, C, item, batch_exec(p, b, ridx), widx);
+    }
+  }
+}
+
+// Bookkeeping at the start of round r, done by one thread: rounds counter
+// per batch, clear the rotating slot that round r+1 will write.
+__device__ void round_bookkeeping(const LaunchParams& p, u32 r) {
+  const u32 ridx = r % 3u, zidx = (r + 2u) % 3u;
+  for (u32 b = threadIdx.x; b < p.nb; b += blockDim.x) {
+    DCtl& C = p.ctl[b];
+    const bool work = p.engine == BFX_ENGINE_FRONTIER_PUSH ? dev::ld_cg(&C.count[ridx]) != 0u
+                                                          : batch_exec(p, b, ridx) != 0u;
+    if (work) C.rounds = r + 1u;
+    C.count[zidx] = 0u;
+    C.changed[zidx] = 0u;
+  }
+}
+
+__global__ void __launch_bounds__(1024) persistent_kernel(LaunchParams p) {
+  extern __shared__ u32 prefix[];
+  const u32 nblocks = gridDim.x;
+  u32 r = 0;
+  for (;; ++r) {
+    const u32 total = round_work(p, r, prefix);
+    if (total == 0u || r >= p.max_rounds) break;
+    if (blockIdx.x == 0) round_bookkeeping(p, r);
+    round_body(p, r, prefix);
+    if (!dev::grid_barrier(&p.run->sync, nblocks, kBarrierTimeoutNs)) {
+      if (threadIdx.x == 0) atomicExch(&p.run->abort, 1u);
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    p.run->round = r;
+    p.run->done = 1u;
+  }
+}
+
+// Host-poll modes: one round per launch over a fixed grid ...
+__global__ void __launch_bounds__(1024) round_kernel(LaunchParams p) {
+  extern __shared__ u32 prefix[];
+  if (dev::ld_cg(&p.run->done) != 0u) return;
+  const u32 r = dev::ld_cg(&p.run->round);
+  const u32 total = round_work(p, r, prefix);
+  if (total == 0u) return;
+  round_body(p, r, prefix);
+}
+
+// ... followed by a one-block advance: stop test, bookkeeping, next round.
+__global__ void advance_kernel(LaunchParams p) {
+  extern __shared__ u32 prefix[];
+  if (dev::ld_cg(&p.run->done) != 0u) return;
+  const u32 r = dev::ld_cg(&p.run->round);
+  // Bookkeeping for the round that just ran happens before the next one
+  // starts; the stop test looks at the round that would run next.
+  round_bookkeeping(p, r);
+  __syncthreads();
+  const u32 next_total = round_work(p, r + 1u, prefix);
+  if (threadIdx.x == 0) {
+    p.run->round = r + 1u;
+    if (next_total == 0u || static_cast<u64>(r + 1u) >= p.max_rounds) p.run->done = 1u;
+  }
+}
+
+// Before the first host-poll round: stop immediately if nothing to do.
+__global__ void start_kernel(LaunchParams p) {
+  extern __shared__ u32 prefix[];
+  const u32 total = round_work(p, 0u, prefix);
+  if (threadIdx.x == 0) {
+    p.run->round = 0u;
+    p.run->done = (total == 0u || p.max_rounds == 0u) ? 1u : 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Finalize: one block per batch.  Reached / miss lanes from target
+// finiteness (src/hip/batched_frontier_push.hip.cpp:971-1010), pending lanes
+// for round-limited stops, and the reference-format controller and status.
+// ---------------------------------------------------------------------------
+
+__global__ void finalize_kernel(LaunchParams p, bfx_device_controller* controllers, bfx_device_run_status* statuses) {
+  const u32 b = blockIdx.x;
+  const DBatch& B = p.batches[b];
+  DCtl& C = p.ctl[b];
+  __shared__ u32 s_missing, s_active;
+  if (threadIdx.x == 0) {
+    s_missing = 0u;
+    s_active = 0u;
+  }
+  __syncthreads();
+  const u32 r_end = p.run->round;
+  const u32 ridx = r_end % 3u;
+  const bool aborted = p.run->abort != 0u;
+  bool pending;
+  if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
+    pending = C.count[ridx] != 0u;
+  } else {
+    pending = batch_exec(p, b, ridx) != 0u;
+  }
+  const u32 final_slot = p.engine == BFX_ENGINE_JACOBI_PULL ? (C.rounds & 1u) : 0u;
+  const u64* const d = B.dist[final_slot];
+  for (u32 i = threadIdx.x; i < B.tgt_count; i += blockDim.x) {
+    const u32 lane = lane_of_position(B.tgt_off, B.W, i);
+    const u32 v = B.tgt[i];
+    const uint2 t = B.tiles[p.g.owner[v]];
+    bool reached = false;
+    if ((t.x >> lane) & 1u) reached = dev::hi(d[(static_cast<u64>(v - t.y) << B.shift) + lane]) != dev::kInfBits;
+    if (!reached) atomicOr(&s_missing, 1u << lane);
+  }
+  if (pending && !aborted) {
+    if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
+      const u32* const mk = B.mask[r_end & 1u];
+      u32 acc = 0u;
+      for (u32 i = threadIdx.x; i < B.U; i += blockDim.x) acc |= mk[i];
+      acc = __reduce_or_sync(0xFFFFFFFFu, acc);
+      if (lane_id() == 0 && acc) atomicOr(&s_active, acc);
+    } else if (threadIdx.x == 0) {
+      s_active = C.changed[ridx];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  u32 error_bits = C.error_bits;
+  u32 stop;
+  if (aborted) {
+    error_bits |= BFX_DEVICE_ERROR_DEVICE_FAILURE;
+  }
+  if (error_bits & BFX_DEVICE_ERROR_DEVICE_FAILURE) {
+    stop = BFX_STOP_DEVICE_FAILURE;
+    error_bits = BFX_DEVICE_ERROR_DEVICE_FAILURE;
+  } else if (error_bits & BFX_DEVICE_ERROR_QUEUE_OVERFLOW) {
+    stop = BFX_STOP_QUEUE_OVERFLOW;
+    error_bits = BFX_DEVICE_ERROR_QUEUE_OVERFLOW;
+  } else if (error_bits != 0u) {
+    stop = BFX_STOP_INVALID_CONTROLLER_STATE;
+    error_bits = BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE;
+  } else if (!pending) {
+    stop = BFX_STOP_CONVERGED;
+  } else {
+    stop = BFX_STOP_MAXIMUM_ROUNDS;
+  }
+  const bool converged = stop == BFX_STOP_CONVERGED;
+  const u32 valid = B.valid;
+  const u32 active = converged || error_bits ? 0u : (s_active & valid);
+  const u32 conv_lanes = converged ? valid : ((p.per_lane && !error_bits) ? (valid & ~active) : 0u);
+  bfx_device_run_status st;
+  st.final_distance_slot = final_slot;
+  st.converged = converged ? 1u : 0u;
+  st.rounds_completed = C.rounds;
+  st.reached_target_mask = converged ? (valid & ~s_missing) : 0u;
+  st.bounding_box_miss_mask = converged ? (valid & s_missing) : 0u;
+  st.valid_lane_mask = valid;
+  st.active_lane_mask = active;
+  st.converged_lane_mask = conv_lanes;
+  st.stop_reason = stop;
+  st.error_bits = error_bits;
+  st.reserved0 = 0u;
+  statuses[b] = st;
+  bfx_device_controller c;
+  memset(&c, 0, sizeof(c));
+  c.valid_lane_mask = valid;
+  c.active_lane_mask = active;
+  c.converged_lane_mask = conv_lanes;
+  c.engine_kind = p.engine;
+  c.enable_per_lane_convergence = p.per_lane;
+  c.rounds_completed = C.rounds;
+  c.maximum_rounds = p.max_rounds;
+  c.distance_read_slot = final_slot;
+  c.distance_write_slot = p.engine == BFX_ENGINE_JACOBI_PULL ? (final_slot ^ 1u) : 0u;
+  c.frontier_read_slot = r_end & 1u;
+  c.frontier_write_slot = (r_end & 1u) ^ 1u;
+  c.frontier_size[r_end & 1u] = p.engine == BFX_ENGINE_FRONTIER_PUSH ? C.count[ridx] : 0u;
+  c.done = 1u;
+  c.stop_reason = stop;
+  c.error_bits = error_bits;
+  controllers[b] = c;
+}
+
+// Graph-sized label image of one batch: bits / predecessor edge ids.
+__global__ void expand_kernel(DGraph g, DBatch B, u32 slot, u32* bits, u32* preds) {
+  const u64 n = static_cast<u64>(g.V) << B.shift;
+  for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<u64>(gridDim.x) * blockDim.x) {
+    const u32 v = static_cast<u32>(i >> B.shift);
+    const u32 l = static_cast<u32>(i & (B.W - 1u));
+    const uint2 t = B.tiles[g.owner[v]];
+    u64 w = dev::kUnreached;
+    if ((t.x >> l) & 1u) w = B.dist[slot][(static_cast<u64>(v - t.y) << B.shift) + l];
+    if (bits) bits[i] = dev::hi(w);
+    if (preds) {
+      const u32 lo = static_cast<u32>(w);
+      preds[i] = (lo == 0u || lo == 0xFFFFFFFFu) ? 0xFFFFFFFFu : lo - 1u;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+struct DeviceBuffer {
+  void* ptr{nullptr};
+  size_t bytes{0};
+  int device{0};
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer() { release(); }
+  void release() {
+    if (ptr) {
+      cudaSetDevice(device);
+      cudaFree(ptr);
+    }
+    ptr = nullptr;
+    bytes = 0;
+  }
+  // Grows geometrically; contents are not preserved.
+  void reserve(size_t need, int dev) {
+    if (need <= bytes && ptr) return;
+    release();
+    device = dev;
+    size_t cap = std::max(need, bytes + bytes / 2);
+    cap = (cap + 255) & ~size_t{255};
+    BFX_CUDA(cudaMalloc(&ptr, cap));
+    bytes = cap;
+  }
+};
+
+struct PinnedBuffer {
+  void* ptr{nullptr};
+  size_t bytes{0};
+  PinnedBuffer() = default;
+  PinnedBuffer(const PinnedBuffer&) = delete;
+  PinnedBuffer& operator=(const PinnedBuffer&) = delete;
+  ~PinnedBuffer() {
+    if (ptr) cudaFreeHost(ptr);
+  }
+  void reserve(size_t need) {
+    if (need <= bytes && ptr) return;
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    size_t cap = std::max(need, bytes + bytes / 2);
+    cap = (cap + 255) & ~size_t{255};
+    BFX_CUDA(cudaHostAlloc(&ptr, cap, cudaHostAllocDefault));
+    bytes = cap;
+  }
+};
+
+}  // namespace bfx
+
+struct bfx_resident_graph {
+  int device{0};
+  bfx::DGraph g{};
+  bfx::DeviceBuffer mem;
+  std::vector<std::uint32_t> tile_vertex_offsets;  // host copy, [T+1]
+  std::uint64_t bytes{0};
+};
+
+struct bfx_workspace {
+  bfx_resident_graph* graph{nullptr};
+  cudaStream_t stream{nullptr};
+  int sm_count{0};
+  // Prepared batch set.
+  std::uint32_t nb{0};
+  std::uint64_t src_total{0};
+  std::vector<bfx::DBatch> batches;
+  bfx::DeviceBuffer meta;   // DBatch[], DCtl[], DRun, unit_base, src_base, uploaded descriptions
+  bfx::DeviceBuffer arena;  // labels, masks, queues, c2g, tile tables
+  bfx::PinnedBuffer staging;
+  bfx::PinnedBuffer status_host;
+  size_t meta_bytes{0};
+  size_t arena_bytes{0};
+  bool needs_slot2{false};
+  bfx::LaunchParams params{};
+  bfx::u32* src_base{nullptr};
+  bfx_device_run_status* d_status{nullptr};
+  bfx_device_controller* d_ctrl{nullptr};
+  std::uint64_t last_launches{0};
+  bool executed{false};
+  // Host-poll graph cache, keyed by the exact launch parameters.
+  cudaGraphExec_t chunk_exec{nullptr};
+  std::uint32_t chunk_rounds{0};
+  int chunk_grid{0};
+  int chunk_block{0};
+  bfx::LaunchParams chunk_params{};
+  std::uint64_t generation{0};
+};
+
+namespace bfx {
+namespace {
+
+std::mutex g_graph_mutex;
+
+size_t align256(size_t x) { return (x + 255) & ~size_t{255}; }
+
+void upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes) BFX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+}
+
+void check_layout(const bfx_device_graph_layout32& L) {
+  require(L.owner_tiles && L.csr_row_offsets && L.csr_destinations && L.csr_weights && L.csc_column_offsets &&
+              L.csc_sources && L.csc_weights && L.csc_edge_ids,
+          "device layout arrays must be non-null");
+  const std::uint32_t V = L.vertex_count, E = L.edge_count, T = L.tile_count;
+  require(T >= 1, "device layout needs at least one tile");
+  require(L.csr_row_offsets[0] == 0 && L.csr_row_offsets[V] == E, "invalid CSR offsets");
+  require(L.csc_column_offsets[0] == 0 && L.csc_column_offsets[V] == E, "invalid CSC offsets");
+  for (std::uint32_t v = 0; v < V; ++v) {
+    require(L.csr_row_offsets[v] <= L.csr_row_offsets[v + 1], "invalid CSR offsets");
+    require(L.csc_column_offsets[v] <= L.csc_column_offsets[v + 1], "invalid CSC offsets");
+    require(L.owner_tiles[v] < T, "owner tile out of range");
+    require(v == 0 || L.owner_tiles[v] >= L.owner_tiles[v - 1], "owner tiles must be contiguous spans");
+  }
+  for (std::uint32_t e = 0; e < E; ++e) {
+    if (L.csr_destinations[e] >= V || L.csc_sources[e] >= V) throw std::out_of_range("edge endpoint out of range");
+    if (L.csc_edge_ids[e] >= E) throw std::out_of_range("edge id out of range");
+    require(L.csr_weights[e] >= 0.0F && L.csc_weights[e] >= 0.0F, "invalid stored weight");
+  }
+}
+
+}  // namespace
+}  // namespace bfx
+
+extern "C" {
+
+int bfx_abi_version(void) { return BFX_ABI_VERSION; }
+
+const char* bfx_last_error(void) { return bfx::g_last_error.c_str(); }
+
+int bfx_device_count(int* count) {
+  return bfx::guarded([&] {
+    bfx::require(count != nullptr, "null output");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+      cudaGetLastError();
+      n = 0;
+    }
+    *count = n;
+  });
+}
+
+int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int device, bfx_resident_graph** out) {
+  return bfx::guarded([&] {
+    bfx::require(layout && out, "null argument");
+    *out = nullptr;
+    const bfx_device_graph_layout32& L = *layout;
+    bfx::check_layout(L);
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+      cudaGetLastError();
+      throw bfx::Error(BFX_ERR_NO_DEVICE, "no CUDA device is available");
+    }
+    if (device < 0 || device >= n) throw std::out_of_range("device index");
+    BFX_CUDA(cudaSetDevice(device));
+    const std::uint32_t V = L.vertex_count, E = L.edge_count, T = L.tile_count;
+    // Stable EdgeId per CSR position: given, or matched from the CSC image
+    // (each CSC entry (dst, src, eid) is one CSR entry of row src).
+    std::vector<std::uint32_t> csr_eid;
+    const std::uint32_t* eids = L.csr_edge_ids;
+    if (!eids) {
+      csr_eid.assign(E, 0xFFFFFFFFu);
+      std::vector<std::uint32_t> cursor(L.csr_row_offsets, L.csr_row_offsets + V);
+      // CSR rows are ordered by (dst tile, dst, eid); visiting CSC entries in
+      // increasing eid per (src, dst) pair reproduces that order.
+      std::vector<std::uint64_t> order(E);
+      for (std::uint32_t v = 0; v < V; ++v) {
+        for (std::uint32_t q = L.csc_column_offsets[v]; q < L.csc_column_offsets[v + 1]; ++q) order[q] = q;
+      }
+      std::vector<std::uint32_t> col_of(E);
+      for (std::uint32_t v = 0; v < V; ++v) {
+        for (std::uint32_t q = L.csc_column_offsets[v]; q < L.csc_column_offsets[v + 1]; ++q) col_of[q] = v;
+      }
+      std::sort(order.begin(), order.end(), [&](std::uint64_t a, std::uint64_t b) {
+        const std::uint32_t sa = L.csc_sources[a], sb = L.csc_sources[b];
+        if (sa != sb) return sa < sb;
+        const std::uint32_t da = col_of[a], db = col_of[b];
+        if (L.owner_tiles[da] != L.owner_tiles[db]) return L.owner_tiles[da] < L.owner_tiles[db];
+        if (da != db) return da < db;
+        return L.csc_edge_ids[a] < L.csc_edge_ids[b];
+      });
+      for (std::uint64_t i = 0; i < E; ++i) {
+        const std::uint32_t q = static_cast<std::uint32_t>(order[i]);
+        const std::uint32_t p = cursor[L.csc_sources[q]]++;
+        bfx::require(L.csr_destinations[p] == col_of[q], "CSR and CSC images disagree");
+        csr_eid[p] = L.csc_edge_ids[q];
+      }
+      eids = csr_eid.data();
+    }
+    auto G = std::make_unique<bfx_resident_graph>();
+    G->device = device;
+    G->tile_vertex_offsets.assign(T + 1U, 0U);
+    for (std::uint32_t v = 0; v < V; ++v) ++G->tile_vertex_offsets[L.owner_tiles[v] + 1U];
+    for (std::uint32_t t = 0; t < T; ++t) G->tile_vertex_offsets[t + 1] += G->tile_vertex_offsets[t];
+
+    std::vector<uint4> csr(E), csc(E);
+    bfx::parallel_for(V, 0, [&](std::uint64_t b, std::uint64_t e) {
+      for (std::uint64_t v = b; v < e; ++v) {
+        for (std::uint32_t p = L.csr_row_offsets[v]; p < L.csr_row_offsets[v + 1]; ++p) {
+          const std::uint32_t d = L.csr_destinations[p];
+          std::uint32_t wb;
+          std::memcpy(&wb, &L.csr_weights[p], 4);
+          csr[p] = make_uint4(d, wb, eids[p] + 1U, L.owner_tiles[d]);
+        }
+        for (std::uint32_t q = L.csc_column_offsets[v]; q < L.csc_column_offsets[v + 1]; ++q) {
+          const std::uint32_t s = L.csc_sources[q];
+          std::uint32_t wb;
+          std::memcpy(&wb, &L.csc_weights[q], 4);
+          csc[q] = make_uint4(s, wb, L.csc_edge_ids[q] + 1U, L.owner_tiles[s]);
+        }
+      }
+    });
+    const size_t o_owner = 0;
+    const size_t o_csr_off = bfx::align256(o_owner + size_t{V} * 4);
+    const size_t o_csc_off = bfx::align256(o_csr_off + (size_t{V} + 1) * 4);
+    const size_t o_csr = bfx::align256(o_csc_off + (size_t{V} + 1) * 4);
+    const size_t o_csc = bfx::align256(o_csr + size_t{E} * 16);
+    const size_t total = bfx::align256(o_csc + size_t{E} * 16);
+    G->mem.reserve(total, device);
+    char* base = static_cast<char*>(G->mem.ptr);
+    BFX_CUDA(cudaMemcpy(base + o_owner, L.owner_tiles, size_t{V} * 4, cudaMemcpyHostToDevice));
+    BFX_CUDA(cudaMemcpy(base + o_csr_off, L.csr_row_offsets, (size_t{V} + 1) * 4, cudaMemcpyHostToDevice));
+    BFX_CUDA(cudaMemcpy(base + o_csc_off, L.csc_column_offsets, (size_t{V} + 1) * 4, cudaMemcpyHostToDevice));
+    BFX_CUDA(cudaMemcpy(base + o_csr, csr.data(), size_t{E} * 16, cudaMemcpyHostToDevice));
+    BFX_CUDA(cudaMemcpy(base + o_csc, csc.data(), size_t{E} * 16, cudaMemcpyHostToDevice));
+    G->g.V = V;
+    G->g.E = E;
+    G->g.T = T;
+    G->g.owner = reinterpret_cast<const std::uint32_t*>(base + o_owner);
+    G->g.csr_off = reinterpret_cast<const std::uint32_t*>(base + o_csr_off);
+    G->g.csc_off = reinterpret_cast<const std::uint32_t*>(base + o_csc_off);
+    G->g.csr = reinterpret_cast<const uint4*>(base + o_csr);
+    G->g.csc = reinterpret_cast<const uint4*>(base + o_csc);
+    G->bytes = total;
+    *out = G.release();
+  });
+}
+
+int bfx_resident_graph_destroy(bfx_resident_graph* graph) {
+  return bfx::guarded([&] { delete graph; });
+}
+
+int bfx_resident_graph_info(const bfx_resident_graph* graph, uint64_t out[4]) {
+  return bfx::guarded([&] {
+    bfx::require(graph && out, "null argument");
+    out[0] = graph->g.V;
+    out[1] = graph->g.E;
+    out[2] = graph->g.T;
+    out[3] = graph->bytes;
+  });
+}
+
+int bfx_workspace_create(bfx_resident_graph* graph, bfx_workspace** out) {
+  return bfx::guarded([&] {
+    bfx::require(graph && out, "null argument");
+    *out = nullptr;
+    BFX_CUDA(cudaSetDevice(graph->device));
+    auto ws = std::make_unique<bfx_workspace>();
+    ws->graph = graph;
+    BFX_CUDA(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
+    BFX_CUDA(cudaDeviceGetAttribute(&ws->sm_count, cudaDevAttrMultiProcessorCount, graph->device));
+    *out = ws.release();
+  });
+}
+
+int bfx_workspace_destroy(bfx_workspace* ws) {
+  return bfx::guarded([&] {
+    if (!ws) return;
+    cudaSetDevice(ws->graph->device);
+    if (ws->stream) cudaStreamSynchronize(ws->stream);
+    if (ws->chunk_exec) cudaGraphExecDestroy(ws->chunk_exec);
+    if (ws->stream) cudaStreamDestroy(ws->stream);
+    delete ws;
+  });
+}
+
+int bfx_workspace_stream(bfx_workspace* ws, void** stream) {
+  return bfx::guarded([&] {
+    bfx::require(ws && stream, "null argument");
+    *stream = ws->stream;
+  });
+}
+
+int bfx_workspace_bytes(bfx_workspace* ws, uint64_t* bytes) {
+  return bfx::guarded([&] {
+    bfx::require(ws && bytes, "null argument");
+    *bytes = ws->meta.bytes + ws->arena.bytes;
+  });
+}
+
+int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_description* batches) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null workspace");
+    bfx::require(count > 0 && batches, "at least one batch is required");
+    if (count > bfx::kMaxBatchesPerLaunch) throw std::length_error("too many batches for one launch");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    const bfx::DGraph& g = ws->graph->g;
+    const auto& tvo = ws->graph->tile_vertex_offsets;
+    // Validate descriptions (validate_batch_device_description,
+    // include/bfnew/batch_layout.hpp:176-199) and size everything.
+    struct Sizes {
+      std::uint32_t U, R, S, Tg, W, shift;
+    };
+    std::vector<Sizes> sz(count);
+    size_t up_bytes = 0;
+    for (std::uint32_t b = 0; b < count; ++b) {
+      const bfx_batch_description& d = batches[b];
+      const std::uint32_t W = d.lane_width;
+      bfx::require(W == 1 || W == 8 || W == 16 || W == 32, "unsupported lane width");
+      const std::uint32_t wmask = W == 32 ? 0xFFFFFFFFu : ((1u << W) - 1u);
+      bfx::require(d.valid_lane_mask != 0 && (d.valid_lane_mask & ~wmask) == 0, "invalid valid lane mask");
+      bfx::require(d.tile_count == g.T, "description tile count does not match the graph");
+      bfx::require(d.source_offsets && d.target_offsets && d.tile_lane_masks && d.union_tiles &&
+                       (d.range_count == 0 || d.selected_vertex_ranges),
+                   "null description array");
+      bfx::require(d.source_offsets[0] == 0 && d.target_offsets[0] == 0, "invalid terminal offsets");
+      for (std::uint32_t l = 0; l < W; ++l) {
+        bfx::require(d.source_offsets[l + 1] >= d.source_offsets[l] && d.target_offsets[l + 1] >= d.target_offsets[l],
+                     "invalid terminal offsets");
+        const bool valid = (d.valid_lane_mask >> l) & 1u;
+        const bool has_s = d.source_offsets[l + 1] > d.source_offsets[l];
+        const bool has_t = d.target_offsets[l + 1] > d.target_offsets[l];
+        bfx::require(valid ? (has_s && has_t) : (!has_s && !has_t), "invalid terminal payload");
+      }
+      const std::uint32_t S = d.source_offsets[W], Tg = d.target_offsets[W];
+      bfx::require(S == 0 || d.sources, "null sources");
+      bfx::require(Tg == 0 || d.targets, "null targets");
+      bfx::require(d.range_count == d.union_tile_count, "one vertex range per union tile is required");
+      std::uint64_t U = 0;
+      for (std::uint32_t i = 0; i < d.union_tile_count; ++i) {
+        const std::uint32_t t = d.union_tiles[i];
+        if (t >= g.T) throw std::out_of_range("union tile out of range");
+        bfx::require(i == 0 || t > d.union_tiles[i - 1], "union tiles must be strictly increasing");
+        const bfx_batch_vertex_range& r = d.selected_vertex_ranges[i];
+        bfx::require(r.begin == tvo[t] && r.end == tvo[t + 1], "vertex range does not match its tile");
+        bfx::require(r.lane_mask == d.tile_lane_masks[t] && r.lane_mask != 0 && (r.lane_mask & ~d.valid_lane_mask) == 0,
+                     "invalid tile lane mask");
+        U += r.end - r.begin;
+      }
+      bfx::require(U > 0, "batch has no selected vertices");
+      if (U > 0x7FFFFFFFull) throw std::overflow_error("union vertex count exceeds the device index range");
+      for (std::uint32_t l = 0; l < W; ++l) {
+        for (std::uint32_t i = d.source_offsets[l]; i < d.source_offsets[l + 1]; ++i) {
+          const std::uint32_t v = d.sources[i];
+          if (v >= g.V) throw std::out_of_range("source out of range");
+        }
+        for (std::uint32_t i = d.target_offsets[l]; i < d.target_offsets[l + 1]; ++i) {
+          if (d.targets[i] >= g.V) throw std::out_of_range("target out of range");
+        }
+      }
+      sz[b] = Sizes{static_cast<std::uint32_t>(U), d.range_count, S, Tg, W, static_cast<std::uint32_t>(__builtin_ctz(W))};
+      up_bytes += bfx::align256((W + 1) * 4) * 2 + bfx::align256(size_t{S} * 4) + bfx::align256(size_t{Tg} * 4) +
+                  bfx::align256(size_t{d.range_count} * 16) + bfx::align256((size_t{d.range_count} + 1) * 4);
+    }
+    // Terminal ownership: a terminal's owner tile must be selected for its
+    // lane (terminal_owner_tile_not_selected, src/query.cpp:221-236).
+    auto owner_of = [&](std::uint32_t v) {
+      return static_cast<std::uint32_t>(std::upper_bound(tvo.begin(), tvo.end(), v) - tvo.begin()) - 1U;
+    };
+    for (std::uint32_t b = 0; b < count; ++b) {
+      const bfx_batch_description& d = batches[b];
+      for (std::uint32_t l = 0; l < d.lane_width; ++l) {
+        for (std::uint32_t i = d.source_offsets[l]; i < d.source_offsets[l + 1]; ++i) {
+          bfx::require((d.tile_lane_masks[owner_of(d.sources[i])] >> l) & 1u, "terminal owner tile not selected");
+          bfx::require(i == d.source_offsets[l] || d.sources[i] > d.sources[i - 1], "noncanonical sources");
+        }
+        for (std::uint32_t i = d.target_offsets[l]; i < d.target_offsets[l + 1]; ++i) {
+          bfx::require((d.tile_lane_masks[owner_of(d.targets[i])] >> l) & 1u, "terminal owner tile not selected");
+          bfx::require(i == d.target_offsets[l] || d.targets[i] > d.targets[i - 1], "noncanonical targets");
+        }
+      }
+    }
+    // Metadata block: DBatch[nb], DCtl[nb], DRun, unit_base[nb+1], src_base[nb+1],
+    // statuses, controllers, then uploaded description arrays.
+    const size_t o_batch = 0;
+    const size_t o_ctl = bfx::align256(o_batch + count * sizeof(bfx::DBatch));
+    const size_t o_run = bfx::align256(o_ctl + count * sizeof(bfx::DCtl));
+    const size_t o_ubase = bfx::align256(o_run + sizeof(bfx::DRun));
+    const size_t o_sbase = bfx::align256(o_ubase + (count + 1) * 4);
+    const size_t o_status = bfx::align256(o_sbase + (count + 1) * 4);
+    const size_t o_ctrl = bfx::align256(o_status + count * sizeof(bfx_device_run_status));
+    const size_t o_up = bfx::align256(o_ctrl + count * sizeof(bfx_device_controller));
+    const size_t meta_total = o_up + up_bytes;
+    // Arena: per batch labels (2 slots reserved so one prepare serves every
+    // engine), masks, queues, c2g, tile table.
+    std::vector<size_t> arena_off(count);
+    size_t arena_total = 0;
+    for (std::uint32_t b = 0; b < count; ++b) {
+      arena_off[b] = arena_total;
+      const size_t U = sz[b].U;
+      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 5 + bfx::align256(size_t{g.T} * 8);
+    }
+    const bool grew = meta_total > ws->meta.bytes || arena_total > ws->arena.bytes;
+    ws->meta.reserve(meta_total, ws->graph->device);
+    ws->arena.reserve(arena_total, ws->graph->device);
+    if (grew) ++ws->generation;
+    ws->staging.reserve(meta_total);
+    char* hb = static_cast<char*>(ws->staging.ptr);
+    char* db = static_cast<char*>(ws->meta.ptr);
+    char* ab = static_cast<char*>(ws->arena.ptr);
+    std::memset(hb, 0, o_up);
+    ws->batches.assign(count, bfx::DBatch{});
+    std::uint32_t* ubase = reinterpret_cast<std::uint32_t*>(hb + o_ubase);
+    std::uint32_t* sbase = reinterpret_cast<std::uint32_t*>(hb + o_sbase);
+    size_t up = o_up;
+    std::uint64_t usum = 0, ssum = 0;
+    for (std::uint32_t b = 0; b < count; ++b) {
+      const bfx_batch_description& d = batches[b];
+      const Sizes& s = sz[b];
+      bfx::DBatch& B = ws->batches[b];
+      B.W = s.W;
+      B.shift = s.shift;
+      B.valid = d.valid_lane_mask;
+      B.U = s.U;
+      B.src_count = s.S;
+      B.tgt_count = s.Tg;
+      B.range_count = s.R;
+      auto put = [&](const void* src, size_t bytes) -> const void* {
+        std::memcpy(hb + up, src, bytes);
+        const void* dptr = db + up;
+        up += bfx::align256(bytes);
+        return dptr;
+      };
+      B.src_off = static_cast<const std::uint32_t*>(put(d.source_offsets, (s.W + 1) * 4));
+      B.src = static_cast<const std::uint32_t*>(put(d.sources, size_t{s.S} * 4));
+      B.tgt_off = static_cast<const std::uint32_t*>(put(d.target_offsets, (s.W + 1) * 4));
+      B.tgt = static_cast<const std::uint32_t*>(put(d.targets, size_t{s.Tg} * 4));
+      std::vector<uint4> ranges(s.R);
+      std::vector<std::uint32_t> roff(s.R + 1, 0U);
+      for (std::uint32_t i = 0; i < s.R; ++i) {
+        const bfx_batch_vertex_range& r = d.selected_vertex_ranges[i];
+        ranges[i] = make_uint4(d.union_tiles[i], r.begin, r.end, r.lane_mask);
+        roff[i + 1] = roff[i] + (r.end - r.begin);
+      }
+      B.ranges = static_cast<const uint4*>(put(ranges.data(), size_t{s.R} * 16));
+      B.range_off = static_cast<const std::uint32_t*>(put(roff.data(), (size_t{s.R} + 1) * 4));
+      char* a = ab + arena_off[b];
+      const size_t U = s.U;
+      B.dist[0] = reinterpret_cast<bfx::u64*>(a);
+      a += bfx::align256(U * s.W * 8);
+      B.dist[1] = reinterpret_cast<bfx::u64*>(a);
+      a += bfx::align256(U * s.W * 8);
+      B.mask[0] = reinterpret_cast<std::uint32_t*>(a);
+      a += bfx::align256(U * 4);
+      B.mask[1] = reinterpret_cast<std::uint32_t*>(a);
+      a += bfx::align256(U * 4);
+      B.queue[0] = reinterpret_cast<std::uint32_t*>(a);
+      a += bfx::align256(U * 4);
+      B.queue[1] = reinterpret_cast<std::uint32_t*>(a);
+      a += bfx::align256(U * 4);
+      B.c2g = reinterpret_cast<std::uint32_t*>(a);
+      a += bfx::align256(U * 4);
+      B.tiles = reinterpret_cast<uint2*>(a);
+      ubase[b] = static_cast<std::uint32_t>(usum);
+      sbase[b] = static_cast<std::uint32_t>(ssum);
+      usum += U;
+      ssum += s.S;
+      if (usum > 0xFFFFFFFFull) throw std::overflow_error("total union vertices exceed 32 bits");
+    }
+    ubase[count] = static_cast<std::uint32_t>(usum);
+    sbase[count] = static_cast<std::uint32_t>(ssum);
+    std::memcpy(hb + o_batch, ws->batches.data(), count * sizeof(bfx::DBatch));
+    bfx::upload(db, hb, meta_total, ws->stream);
+    // Tile tables must read 0 outside the union.
+    for (std::uint32_t b = 0; b < count; ++b) {
+      BFX_CUDA(cudaMemsetAsync(ws->batches[b].tiles, 0, size_t{g.T} * 8, ws->stream));
+    }
+    ws->nb = count;
+    ws->src_total = ssum;
+    ws->params = bfx::LaunchParams{};
+    ws->params.g = g;
+    ws->params.batches = reinterpret_cast<const bfx::DBatch*>(db + o_batch);
+    ws->params.ctl = reinterpret_cast<bfx::DCtl*>(db + o_ctl);
+    ws->params.run = reinterpret_cast<bfx::DRun*>(db + o_run);
+    ws->params.unit_base = reinterpret_cast<const std::uint32_t*>(db + o_ubase);
+    ws->params.nb = count;
+    ws->src_base = reinterpret_cast<bfx::u32*>(db + o_sbase);
+    ws->d_status = reinterpret_cast<bfx_device_run_status*>(db + o_status);
+    ws->d_ctrl = reinterpret_cast<bfx_device_controller*>(db + o_ctrl);
+    ws->executed = false;
+    // Staging must outlive the async copy: synchronise before the host may
+    // reuse it (the next prepare overwrites it).
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+  });
+}
+
+}  // extern "C"
+
+namespace bfx {
+namespace {
+
+void validate_options(const bfx_gpu_run_options& o) {
+  if (o.engine > 2u) throw std::invalid_argument("invalid engine");
+  if (o.control_mode > 2u) throw std::invalid_argument("invalid control mode");
+  if (o.rounds_per_chunk == 0u) throw std::invalid_argument("invalid rounds per chunk");
+  if (o.block_size == 0u || o.block_size % 32u != 0u || o.block_size > 1024u)
+    throw std::invalid_argument("invalid block size");
+  if (o.grid_policy > 1u) throw std::invalid_argument("invalid grid policy");
+  if (o.grid_policy == 1u && o.blocks_per_wgp == 0u) throw std::invalid_argument("invalid blocks per SM");
+  if (o.grid_policy == 0u && o.blocks_per_wgp != 0u) throw std::invalid_argument("invalid blocks per SM");
+  if (o.instrumentation > 2u) throw std::invalid_argument("invalid instrumentation");
+  if (o.maximum_rounds == 0u) throw std::invalid_argument("invalid maximum rounds");
+  if (o.enable_per_lane_convergence > 1u) throw std::invalid_argument("invalid per-lane convergence flag");
+}
+
+int grid_blocks(bfx_workspace* ws, const void* kernel, int block, size_t smem, const bfx_gpu_run_options& o) {
+  int per_sm = 0;
+  BFX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem));
+  if (per_sm <= 0) throw Error(BFX_ERR_CUDA, "kernel cannot be resident with this block size");
+  if (o.grid_policy == 1u) {
+    if (static_cast<int>(o.blocks_per_wgp) > per_sm)
+      throw std::invalid_argument("blocks per SM exceed the cooperative residency limit");
+    per_sm = static_cast<int>(o.blocks_per_wgp);
+  }
+  return per_sm * ws->sm_count;
+}
+
+void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
+  require(ws->nb > 0, "no prepared batches");
+  validate_options(o);
+  BFX_CUDA(cudaSetDevice(ws->graph->device));
+  LaunchParams p = ws->params;
+  p.engine = o.engine;
+  p.per_lane = o.enable_per_lane_convergence;
+  p.max_rounds = o.maximum_rounds;
+  const int block = static_cast<int>(o.block_size);
+  const size_t smem = (size_t{ws->nb} + 1) * 4;
+  std::uint64_t launches = 0;
+  // init + seed with a wide ordinary grid
+  const int wide = ws->sm_count * 8;
+  init_kernel<<<wide, 256, 0, ws->stream>>>(p);
+  ++launches;
+  BFX_CUDA(cudaGetLastError());
+  const int seed_blocks = static_cast<int>(std::min<std::uint64_t>(
+      std::max<std::uint64_t>(1, (ws->src_total + 255) / 256), static_cast<std::uint64_t>(wide)));
+  seed_kernel<<<seed_blocks, 256, 0, ws->stream>>>(p, ws->src_base);
+  ++launches;
+  BFX_CUDA(cudaGetLastError());
+  if (o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
+    const int grid = grid_blocks(ws, reinterpret_cast<const void*>(persistent_kernel), block, smem, o);
+    void* args[] = {&p};
+    BFX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(persistent_kernel), grid, block, args, smem,
+                                         ws->stream));
+    ++launches;
+  } else {
+    const std::uint32_t K = o.control_mode == BFX_CONTROL_PER_ROUND_HOST_POLL ? 1u : o.rounds_per_chunk;
+    const int grid = grid_blocks(ws, reinterpret_cast<const void*>(round_kernel), block, smem, o);
+    start_kernel<<<1, 1024, smem, ws->stream>>>(p);
+    ++launches;
+    BFX_CUDA(cudaGetLastError());
+    // Capture K x (round, advance) once per workspace generation / K / engine.
+    const bool reuse = ws->chunk_exec && ws->chunk_rounds == K && ws->chunk_grid == grid &&
+                       ws->chunk_block == block && std::memcmp(&ws->chunk_params, &p, sizeof(p)) == 0;
+    if (!reuse) {
+      if (ws->chunk_exec) cudaGraphExecDestroy(ws->chunk_exec);
+      ws->chunk_exec = nullptr;
+      cudaGraph_t graph;
+      BFX_CUDA(cudaStreamBeginCapture(ws->stream, cudaStreamCaptureModeThreadLocal));
+      for (std::uint32_t k = 0; k < K; ++k) {
+        round_kernel<<<grid, block, smem, ws->stream>>>(p);
+        advance_kernel<<<1, 1024, smem, ws->stream>>>(p);
+      }
+      BFX_CUDA(cudaStreamEndCapture(ws->stream, &graph));
+      const cudaError_t ie = cudaGraphInstantiate(&ws->chunk_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      BFX_CUDA(ie);
+      ws->chunk_rounds = K;
+      ws->chunk_grid = grid;
+      ws->chunk_block = block;
+      ws->chunk_params = p;
+    }
+    // Poll the device controller after every chunk, as the reference's
+    // ordinary modes do (src/hip/batched_frontier_push.hip.cpp:1613-1654).
+    ws->status_host.reserve(256);
+    std::uint32_t* const done_host = static_cast<std::uint32_t*>(ws->status_host.ptr);
+    const std::uint64_t max_chunks = (o.maximum_rounds + K - 1) / K + 1;
+    for (std::uint64_t c = 0; c < max_chunks; ++c) {
+      BFX_CUDA(cudaMemcpyAsync(done_host, &p.run->done, 4, cudaMemcpyDeviceToHost, ws->stream));
+      BFX_CUDA(cudaStreamSynchronize(ws->stream));
+      if (*done_host) break;
+      BFX_CUDA(cudaGraphLaunch(ws->chunk_exec, ws->stream));
+      launches += 2ull * K;
+    }
+  }
+  BFX_CUDA(cudaGetLastError());
+  finalize_kernel<<<ws->nb, 256, 0, ws->stream>>>(p, ws->d_ctrl, ws->d_status);
+  ++launches;
+  BFX_CUDA(cudaGetLastError());
+  ws->last_launches = launches;
+  ws->executed = true;
+  ws->params.engine = o.engine;
+  ws->params.per_lane = o.enable_per_lane_convergence;
+}
+
+}  // namespace
+}  // namespace bfx
+
+extern "C" {
+
+int bfx_execute(bfx_workspace* ws, const bfx_gpu_run_options* options) {
+  return bfx::guarded([&] {
+    bfx::require(ws && options, "null argument");
+    bfx::execute(ws, *options);
+  });
+}
+
+int bfx_fetch_statuses(bfx_workspace* ws, bfx_device_run_status* statuses, bfx_device_controller* controllers) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null workspace");
+    bfx::require(ws->executed, "no executed batches");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    const size_t sb = ws->nb * sizeof(bfx_device_run_status);
+    const size_t cb = ws->nb * sizeof(bfx_device_controller);
+    ws->status_host.reserve(sb + cb + 256);
+    char* h = static_cast<char*>(ws->status_host.ptr);
+    if (statuses) BFX_CUDA(cudaMemcpyAsync(h, ws->d_status, sb, cudaMemcpyDeviceToHost, ws->stream));
+    if (controllers) BFX_CUDA(cudaMemcpyAsync(h + sb, ws->d_ctrl, cb, cudaMemcpyDeviceToHost, ws->stream));
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    if (statuses) std::memcpy(statuses, h, sb);
+    if (controllers) std::memcpy(controllers, h + sb, cb);
+  });
+}
+
+int bfx_run_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_description* batches,
+                    const bfx_gpu_run_options* options, bfx_device_run_status* statuses) {
+  int rc = bfx_prepare_batches(ws, count, batches);
+  if (rc != BFX_OK) return rc;
+  rc = bfx_execute(ws, options);
+  if (rc != BFX_OK) return rc;
+  return bfx_fetch_statuses(ws, statuses, nullptr);
+}
+
+int bfx_download_labels(bfx_workspace* ws, uint32_t batch, uint32_t* distance_bits, uint32_t* predecessor_edges) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null workspace");
+    bfx::require(ws->executed, "no executed batches");
+    if (batch >= ws->nb) throw std::out_of_range("batch index");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    const bfx::DBatch& B = ws->batches[batch];
+    const size_t n = static_cast<size_t>(ws->graph->g.V) << B.shift;
+    std::uint32_t slot = 0;
+    if (ws->params.engine == BFX_ENGINE_JACOBI_PULL) {
+      bfx_device_run_status st;
+      BFX_CUDA(cudaMemcpy(&st, ws->d_status + batch, sizeof(st), cudaMemcpyDeviceToHost));
+      slot = st.final_distance_slot;
+    }
+    std::uint32_t* d_out = nullptr;
+    BFX_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_out), n * 8, ws->stream));
+    bfx::expand_kernel<<<ws->sm_count * 8, 256, 0, ws->stream>>>(ws->graph->g, B, slot, d_out, d_out + n);
+    const cudaError_t le = cudaGetLastError();
+    if (le == cudaSuccess) {
+      if (distance_bits) cudaMemcpyAsync(distance_bits, d_out, n * 4, cudaMemcpyDeviceToHost, ws->stream);
+      if (predecessor_edges) cudaMemcpyAsync(predecessor_edges, d_out + n, n * 4, cudaMemcpyDeviceToHost, ws->stream);
+    }
+    cudaFreeAsync(d_out, ws->stream);
+    BFX_CUDA(le);
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+  });
+}
+
+int bfx_last_launch_count(bfx_workspace* ws, uint64_t* launches) {
+  return bfx::guarded([&] {
+    bfx::require(ws && launches, "null argument");
+    *launches = ws->last_launches;
+  });
+}
+
+int bfx_run_query(bfx_workspace* ws, uint32_t source_count, const uint32_t* sources, uint32_t target_count,
+                  const uint32_t* targets, uint32_t selected_tile_count, const uint32_t* selected_tiles,
+                  const bfx_gpu_run_options* options, bfx_device_run_status* status) {
+  return bfx::guarded([&] {
+    bfx::require(ws && options && status, "null argument");
+    bfx::require(source_count > 0 && target_count > 0, "route queries require sources and targets");
+    bfx::require(sources && targets && selected_tiles && selected_tile_count > 0, "null query array");
+    const auto& tvo = ws->graph->tile_vertex_offsets;
+    const std::uint32_t T = ws->graph->g.T;
+    std::vector<std::uint32_t> masks(T, 0U);
+    std::vector<bfx_batch_vertex_range> ranges(selected_tile_count);
+    for (std::uint32_t i = 0; i < selected_tile_count; ++i) {
+      const std::uint32_t t = selected_tiles[i];
+      if (t >= T) throw std::out_of_range("selected tile out of range");
+      bfx::require(i == 0 || t > selected_tiles[i - 1], "selected tiles must be strictly increasing");
+      masks[t] = 1U;
+      ranges[i] = bfx_batch_vertex_range{tvo[t], tvo[t + 1], 1U};
+    }
+    const std::uint32_t so[2] = {0U, source_count};
+    const std::uint32_t to[2] = {0U, target_count};
+    bfx_batch_description d;
+    std::memset(&d, 0, sizeof(d));
+    d.lane_width = 1;
+    d.valid_lane_mask = 1;
+    d.source_offsets = so;
+    d.sources = sources;
+    d.target_offsets = to;
+    d.targets = targets;
+    d.union_tile_count = selected_tile_count;
+    d.tile_count = T;
+    d.union_tiles = selected_tiles;
+    d.tile_lane_masks = masks.data();
+    d.range_count = selected_tile_count;
+    d.selected_vertex_ranges = ranges.data();
+    int rc = bfx_run_batches(ws, 1, &d, options, status);
+    if (rc != BFX_OK) throw bfx::Error(rc, bfx_last_error());
+  });
+}
+
+}  // extern "C"

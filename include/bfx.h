@@ -1,0 +1,216 @@
+/*
+ * bfx — batched regional shortest paths on NVIDIA B200 (sm_100a).
+ *
+ * C ABI of the product library libbfx.so.  Every entry point returns an int
+ * status (BFX_OK == 0) and never throws; bfx_last_error() gives the calling
+ * thread's last message.  All structs are plain data with fixed layouts; no
+ * C++ or torch types cross this boundary.
+ *
+ * The functions replace the batched relaxation path of the reference engine
+ * (amber-bajaj-1/bf-new).  Each declaration names the reference interface it
+ * stands in for (file:line in the reference repository).
+ */
+#ifndef BFX_H
+#define BFX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BFX_ABI_VERSION 1
+
+/* Status codes (host errors).  Device-side failures are reported through
+ * bfx_device_run_status.error_bits / stop_reason as in the reference. */
+enum {
+  BFX_OK = 0,
+  BFX_ERR_INVALID_ARGUMENT = 1, /* reference: std::invalid_argument */
+  BFX_ERR_OUT_OF_RANGE = 2,     /* reference: std::out_of_range */
+  BFX_ERR_OVERFLOW = 3,         /* reference: std::overflow_error / length_error */
+  BFX_ERR_CUDA = 4,             /* reference: HipRuntimeError (hip/runtime.hpp:22-35) */
+  BFX_ERR_NO_DEVICE = 5,
+  BFX_ERR_STATE = 6,            /* reference: std::logic_error */
+  BFX_ERR_OUT_OF_MEMORY = 7
+};
+
+/* Engine, control and stop enums: same values as include/bfnew/gpu_api.hpp:14-55. */
+enum { BFX_ENGINE_JACOBI_PULL = 0, BFX_ENGINE_DENSE_CHAOTIC_PUSH = 1, BFX_ENGINE_FRONTIER_PUSH = 2,
+       BFX_ENGINE_AUTO = 0xFFFFFFFFu /* bfx extension: the autotuner picks per batch */ };
+enum { BFX_CONTROL_PERSISTENT_COOPERATIVE = 0, BFX_CONTROL_CHUNKED_HOST_POLL = 1,
+       BFX_CONTROL_PER_ROUND_HOST_POLL = 2 };
+enum { BFX_STOP_NONE = 0, BFX_STOP_CONVERGED = 1, BFX_STOP_MAXIMUM_ROUNDS = 2,
+       BFX_STOP_QUEUE_OVERFLOW = 3, BFX_STOP_INVALID_CONTROLLER_STATE = 4,
+       BFX_STOP_DEVICE_FAILURE = 5 };
+enum { BFX_DEVICE_ERROR_QUEUE_OVERFLOW = 1u, BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE = 2u,
+       BFX_DEVICE_ERROR_DEVICE_FAILURE = 4u };
+
+/* Mirrors bfnew::GpuRunOptions (include/bfnew/gpu_api.hpp:57-67), 48 bytes,
+ * validated like validate_gpu_run_options (src/gpu_api.cpp:71-105). */
+typedef struct bfx_gpu_run_options {
+  uint32_t engine;
+  uint32_t control_mode;
+  uint32_t rounds_per_chunk;
+  uint32_t block_size;
+  uint32_t grid_policy;      /* 0 occupancy-derived, 1 fixed blocks per SM */
+  uint32_t blocks_per_wgp;   /* blocks per SM when grid_policy == 1 */
+  uint32_t instrumentation;  /* 0 none, 1 light, 2 debug */
+  uint32_t reserved0;
+  uint64_t maximum_rounds;
+  uint32_t enable_per_lane_convergence;
+  uint32_t reserved1;
+} bfx_gpu_run_options;
+
+/* Mirrors bfnew::DeviceController (gpu_api.hpp:100-120), 96 bytes. */
+typedef struct bfx_device_controller {
+  uint32_t valid_lane_mask, active_lane_mask, changed_lane_mask, converged_lane_mask;
+  uint32_t execute_lane_mask, engine_kind, enable_per_lane_convergence, reserved0;
+  uint64_t rounds_completed, maximum_rounds;
+  uint32_t distance_read_slot, distance_write_slot, frontier_read_slot, frontier_write_slot;
+  uint64_t frontier_size[2];
+  uint32_t next_frontier_lane_mask, done, stop_reason, error_bits;
+} bfx_device_controller;
+
+/* Mirrors bfnew::DeviceRunStatus (gpu_api.hpp:176-187), 48 bytes. */
+typedef struct bfx_device_run_status {
+  uint32_t final_distance_slot;
+  uint32_t converged;
+  uint64_t rounds_completed;
+  uint32_t reached_target_mask;
+  uint32_t bounding_box_miss_mask;
+  uint32_t valid_lane_mask;
+  uint32_t active_lane_mask;
+  uint32_t converged_lane_mask;
+  uint32_t stop_reason;
+  uint32_t error_bits;
+  uint32_t reserved0;
+} bfx_device_run_status;
+
+/* Flattened bfnew::DeviceGraphLayout32 (include/bfnew/device_layout.hpp:72-93)
+ * plus csr_edge_ids, the stable EdgeId of every CSR position
+ * (WeightedGraph::outgoing().edge_ids); NULL derives it from the CSC image.
+ * Host pointers. */
+typedef struct bfx_device_graph_layout32 {
+  uint32_t vertex_count, edge_count, tile_count, csr_run_count, csc_run_count, reserved0;
+  const uint32_t *owner_tiles;                /* [V] */
+  const uint32_t *csr_row_offsets;            /* [V+1] */
+  const uint32_t *csr_destinations;           /* [E] */
+  const float *csr_weights;                   /* [E] */
+  const uint32_t *csr_row_run_offsets;        /* [V+1] */
+  const uint32_t *csr_run_edge_offsets;       /* [csr_run_count+1] */
+  const uint32_t *csr_run_destination_tiles;  /* [csr_run_count] */
+  const uint32_t *csc_column_offsets;         /* [V+1] */
+  const uint32_t *csc_sources;                /* [E] */
+  const float *csc_weights;                   /* [E] */
+  const uint32_t *csc_edge_ids;               /* [E] */
+  const uint32_t *csc_column_run_offsets;     /* [V+1] */
+  const uint32_t *csc_run_edge_offsets;       /* [csc_run_count+1] */
+  const uint32_t *csc_run_source_tiles;       /* [csc_run_count] */
+  const uint32_t *csr_edge_ids;               /* [E] or NULL */
+} bfx_device_graph_layout32;
+
+/* bfnew::BatchVertexRange (batch_layout.hpp:23-29), 12 bytes. */
+typedef struct bfx_batch_vertex_range {
+  uint32_t begin, end, lane_mask;
+} bfx_batch_vertex_range;
+
+/* Flattened bfnew::BatchDeviceDescription (batch_layout.hpp:73-120), the
+ * device-materialized-run-mask representation.  Host pointers. */
+typedef struct bfx_batch_description {
+  uint32_t lane_width;       /* 1, 8, 16 or 32 */
+  uint32_t valid_lane_mask;
+  const uint32_t *source_offsets;  /* [lane_width+1] */
+  const uint32_t *sources;         /* [source_offsets[lane_width]] global vertex ids */
+  const uint32_t *target_offsets;  /* [lane_width+1] */
+  const uint32_t *targets;
+  uint32_t union_tile_count;
+  uint32_t tile_count;             /* == graph tile_count */
+  const uint32_t *union_tiles;     /* [union_tile_count], strictly increasing */
+  const uint32_t *tile_lane_masks; /* [tile_count] dense lane mask per tile */
+  uint32_t range_count;
+  uint32_t reserved0;
+  const bfx_batch_vertex_range *selected_vertex_ranges; /* one per union tile */
+} bfx_batch_description;
+
+typedef struct bfx_resident_graph bfx_resident_graph;
+typedef struct bfx_workspace bfx_workspace;
+
+/* ---- library ---------------------------------------------------------- */
+int bfx_abi_version(void);
+const char *bfx_last_error(void);
+/* Number of CUDA devices visible; 0 without a GPU (never an error). */
+int bfx_device_count(int *count);
+
+/* ---- resident graph ----------------------------------------------------
+ * Replaces bfnew::hip::ResidentDeviceGraph::upload_once_async
+ * (include/bfnew/hip/runtime.hpp:238-270) and its content fingerprint guard.
+ * Uploads the checked 32-bit image once; the graph is immutable afterwards. */
+int bfx_resident_graph_upload(const bfx_device_graph_layout32 *layout, int device,
+                              bfx_resident_graph **out);
+int bfx_resident_graph_destroy(bfx_resident_graph *graph);
+/* Counts {V, E, T, device bytes}. */
+int bfx_resident_graph_info(const bfx_resident_graph *graph, uint64_t out[4]);
+
+/* ---- workspace -----------------------------------------------------------
+ * Replaces bfnew::hip::ReusableBatched{Frontier,Jacobi,Dense}Workspace
+ * (include/bfnew/hip/batched_frontier_workspace.hpp:28-80): device buffers for
+ * terminals, tile tables, labels, activity masks, queues, controllers and
+ * statuses, grown geometrically and reused across calls.  A workspace binds
+ * one graph and one CUDA stream; calls on it must be sequential. */
+int bfx_workspace_create(bfx_resident_graph *graph, bfx_workspace **out);
+int bfx_workspace_destroy(bfx_workspace *ws);
+/* The workspace's cudaStream_t (as void*), for event timing by callers. */
+int bfx_workspace_stream(bfx_workspace *ws, void **stream);
+/* Device bytes currently reserved by the workspace. */
+int bfx_workspace_bytes(bfx_workspace *ws, uint64_t *bytes);
+
+/* ---- batched execution ---------------------------------------------------
+ * bfx_prepare_batches + bfx_execute + bfx_fetch_statuses together replace
+ * BatchedFrontierPushEngine::run_compact_status (hip/batched_frontier_push.hpp:
+ * 105-116) and its Jacobi / dense twins (hip/batched_jacobi.hpp:137-200,
+ * hip/batched_dense_chaotic_push.hpp:105-165), generalised to several batches
+ * in one launch.  options->engine selects the relaxation engine for every
+ * batch (BFX_ENGINE_AUTO: the autotuner picks per batch). */
+
+/* Validates and uploads `count` batch descriptions (host memory) into the
+ * workspace (one H2D transfer).  Replaces workspace.prepare_async
+ * (src/hip/batched_frontier_workspace.hip.cpp:178). */
+int bfx_prepare_batches(bfx_workspace *ws, uint32_t count, const bfx_batch_description *batches);
+/* Runs the prepared batches to convergence (or the round limit) on the
+ * workspace stream.  Asynchronous in persistent mode: returns after enqueue.
+ * Host-poll modes poll the device controller as the reference does. */
+int bfx_execute(bfx_workspace *ws, const bfx_gpu_run_options *options);
+/* Synchronises the stream and copies one status (and optionally the final
+ * controller image) per prepared batch to host memory. */
+int bfx_fetch_statuses(bfx_workspace *ws, bfx_device_run_status *statuses,
+                       bfx_device_controller *controllers);
+/* All three in sequence: the one call a user makes. */
+int bfx_run_batches(bfx_workspace *ws, uint32_t count, const bfx_batch_description *batches,
+                    const bfx_gpu_run_options *options, bfx_device_run_status *statuses);
+
+/* Downloads batch `batch`'s final labels as a graph-sized V*W image (vertex-
+ * major, contiguous lanes; +inf bits / 0xffffffff outside the lane's selected
+ * tiles).  distance_bits: float bit patterns; predecessor_edges: stable EdgeId
+ * of the chosen tight in-edge, 0xffffffff for sources and unreached vertices.
+ * Either output may be NULL.  Replaces run_with_distances
+ * (hip/batched_frontier_push.hpp:122-124). */
+int bfx_download_labels(bfx_workspace *ws, uint32_t batch, uint32_t *distance_bits,
+                        uint32_t *predecessor_edges);
+
+/* Kernels launched by the most recent bfx_execute (its own kernels only). */
+int bfx_last_launch_count(bfx_workspace *ws, uint64_t *launches);
+
+/* ---- plain per-query engine ----------------------------------------------
+ * Replaces GpuSsspEngine::run(RouteQuery, GpuRunOptions) (gpu_api.hpp:203-211)
+ * as implemented by hip::FrontierPushEngine (hip/frontier_push.hpp:47): one
+ * query per launch sequence.  selected_tiles must be strictly increasing. */
+int bfx_run_query(bfx_workspace *ws, uint32_t source_count, const uint32_t *sources,
+                  uint32_t target_count, const uint32_t *targets,
+                  uint32_t selected_tile_count, const uint32_t *selected_tiles,
+                  const bfx_gpu_run_options *options, bfx_device_run_status *status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BFX_H */

@@ -1,0 +1,618 @@
+// Test infrastructure only (never linked into the product): a C ABI over the
+// reference's own CPU library so that pytest can (1) generate golden fixtures,
+// (2) check the product's host layout/batch builders against the reference's
+// builders on the same inputs, and (3) time the reference CPU engine as the
+// cpu_baseline.  Compiled by oracle/Makefile directly from the reference
+// sources; outputs land in oracle/_ref/ only.
+//
+// Reference entry points wrapped here (paths relative to the reference repo):
+//   UniformGridPartitioner::partition          src/tiled_graph.cpp:539
+//   build_tile_run_layout                      src/device_layout.cpp:186
+//   build_device_graph_layout32                src/device_layout.cpp:395
+//   make_route_query / build_induced_query_graph  src/query.cpp:128 / :286
+//   dijkstra_oracle / synchronous_bellman_ford src/cpu/reference_dijkstra.cpp:32,
+//                                              src/cpu/reference_bellman_ford.cpp:14
+//   reconstruct_compact_path_payload           src/compact_paths.cpp:540
+//   make_batch_query_features / make_overlapping_batch_plan  src/batch_plan.cpp:578 / :680
+//   prepare_batch_device_description           src/batch_layout.cpp:1056
+//   run_host_batched_{frontier_push,jacobi_pull,dense_chaotic_push}
+//       src/batched_frontier_push.cpp:648, src/batched_jacobi_pull.cpp:572,
+//       src/batched_dense_chaotic_push.cpp:569
+// Fixture suites are included from the reference's tests/ directory.
+
+#include "bfnew/batch_layout.hpp"
+#include "bfnew/batch_plan.hpp"
+#include "bfnew/batched_dense_chaotic_push.hpp"
+#include "bfnew/batched_frontier_push.hpp"
+#include "bfnew/batched_jacobi_pull.hpp"
+#include "bfnew/compact_paths.hpp"
+#include "bfnew/device_layout.hpp"
+#include "bfnew/graph.hpp"
+#include "bfnew/query.hpp"
+#include "bfnew/selected_region_index.hpp"
+#include "bfnew/spatial.hpp"
+#include "bfnew/sssp.hpp"
+
+#include "batched_frontier_fixture_suite.hpp"
+#include "compact_paths_fixture_suite.hpp"
+#include "dense_fixture_suite.hpp"
+#include "frontier_fixture_suite.hpp"
+#include "graph_fixtures.hpp"
+#include "jacobi_fixture_suite.hpp"
+
+#include <atomic>
+#include <bit>
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <mutex>
+#include <optional>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace bfnew;
+
+namespace {
+
+struct RefCase {
+  std::string name;
+  std::optional<PartitionedGraph> partitioned;
+  TileRunLayout64 runs;
+  DeviceGraphLayout32 layout;
+  std::vector<std::uint32_t> csr_edge_ids;
+  std::vector<RouteQuery> queries;
+  // Optional expectations carried by a reference fixture.
+  std::uint32_t expected_reached{1U};
+  std::uint32_t expected_miss{0U};
+  std::uint32_t four_ulps{0U};
+  // Planning state.
+  std::optional<SelectedRegionIndex> regions;
+  std::vector<BatchQueryFeatures> features;
+  BatchPlan plan;
+};
+
+std::mutex g_mutex;
+std::vector<std::unique_ptr<RefCase>> g_cases;
+thread_local std::string g_error;
+
+RefCase* get(int handle) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (handle < 0 || static_cast<std::size_t>(handle) >= g_cases.size()) {
+    return nullptr;
+  }
+  return g_cases[static_cast<std::size_t>(handle)].get();
+}
+
+int store(std::unique_ptr<RefCase> c) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  g_cases.push_back(std::move(c));
+  return static_cast<int>(g_cases.size() - 1U);
+}
+
+void finish_layout(RefCase& c) {
+  const WeightedGraph& g = c.partitioned->graph;
+  c.runs = build_tile_run_layout(g);
+  c.layout = build_device_graph_layout32(g, c.runs);
+  c.csr_edge_ids.clear();
+  for (const EdgeId e : g.outgoing().edge_ids) {
+    c.csr_edge_ids.push_back(static_cast<std::uint32_t>(e.value()));
+  }
+}
+
+std::unique_ptr<RefCase> from_partitioned(std::string name, PartitionedGraph p) {
+  auto c = std::make_unique<RefCase>();
+  c->name = std::move(name);
+  c->partitioned.emplace(std::move(p));
+  finish_layout(*c);
+  return c;
+}
+
+std::vector<test::JacobiFixtureCase> single_query_suite(const std::string& suite) {
+  if (suite == "jacobi") return test::make_jacobi_fixture_suite();
+  if (suite == "dense") return test::make_dense_fixture_suite();
+  if (suite == "frontier") return test::make_frontier_fixture_suite();
+  return {};
+}
+
+template <typename T>
+void copy_out(T* dst, const std::vector<T>& v) {
+  if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(T));
+}
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return -1;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return g_error.c_str(); }
+
+int ref_case_from_input(
+    std::uint32_t nv, const std::int32_t* xs, const std::int32_t* ys,
+    const std::uint8_t* has_loc, const std::uint16_t* classes,
+    std::uint64_t ne, const std::uint32_t* src, const std::uint32_t* dst,
+    const float* w, const std::uint32_t* pdom, const std::uint32_t* pkind,
+    const std::uint64_t* prec, std::int32_t ox, std::int32_t oy,
+    std::uint32_t tw, std::uint32_t th) {
+  return guarded([&] {
+    std::vector<VertexMetadata> vertices;
+    vertices.reserve(nv);
+    for (std::uint32_t v = 0; v < nv; ++v) {
+      const ResourceClassId cls{classes[v]};
+      vertices.push_back(has_loc[v] ? VertexMetadata::located(xs[v], ys[v], cls)
+                                    : VertexMetadata::unlocated(cls));
+    }
+    std::vector<EdgeInputRecord> edges;
+    edges.reserve(ne);
+    for (std::uint64_t e = 0; e < ne; ++e) {
+      edges.push_back(EdgeInputRecord{
+          VertexId{src[e]}, VertexId{dst[e]}, w[e],
+          PhysicalProvenance{pdom[e], pkind[e], prec[e]}});
+    }
+    InputGraph input{std::move(vertices), std::move(edges)};
+    const UniformGridPartitioner part{SpatialOrderConfig{ox, oy, tw, th}};
+    return store(from_partitioned("input", part.partition(input)));
+  });
+}
+
+int ref_fixture_count(const char* suite_c) {
+  const std::string suite{suite_c};
+  if (suite == "jacobi" || suite == "dense" || suite == "frontier") {
+    return static_cast<int>(single_query_suite(suite).size());
+  }
+  if (suite == "batched_mixed" || suite == "compact_paths" || suite == "core" ||
+      suite == "spatial") {
+    return 1;
+  }
+  return 0;
+}
+
+// Builds reference fixture `index` of `suite` as a case.  Single-query suites
+// carry one query; "batched_mixed" carries the five-lane overlap fixture
+// (tests/batched_jacobi_fixture_suite.hpp:57); "compact_paths" the five
+// compact-path queries (tests/compact_paths_fixture_suite.hpp:45).
+int ref_case_fixture(const char* suite_c, int index) {
+  return guarded([&]() -> int {
+    const std::string suite{suite_c};
+    if (suite == "jacobi" || suite == "dense" || suite == "frontier") {
+      auto cases = single_query_suite(suite);
+      if (index < 0 || static_cast<std::size_t>(index) >= cases.size()) {
+        throw std::out_of_range{"fixture index"};
+      }
+      test::JacobiFixtureCase& fc = cases[static_cast<std::size_t>(index)];
+      auto c = from_partitioned(fc.name, std::move(fc.partitioned));
+      c->queries.push_back(std::move(fc.query));
+      c->expected_reached = fc.expected_reached_mask;
+      c->expected_miss = fc.expected_miss_mask;
+      c->four_ulps = fc.comparison == test::JacobiComparisonPolicy::four_ulps;
+      return store(std::move(c));
+    }
+    if (suite == "batched_mixed") {
+      test::BatchedJacobiFixture f = test::make_mixed_duration_batched_jacobi_fixture();
+      auto c = from_partitioned("batched_mixed", std::move(f.partitioned));
+      c->queries = std::move(f.queries);
+      return store(std::move(c));
+    }
+    if (suite == "compact_paths") {
+      test::CompactPathFixture f = test::make_compact_path_fixture();
+      auto c = from_partitioned("compact_paths", std::move(f.partitioned));
+      c->queries.push_back(std::move(f.cycle_query));
+      c->queries.push_back(std::move(f.tie_query));
+      c->queries.push_back(std::move(f.bounded_query));
+      c->queries.push_back(std::move(f.multisource_query));
+      c->queries.push_back(std::move(f.unreachable_query));
+      return store(std::move(c));
+    }
+    throw std::invalid_argument{"unknown fixture suite"};
+  });
+}
+
+const char* ref_case_name(int h) {
+  RefCase* c = get(h);
+  return c ? c->name.c_str() : "";
+}
+
+void ref_case_free(int h) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (h >= 0 && static_cast<std::size_t>(h) < g_cases.size()) {
+    g_cases[static_cast<std::size_t>(h)].reset();
+  }
+}
+
+// out: V, E, T, csr_runs, csc_runs, queries, expected_reached, expected_miss, four_ulps
+int ref_case_counts(int h, std::uint64_t* out) {
+  RefCase* c = get(h);
+  if (!c) return -1;
+  out[0] = c->layout.vertex_count;
+  out[1] = c->layout.edge_count;
+  out[2] = c->layout.tile_count;
+  out[3] = c->layout.csr_run_destination_tiles.size();
+  out[4] = c->layout.csc_run_source_tiles.size();
+  out[5] = c->queries.size();
+  out[6] = c->expected_reached;
+  out[7] = c->expected_miss;
+  out[8] = c->four_ulps;
+  return 0;
+}
+
+// Exports the reference's DeviceGraphLayout32 plus host-only extras:
+// csr_edge_ids (WeightedGraph::outgoing().edge_ids), new_to_old, the tile
+// coordinate table and tile_vertex_offsets.
+int ref_case_layout(
+    int h, std::uint32_t* owner_tiles,
+    std::uint32_t* csr_row_offsets, std::uint32_t* csr_destinations,
+    float* csr_weights, std::uint32_t* csr_row_run_offsets,
+    std::uint32_t* csr_run_edge_offsets, std::uint32_t* csr_run_destination_tiles,
+    std::uint32_t* csc_column_offsets, std::uint32_t* csc_sources,
+    float* csc_weights, std::uint32_t* csc_edge_ids,
+    std::uint32_t* csc_column_run_offsets, std::uint32_t* csc_run_edge_offsets,
+    std::uint32_t* csc_run_source_tiles, std::uint32_t* csr_edge_ids,
+    std::uint32_t* new_to_old, std::int64_t* tile_xy, std::uint8_t* tile_has_loc,
+    std::uint32_t* tile_vertex_offsets) {
+  RefCase* c = get(h);
+  if (!c) return -1;
+  const DeviceGraphLayout32& L = c->layout;
+  copy_out(owner_tiles, L.owner_tiles);
+  copy_out(csr_row_offsets, L.csr_row_offsets);
+  copy_out(csr_destinations, L.csr_destinations);
+  copy_out(csr_weights, L.csr_weights);
+  copy_out(csr_row_run_offsets, L.csr_row_run_offsets);
+  copy_out(csr_run_edge_offsets, L.csr_run_edge_offsets);
+  copy_out(csr_run_destination_tiles, L.csr_run_destination_tiles);
+  copy_out(csc_column_offsets, L.csc_column_offsets);
+  copy_out(csc_sources, L.csc_sources);
+  copy_out(csc_weights, L.csc_weights);
+  copy_out(csc_edge_ids, L.csc_edge_ids);
+  copy_out(csc_column_run_offsets, L.csc_column_run_offsets);
+  copy_out(csc_run_edge_offsets, L.csc_run_edge_offsets);
+  copy_out(csc_run_source_tiles, L.csc_run_source_tiles);
+  copy_out(csr_edge_ids, c->csr_edge_ids);
+  const WeightedGraph& g = c->partitioned->graph;
+  if (new_to_old) {
+    for (std::size_t i = 0; i < g.new_to_old().size(); ++i) new_to_old[i] = g.new_to_old()[i].value();
+  }
+  const auto tiles = g.tile_coordinates();
+  for (std::size_t t = 0; t < tiles.size(); ++t) {
+    if (tile_xy) {
+      tile_xy[2 * t] = tiles[t].tile_x;
+      tile_xy[2 * t + 1] = tiles[t].tile_y;
+    }
+    if (tile_has_loc) tile_has_loc[t] = tiles[t].has_location ? 1U : 0U;
+  }
+  if (tile_vertex_offsets) {
+    const auto off = g.tile_vertex_offsets();
+    for (std::size_t t = 0; t < off.size(); ++t) tile_vertex_offsets[t] = static_cast<std::uint32_t>(off[t]);
+  }
+  return 0;
+}
+
+// Adds a query with explicitly selected tiles (sorted/deduplicated here), as
+// the reference fixture helper with_exact_selected_tiles does
+// (tests/batched_jacobi_fixture_suite.hpp:34).  n_tiles == 0 selects every
+// tile of the graph (make_full_region_query, tests/jacobi_fixture_suite.hpp:64).
+int ref_query_add(int h, std::uint32_t qid, std::uint32_t ns, const std::uint32_t* srcs,
+                  std::uint32_t nt, const std::uint32_t* tgts, std::uint32_t ntiles,
+                  const std::uint32_t* tiles) {
+  return guarded([&]() -> int {
+    RefCase* c = get(h);
+    if (!c) throw std::invalid_argument{"bad handle"};
+    const WeightedGraph& g = c->partitioned->graph;
+    std::vector<VertexId> s, t;
+    for (std::uint32_t i = 0; i < ns; ++i) s.push_back(VertexId{srcs[i]});
+    for (std::uint32_t i = 0; i < nt; ++i) t.push_back(VertexId{tgts[i]});
+    RouteQuery q = make_route_query(QueryId{qid}, g, s, t, 0U);
+    std::vector<TileId> sel;
+    if (ntiles == 0) {
+      for (std::size_t i = 0; i < g.tile_coordinates().size(); ++i) sel.push_back(TileId{static_cast<std::uint32_t>(i)});
+    } else {
+      for (std::uint32_t i = 0; i < ntiles; ++i) sel.push_back(TileId{tiles[i]});
+    }
+    c->queries.push_back(test::with_exact_selected_tiles(std::move(q), std::move(sel), g));
+    return static_cast<int>(c->queries.size() - 1U);
+  });
+}
+
+// Adds a query whose selected tiles come from make_route_query with padding
+// (src/query.cpp:64-118).
+int ref_query_add_padded(int h, std::uint32_t qid, std::uint32_t ns, const std::uint32_t* srcs,
+                         std::uint32_t nt, const std::uint32_t* tgts, std::uint32_t padding) {
+  return guarded([&]() -> int {
+    RefCase* c = get(h);
+    if (!c) throw std::invalid_argument{"bad handle"};
+    std::vector<VertexId> s, t;
+    for (std::uint32_t i = 0; i < ns; ++i) s.push_back(VertexId{srcs[i]});
+    for (std::uint32_t i = 0; i < nt; ++i) t.push_back(VertexId{tgts[i]});
+    c->queries.push_back(make_route_query(QueryId{qid}, c->partitioned->graph, s, t, padding));
+    return static_cast<int>(c->queries.size() - 1U);
+  });
+}
+
+// out: query_id, n_sources, n_targets, n_selected_tiles
+int ref_query_counts(int h, int q, std::uint32_t* out) {
+  RefCase* c = get(h);
+  if (!c || q < 0 || static_cast<std::size_t>(q) >= c->queries.size()) return -1;
+  const RouteQuery& r = c->queries[static_cast<std::size_t>(q)];
+  out[0] = r.query_id.value();
+  out[1] = static_cast<std::uint32_t>(r.sources.size());
+  out[2] = static_cast<std::uint32_t>(r.targets.size());
+  out[3] = static_cast<std::uint32_t>(r.selected_tiles.size());
+  return 0;
+}
+
+int ref_query_export(int h, int q, std::uint32_t* srcs, std::uint32_t* tgts, std::uint32_t* tiles) {
+  RefCase* c = get(h);
+  if (!c || q < 0 || static_cast<std::size_t>(q) >= c->queries.size()) return -1;
+  const RouteQuery& r = c->queries[static_cast<std::size_t>(q)];
+  for (std::size_t i = 0; i < r.sources.size(); ++i) srcs[i] = r.sources[i].value();
+  for (std::size_t i = 0; i < r.targets.size(); ++i) tgts[i] = r.targets[i].value();
+  for (std::size_t i = 0; i < r.selected_tiles.size(); ++i) tiles[i] = r.selected_tiles[i].value();
+  return 0;
+}
+
+// Bounded Dijkstra on the query's induced graph, mapped back to global ids;
+// vertices outside the selected tiles are +inf.  This is exactly the
+// reference tests' oracle (tests/batched_frontier_push_test.cpp:55).
+int ref_dijkstra(int h, int q, float* dist) {
+  return guarded([&]() -> int {
+    RefCase* c = get(h);
+    if (!c) throw std::invalid_argument{"bad handle"};
+    const WeightedGraph& g = c->partitioned->graph;
+    const RouteQuery& r = c->queries.at(static_cast<std::size_t>(q));
+    const InducedQueryGraph induced = build_induced_query_graph(g, r);
+    const SsspResult res = dijkstra_oracle(induced.graph, induced.sources);
+    for (std::uint32_t v = 0; v < g.vertex_count(); ++v) dist[v] = std::numeric_limits<float>::infinity();
+    for (std::size_t l = 0; l < induced.local_to_global.size(); ++l) {
+      dist[induced.local_to_global[l].value()] = res.distances[l];
+    }
+    return 0;
+  });
+}
+
+// Synchronous Bellman-Ford on the induced graph (same mapping as above).
+int ref_bellman_ford(int h, int q, float* dist) {
+  return guarded([&]() -> int {
+    RefCase* c = get(h);
+    if (!c) throw std::invalid_argument{"bad handle"};
+    const WeightedGraph& g = c->partitioned->graph;
+    const RouteQuery& r = c->queries.at(static_cast<std::size_t>(q));
+    const InducedQueryGraph induced = build_induced_query_graph(g, r);
+    const SsspResult res = synchronous_bellman_ford(induced.graph, induced.sources);
+    for (std::uint32_t v = 0; v < g.vertex_count(); ++v) dist[v] = std::numeric_limits<float>::infinity();
+    for (std::size_t l = 0; l < induced.local_to_global.size(); ++l) {
+      dist[induced.local_to_global[l].value()] = res.distances[l];
+    }
+    return 0;
+  });
+}
+
+// Compact path reconstruction for query q from a graph-sized distance image.
+// Per canonical target i: status[i] (CompactPathStatus), reached[i],
+// path_len[i] (edge count); the concatenated paths go to vertices/edge_ids
+// (vertices: sum(len+1), edge ids: sum(len)) when capacity allows.
+// Returns total edge count, or -1.
+long long ref_compact_paths(int h, int q, const float* dist, std::uint32_t* status,
+                            std::uint32_t* reached, std::uint32_t* path_len,
+                            std::uint32_t* vertices, std::uint64_t vcap,
+                            std::uint32_t* edge_ids, std::uint64_t ecap) {
+  try {
+    RefCase* c = get(h);
+    if (!c) throw std::invalid_argument{"bad handle"};
+    const WeightedGraph& g = c->partitioned->graph;
+    const RouteQuery& r = c->queries.at(static_cast<std::size_t>(q));
+    std::span<const float> d{dist, g.vertex_count()};
+    const CompactPathPayload p = reconstruct_compact_path_payload(g, r, d);
+    std::uint64_t vo = 0, eo = 0;
+    for (std::size_t i = 0; i < p.targets.size(); ++i) {
+      const CompactTargetPath& t = p.targets[i];
+      status[i] = static_cast<std::uint32_t>(t.summary.reconstruction);
+      reached[i] = static_cast<std::uint32_t>(t.summary.reached);
+      path_len[i] = t.summary.path_length;
+      for (const VertexId v : t.vertices) {
+        if (vertices && vo < vcap) vertices[vo] = v.value();
+        ++vo;
+      }
+      for (const EdgeId e : t.edge_ids) {
+        if (edge_ids && eo < ecap) edge_ids[eo] = static_cast<std::uint32_t>(e.value());
+        ++eo;
+      }
+    }
+    return static_cast<long long>(eo);
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return -1;
+  }
+}
+
+// Reference planner over all queries of the case.  Returns batch count.
+int ref_plan(int h, std::uint32_t lane_width, std::uint32_t jn, std::uint32_t jd,
+             std::uint32_t in, std::uint32_t id) {
+  return guarded([&]() -> int {
+    RefCase* c = get(h);
+    if (!c) throw std::invalid_argument{"bad handle"};
+    const WeightedGraph& g = c->partitioned->graph;
+    c->regions.emplace(g, c->runs);
+    c->features = make_batch_query_features(g, *c->regions, c->queries);
+    BatchPlannerPolicy policy;
+    policy.lane_width = lane_width;
+    policy.minimum_jaccard_numerator = jn;
+    policy.minimum_jaccard_denominator = jd;
+    policy.maximum_union_inflation_numerator = in;
+    policy.maximum_union_inflation_denominator = id;
+    c->plan = make_overlapping_batch_plan(*c->regions, c->features, policy);
+    return static_cast<int>(c->plan.batches.size());
+  });
+}
+
+// Plan entry b: out_counts = {lane_width, valid_mask, union_tile_count};
+// query index per lane (0xffffffff = padding); union tiles and lane masks;
+// out_estimates = {union_vertex_count, union_edge_estimate,
+// selected_lane_vertex_count, selected_lane_edge_estimate}.
+int ref_plan_batch(int h, int b, std::uint32_t* out_counts, std::uint32_t* lane_query,
+                   std::uint32_t* union_tiles, std::uint32_t* union_masks,
+                   std::uint64_t* out_estimates) {
+  RefCase* c = get(h);
+  if (!c || b < 0 || static_cast<std::size_t>(b) >= c->plan.batches.size()) return -1;
+  const BatchPlanEntry& e = c->plan.batches[static_cast<std::size_t>(b)];
+  out_counts[0] = e.lane_width;
+  out_counts[1] = e.valid_lane_mask;
+  out_counts[2] = static_cast<std::uint32_t>(e.union_tiles.size());
+  if (lane_query) {
+    for (std::size_t l = 0; l < e.lane_width; ++l) lane_query[l] = e.query_indices_by_lane[l];
+  }
+  if (union_tiles) {
+    for (std::size_t i = 0; i < e.union_tiles.size(); ++i) {
+      union_tiles[i] = e.union_tiles[i].value();
+      union_masks[i] = e.union_tile_lane_masks[i];
+    }
+  }
+  if (out_estimates) {
+    out_estimates[0] = e.union_vertex_count;
+    out_estimates[1] = e.union_edge_estimate;
+    out_estimates[2] = e.selected_lane_vertex_count;
+    out_estimates[3] = e.selected_lane_edge_estimate;
+  }
+  return 0;
+}
+
+std::uint64_t ref_plan_fingerprint(int h) {
+  RefCase* c = get(h);
+  return c ? fingerprint_batch_plan(c->plan) : 0U;
+}
+
+// Prepares the description of plan batch b (device-materialized run masks)
+// and exports: counts {lane_width, valid_mask, n_sources, n_targets,
+// n_union_tiles, n_ranges}; source/target offsets (W+1 each), sources,
+// targets, union tiles, dense tile lane masks (T), ranges (3 per range).
+int ref_describe_batch(int h, int b, std::uint32_t* counts, std::uint32_t* source_offsets,
+                       std::uint32_t* sources, std::uint32_t* target_offsets,
+                       std::uint32_t* targets, std::uint32_t* union_tiles,
+                       std::uint32_t* tile_lane_masks, std::uint32_t* ranges) {
+  return guarded([&]() -> int {
+    RefCase* c = get(h);
+    if (!c) throw std::invalid_argument{"bad handle"};
+    const BatchPlanEntry& e = c->plan.batches.at(static_cast<std::size_t>(b));
+    BatchDeviceDescription d;
+    prepare_batch_device_description(c->partitioned->graph, c->runs, c->queries, c->features, e,
+                                     BatchRunRepresentation::device_materialized_run_masks, d);
+    counts[0] = d.lane_width;
+    counts[1] = d.valid_lane_mask;
+    counts[2] = static_cast<std::uint32_t>(d.sources.size());
+    counts[3] = static_cast<std::uint32_t>(d.targets.size());
+    counts[4] = static_cast<std::uint32_t>(d.union_tiles.size());
+    counts[5] = static_cast<std::uint32_t>(d.selected_vertex_ranges.size());
+    copy_out(source_offsets, d.source_offsets);
+    copy_out(sources, d.sources);
+    copy_out(target_offsets, d.target_offsets);
+    copy_out(targets, d.targets);
+    copy_out(union_tiles, d.union_tiles);
+    copy_out(tile_lane_masks, d.tile_lane_masks);
+    if (ranges) {
+      for (std::size_t i = 0; i < d.selected_vertex_ranges.size(); ++i) {
+        ranges[3 * i] = d.selected_vertex_ranges[i].begin;
+        ranges[3 * i + 1] = d.selected_vertex_ranges[i].end;
+        ranges[3 * i + 2] = d.selected_vertex_ranges[i].lane_mask;
+      }
+    }
+    return 0;
+  });
+}
+
+// Runs a reference portable batched engine (engine 0 Jacobi, 1 dense,
+// 2 frontier) on plan batch b, persistent control, unlimited rounds.
+// distance_bits: V*W words (vertex-major, contiguous lanes); status: the 48-byte
+// DeviceRunStatus image.
+int ref_run_batched(int h, int b, int engine, std::uint64_t max_rounds,
+                    std::uint32_t* distance_bits, void* status48) {
+  return guarded([&]() -> int {
+    RefCase* c = get(h);
+    if (!c) throw std::invalid_argument{"bad handle"};
+    const BatchPlanEntry& e = c->plan.batches.at(static_cast<std::size_t>(b));
+    BatchDeviceDescription d;
+    prepare_batch_device_description(c->partitioned->graph, c->runs, c->queries, c->features, e,
+                                     BatchRunRepresentation::retained_per_run_masks, d);
+    GpuRunOptions o;
+    o.engine = static_cast<EngineKind>(engine);
+    o.control_mode = ControlMode::persistent_cooperative;
+    o.maximum_rounds = max_rounds;
+    DeviceRunStatus st{};
+    std::vector<std::uint32_t> bits;
+    if (engine == 2) {
+      const auto r = run_host_batched_frontier_push(c->layout, c->queries, e, d, o);
+      st = r.result.status;
+      bits = r.distance_bits;
+    } else if (engine == 1) {
+      const auto r = run_host_batched_dense_chaotic_push(c->layout, c->queries, e, d, o);
+      st = r.result.status;
+      bits = r.distance_bits;
+    } else {
+      const auto r = run_host_batched_jacobi_pull(c->layout, c->queries, e, d, o);
+      st = r.result.status;
+      for (const float f : r.final_distances) bits.push_back(std::bit_cast<std::uint32_t>(f));
+    }
+    copy_out(distance_bits, bits);
+    std::memcpy(status48, &st, sizeof(st));
+    return 0;
+  });
+}
+
+// CPU baseline: bounded Dijkstra (induced graph build + dijkstra_oracle) for
+// the listed queries, one query at a time per host thread over `threads`
+// threads.  Returns wall seconds for the whole set; induced_seconds receives
+// the summed per-thread induced-graph build time (excluded from the SSSP
+// figure by the caller), and edges_out the summed induced edge counts.
+double ref_time_dijkstra(int h, std::uint32_t nq, const std::uint32_t* qidx,
+                         std::uint32_t threads, double* induced_seconds,
+                         double* sssp_seconds, std::uint64_t* edges_out) {
+  RefCase* c = get(h);
+  if (!c) return -1.0;
+  const WeightedGraph& g = c->partitioned->graph;
+  std::atomic<std::uint32_t> next{0U};
+  std::vector<double> ind(threads, 0.0), ss(threads, 0.0);
+  std::vector<std::uint64_t> edges(threads, 0U);
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> pool;
+  for (std::uint32_t t = 0; t < threads; ++t) {
+    pool.emplace_back([&, t] {
+      for (;;) {
+        const std::uint32_t i = next.fetch_add(1U);
+        if (i >= nq) break;
+        const RouteQuery& r = c->queries[qidx[i]];
+        const auto a = std::chrono::steady_clock::now();
+        const InducedQueryGraph induced = build_induced_query_graph(g, r);
+        const auto b = std::chrono::steady_clock::now();
+        const SsspResult res = dijkstra_oracle(induced.graph, induced.sources);
+        const auto e = std::chrono::steady_clock::now();
+        ind[t] += std::chrono::duration<double>(b - a).count();
+        ss[t] += std::chrono::duration<double>(e - b).count();
+        edges[t] += induced.graph.edge_count();
+        (void)res;
+      }
+    });
+  }
+  for (auto& th : pool) th.join();
+  const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  double si = 0, sd = 0;
+  std::uint64_t se = 0;
+  for (std::uint32_t t = 0; t < threads; ++t) {
+    si += ind[t];
+    sd += ss[t];
+    se += edges[t];
+  }
+  if (induced_seconds) *induced_seconds = si;
+  if (sssp_seconds) *sssp_seconds = sd;
+  if (edges_out) *edges_out = se;
+  return wall;
+}
+
+}  // extern "C"

@@ -1,0 +1,183 @@
+"""GPU parity: the sm_100a engines in libbfx.so against the oracle and the
+reference's golden vectors.  Distances and predecessors must be bit-exact;
+statuses must match the reference semantics (reached / miss lanes,
+convergence, stop reason)."""
+import numpy as np
+import pytest
+
+import bfx
+from bfx import workloads
+from golden_cases import GOLDEN, fixture_paths, load_case
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+ENGINES = [bfx.ENGINE_FRONTIER_PUSH, bfx.ENGINE_JACOBI_PULL, bfx.ENGINE_DENSE_CHAOTIC_PUSH]
+ENGINE_CLASS = {bfx.ENGINE_FRONTIER_PUSH: bfx.BatchedFrontierPushEngine,
+                bfx.ENGINE_JACOBI_PULL: bfx.BatchedJacobiPullEngine,
+                bfx.ENGINE_DENSE_CHAOTIC_PUSH: bfx.BatchedDenseChaoticPushEngine}
+
+
+def check_batches(layout, descs, lane_queries, statuses, labels, orc, golden_dist=None):
+    """Every valid lane of every batch equals the oracle bit for bit."""
+    for b, d in enumerate(descs):
+        bits, pred = labels[b]
+        st = statuses[b]
+        assert st.stop_reason == bfx.STOP_CONVERGED, st.as_dict()
+        assert st.converged == 1 and st.error_bits == 0
+        reached = 0
+        for lane in range(d.lane_width):
+            if not (d.valid_lane_mask >> lane) & 1:
+                assert np.all(bits[:, lane] == bfx.INF_BITS)
+                continue
+            q = lane_queries[b][lane]
+            od, op = orc.region_sssp(q.sources, q.targets, q.selected_tiles)
+            np.testing.assert_array_equal(bits[:, lane], od, err_msg=f"batch {b} lane {lane} distances")
+            np.testing.assert_array_equal(pred[:, lane], op, err_msg=f"batch {b} lane {lane} predecessors")
+            if golden_dist is not None:
+                np.testing.assert_array_equal(bits[:, lane], golden_dist[q.query_id])
+            if np.all(od[q.targets] != bfx.INF_BITS):
+                reached |= 1 << lane
+        assert st.reached_target_mask == reached
+        assert st.bounding_box_miss_mask == d.valid_lane_mask & ~reached
+        assert st.valid_lane_mask == d.valid_lane_mask
+        assert st.converged_lane_mask == d.valid_lane_mask and st.active_lane_mask == 0
+
+
+def run(layout, descs, engine, control=bfx.CONTROL_PERSISTENT, **kw):
+    res = bfx.ResidentDeviceGraph.upload_once(layout)
+    ws = bfx.Workspace(res)
+    eng = ENGINE_CLASS[engine](res, ws)
+    opts = bfx.GpuRunOptions(control_mode=control, **kw)
+    st, labels = eng.run_with_distances(descs, opts)
+    launches = ws.last_launch_count()
+    ws.close()
+    res.close()
+    return st, labels, launches
+
+
+@pytest.mark.parametrize("path", fixture_paths(), ids=lambda p: p.stem)
+@pytest.mark.parametrize("engine", ENGINES, ids=["frontier", "jacobi", "dense"])
+def test_reference_fixtures_single_lane(gpu, path, engine):
+    case = load_case(path)
+    orc = Oracle.from_layout(case.layout)
+    descs = [bfx.make_description(case.layout, [gq.query], 1) for gq in case.queries]
+    lanes = [[gq.query] for gq in case.queries]
+    golden = {gq.query.query_id: gq.dist for gq in case.queries}
+    st, labels, _ = run(case.layout, descs, engine)
+    check_batches(case.layout, descs, lanes, st, labels, orc, golden)
+    if case.name != "compact_paths" and len(case.queries) == 1:
+        assert st[0].reached_target_mask == case.expected_reached
+        assert st[0].bounding_box_miss_mask == case.expected_miss
+
+
+@pytest.mark.parametrize("engine", ENGINES, ids=["frontier", "jacobi", "dense"])
+@pytest.mark.parametrize("control", [bfx.CONTROL_PERSISTENT, bfx.CONTROL_CHUNKED, bfx.CONTROL_PER_ROUND],
+                         ids=["persistent", "chunked", "per_round"])
+def test_batched_mixed_fixture_matches_reference_engines(gpu, engine, control):
+    """The five-lane overlap fixture (tests/batched_jacobi_fixture_suite.hpp:57):
+    our plan equals the reference plan and our labels equal the reference's
+    portable batched engines' labels, in every control mode."""
+    z = dict(np.load(GOLDEN / "batched_mixed.npz"))
+    case = load_case(GOLDEN / "batched_mixed.npz")
+    queries = [gq.query for gq in case.queries]
+    plan = bfx.make_overlapping_batch_plan(case.layout, queries, bfx.BatchPlannerPolicy(8, 0, 1, 4, 1))
+    assert plan.batch_count == int(z["batch_count"]) == 1
+    d = plan.descriptions()[0]
+    np.testing.assert_array_equal(d.query_index_by_lane, z["B0_lane_query"])
+    np.testing.assert_array_equal(d.union_tiles, z["B0_union_tiles"])
+    st, labels, _ = run(case.layout, [d], engine, control, rounds_per_chunk=2)
+    bits, _ = labels[0]
+    for eng in (0, 1, 2):
+        ref_bits = z[f"B0_E{eng}_bits"]
+        np.testing.assert_array_equal(bits, ref_bits)
+        ref_st = z[f"B0_E{eng}_status"]
+        assert st[0].converged == ref_st[0]
+        assert st[0].reached_target_mask == ref_st[1]
+        assert st[0].bounding_box_miss_mask == ref_st[2]
+        assert st[0].valid_lane_mask == ref_st[3]
+        assert st[0].stop_reason == ref_st[6] and st[0].error_bits == ref_st[7]
+    lanes = [[queries[i] if i != bfx.NO_EDGE else None for i in d.query_index_by_lane]]
+    check_batches(case.layout, [d], lanes, st, labels, Oracle.from_layout(case.layout))
+
+
+@pytest.fixture(scope="module")
+def c1():
+    return workloads.make_workload("c1")
+
+
+@pytest.mark.parametrize("engine", ENGINES, ids=["frontier", "jacobi", "dense"])
+def test_c1_full_graph_batch_bit_exact(gpu, c1, engine):
+    """c1: 8 full-graph sources in one width-8 batch; uint costs."""
+    d = bfx.make_description(c1.layout, c1.queries, 8)
+    st, labels, launches = run(c1.layout, [d], engine)
+    check_batches(c1.layout, [d], [c1.queries], st, labels, Oracle.from_layout(c1.layout))
+    assert launches >= 3
+
+
+@pytest.mark.parametrize("engine", ENGINES, ids=["frontier", "jacobi", "dense"])
+def test_regional_multi_batch_one_launch(gpu, engine):
+    """Uneven regional queries planned into several batches of different
+    widths and relaxed in one launch (c2 recipe on a 32x32-tile grid)."""
+    layout, grid = workloads.build_graph("c2", scale_tiles=(32, 32))
+    qs = workloads.box_queries(layout, grid, 48, 2, 16, seed=9)
+    plan = workloads.plan_batches(layout, qs, 32, narrow=True,
+                                  policy=bfx.BatchPlannerPolicy(32, 0, 1, 8, 1, narrow_lanes=True))
+    descs = plan.descriptions()
+    assert len(descs) >= 2
+    lanes = [[qs[i] if i != bfx.NO_EDGE else None for i in d.query_index_by_lane] for d in descs]
+    st, labels, _ = run(layout, descs, engine)
+    check_batches(layout, descs, lanes, st, labels, Oracle.from_layout(layout))
+
+
+def test_plain_per_query_engine_matches(gpu, c1):
+    """bfx_run_query (the plain one-query-per-launch engine) on c1 queries."""
+    res = bfx.ResidentDeviceGraph.upload_once(c1.layout)
+    ws = bfx.Workspace(res)
+    orc = Oracle.from_layout(c1.layout)
+    for q in c1.queries[:3]:
+        st = ws.run_query(q.sources, q.targets, q.selected_tiles, bfx.GpuRunOptions())
+        bits, pred = ws.download_labels(0, 1)
+        od, op = orc.region_sssp(q.sources, q.targets, q.selected_tiles)
+        np.testing.assert_array_equal(bits[:, 0], od)
+        np.testing.assert_array_equal(pred[:, 0], op)
+        assert st.converged == 1 and st.reached_target_mask == 1
+    ws.close()
+    res.close()
+
+
+@pytest.mark.parametrize("engine", ENGINES, ids=["frontier", "jacobi", "dense"])
+def test_round_limit_stops_without_result_masks(gpu, c1, engine):
+    """maximum_rounds reached: not converged, no reached/miss bits
+    (make_frontier_run_status, include/bfnew/frontier_push.hpp:270-294)."""
+    d = bfx.make_description(c1.layout, c1.queries, 8)
+    res = bfx.ResidentDeviceGraph.upload_once(c1.layout)
+    ws = bfx.Workspace(res)
+    eng = ENGINE_CLASS[engine](res, ws)
+    st, ctl = eng.run_status_only([d], bfx.GpuRunOptions(maximum_rounds=2))
+    s = st[0]
+    assert s.stop_reason == bfx.STOP_MAXIMUM_ROUNDS and s.converged == 0
+    assert s.reached_target_mask == 0 and s.bounding_box_miss_mask == 0
+    assert s.rounds_completed == 2
+    assert s.active_lane_mask != 0 and (s.active_lane_mask & ~d.valid_lane_mask) == 0
+    assert ctl[0].done == 1 and ctl[0].stop_reason == bfx.STOP_MAXIMUM_ROUNDS
+    ws.close()
+    res.close()
+
+
+def test_invalid_options_and_descriptions_rejected(gpu, c1):
+    res = bfx.ResidentDeviceGraph.upload_once(c1.layout)
+    ws = bfx.Workspace(res)
+    d = bfx.make_description(c1.layout, c1.queries, 8)
+    eng = bfx.BatchedFrontierPushEngine(res, ws)
+    with pytest.raises(ValueError):
+        eng.run_compact_status([d], bfx.GpuRunOptions(maximum_rounds=0))
+    with pytest.raises(ValueError):
+        eng.run_compact_status([d], bfx.GpuRunOptions(block_size=100))
+    bad = bfx.make_description(c1.layout, c1.queries, 8)
+    bad.tile_lane_masks = bad.tile_lane_masks.copy()
+    bad.tile_lane_masks[bad.union_tiles[0]] ^= 1
+    with pytest.raises(ValueError):
+        eng.run_compact_status([bad], bfx.GpuRunOptions())
+    ws.close()
+    res.close()
