@@ -1,0 +1,356 @@
+"""Benchmark: batched regional SSSP on B200 (queries/s, GTEPS, HBM roofline).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bfx|reference]
+
+Workload (default c2): 128x128 tiles x 128 nodes (2,097,152 vertices,
+16,777,216 edges), float costs base(span) * lognormal(0, 0.5); 256 regional
+queries with box sides U[4,64] tiles, one source and one target each; the
+planner groups overlapping queries into batches (narrowed to 1/8/16/32
+lanes) and one persistent cooperative launch relaxes all of them.
+
+A step is one pass of the hot path over the whole query set: labels reset,
+seeded, relaxed to convergence, targets classified.  `value` times the steps
+with inputs resident in HBM (device events on the launching stream);
+`e2e.value` times the same steps through the C ABI from host buffers
+(descriptions H2D from pinned staging, statuses D2H).  Inputs (graph 0.5 GB
++ labels) exceed the 126 MB L2, so no flush is needed between steps.
+
+Multi-GPU (torchrun): replicas -- each rank holds the graph and relaxes its
+own query set (weak scaling, no data-path collective); only the timing
+max-reduction uses torch.distributed.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+for _p in (REPO, REPO / "bf-new_b200"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+import numpy as np  # noqa: E402
+
+METRIC = "batched SSSP queries/s (256 uneven regional queries, 2.1M V / 16.8M E, one persistent launch)"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                           "--format=csv,noheader,nounits", "-lms", "200"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except FileNotFoundError:
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+
+    def summary(self) -> dict:
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def cpu_reference_baseline(graph_input, order, queries, sample: int, threads: int):
+    """The reference's own CPU engine (oracle/_ref: dijkstra_oracle on each
+    query's induced graph, one query per host thread) on a bounded sample."""
+    from oracle.oracle import Ref
+    if not Ref.available():
+        return None
+    ref = Ref()
+    t0 = time.time()
+    h = ref.case_from_input(graph_input, order)
+    build_s = time.time() - t0
+    idx = []
+    for q in queries[:sample]:
+        idx.append(ref.query_add(h, q.query_id, q.sources, q.targets, q.selected_tiles))
+    r = ref.time_dijkstra(h, idx, threads)
+    ref.free(h)
+    return {"value": sample / r["wall_s"], "unit": "queries/s", "cores": threads, "kind": "reference",
+            "sample": f"first {sample} of the {len(queries)} queries, reference dijkstra_oracle on each induced "
+                      f"graph, one query per thread ({r['induced_s']:.2f} s induced-graph build excluded)",
+            "wall_s": r["wall_s"], "gteps": r["edges"] / max(r["sssp_s"] / threads, 1e-9) / 1e9 / 1.0,
+            "graph_build_s": build_s}
+
+
+def cpu_port_baseline(layout, queries, sample: int, threads: int):
+    """Fallback when the reference build is absent: the oracle's C restatement."""
+    from oracle.oracle import Oracle
+    orc = Oracle.from_layout(layout)
+    t0 = time.time()
+    orc.region_sssp_many(queries[:sample], threads)
+    wall = time.time() - t0
+    return {"value": sample / wall, "unit": "queries/s", "cores": threads, "kind": "port",
+            "sample": f"first {sample} of {len(queries)} queries, oracle bounded Dijkstra, one query per thread",
+            "wall_s": wall}
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import bfx
+    from bfx import workloads
+    g, order, _ = bfx.synth_graph(**workloads.GRAPHS["c2"])
+    layout = bfx.build_device_graph_layout(g, order)
+    grid = (128, 128)
+    queries = workloads.box_queries(layout, grid, 256, 4, 64, 202)
+    threads = os.cpu_count() or 1
+    from oracle.oracle import Ref
+    if not Ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU library (oracle/_ref) was not built"}))
+        return
+    ref = Ref()
+    h = ref.case_from_input(g, order)
+    idx = [ref.query_add(h, q.query_id, q.sources, q.targets, q.selected_tiles) for q in queries]
+    sample = 64
+    for _ in range(args.warmup):
+        ref.time_dijkstra(h, idx[:8], threads)
+    walls = []
+    for s in range(args.steps):
+        part = [idx[(s * sample + i) % len(idx)] for i in range(sample)]
+        walls.append(ref.time_dijkstra(h, part, threads)["wall_s"])
+    total = sum(walls)
+    v = sample * args.steps / total
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "c2: 256 regional queries on 128x128x128 tiles (2.1M V, 16.8M E), f32 lognormal "
+                                   "costs; each step a bounded sample of 64 of those queries"},
+            "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "reference",
+                             "sample": "64 queries per step, reference dijkstra_oracle on induced graphs"},
+            "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="bfx", choices=["bfx", "reference"])
+    ap.add_argument("--engine", default="frontier", choices=["frontier", "jacobi", "dense"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--queries", type=int, default=256)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    rank, world, local = dist_env()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = tdist
+
+    import bfx
+    from bfx import workloads
+
+    t0 = time.time()
+    g, order, gstats = bfx.synth_graph(**workloads.GRAPHS["c2"])
+    layout = bfx.build_device_graph_layout(g, order)
+    grid = (128, 128)
+    queries = workloads.box_queries(layout, grid, args.queries, 4, 64, 202 + 1000 * rank)
+    t1 = time.time()
+    policy = bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True)
+    plan = bfx.make_overlapping_batch_plan(layout, queries, policy)
+    descs = plan.descriptions()
+    t2 = time.time()
+    lane_edges = sum(e[3] for e in plan.estimates)
+    log(f"[bench] graph+layout {t1 - t0:.1f}s plan {t2 - t1:.1f}s: {plan.batch_count} batches, "
+        f"widths {sorted({d.lane_width for d in descs})}, sum selected edges {lane_edges:,}")
+
+    device = local if world > 1 else 0
+    resident = bfx.ResidentDeviceGraph.upload_once(layout, device)
+    ws = bfx.Workspace(resident)
+    engine_id = {"frontier": bfx.ENGINE_FRONTIER_PUSH, "jacobi": bfx.ENGINE_JACOBI_PULL,
+                 "dense": bfx.ENGINE_DENSE_CHAOTIC_PUSH}[args.engine]
+    opts = bfx.GpuRunOptions(engine=engine_id)
+    opts_instr = bfx.GpuRunOptions(engine=engine_id, instrumentation=1)
+
+    import torch
+    torch.cuda.set_device(device)
+    stream = torch.cuda.ExternalStream(ws.stream, device=device)
+
+    def barrier():
+        torch.cuda.synchronize(device)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- instrumented pass (untimed): algorithmic work counts + parity spot check
+    ws.prepare(descs)
+    ws.execute(opts_instr)
+    statuses = ws.fetch_statuses()
+    work = ws.work_counters()
+    assert all(s.stop_reason == bfx.STOP_CONVERGED for s in statuses), "benchmark run did not converge"
+    reached = sum(bin(s.reached_target_mask).count("1") for s in statuses)
+
+    # ---- device-resident timing (value)
+    for _ in range(args.warmup):
+        ws.execute(opts)
+    barrier()
+    kernel_ms = []
+    with ClockSampler(device) as clocks:
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(args.steps):
+            ws.execute(opts)
+            kernel_ms.append(ws.last_execute_timing()[0])
+        end.record(stream)
+        barrier()
+    dev_ms = start.elapsed_time(end)
+    launches_per_step = ws.last_launch_count()
+    dev_ms = max_over_ranks(dev_ms)
+    statuses = ws.fetch_statuses()
+    assert all(s.stop_reason == bfx.STOP_CONVERGED for s in statuses)
+
+    # ---- end-to-end timing through the C ABI from host buffers (e2e)
+    for _ in range(args.warmup):
+        ws.prepare(descs)
+        ws.execute(opts)
+        ws.fetch_statuses()
+    barrier()
+    s2 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(args.steps):
+        ws.prepare(descs)
+        ws.execute(opts)
+        ws.fetch_statuses()
+    e2.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(s2.elapsed_time(e2))
+    h2d, d2h = ws.transfer_bytes()
+
+    # ---- plain per-query engine (one query per launch sequence) on a sample
+    sample_q = queries[:64]
+    barrier()
+    s3 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    s3.record(stream)
+    for q in sample_q:
+        ws.run_query(q.sources, q.targets, q.selected_tiles, opts)
+    e3.record(stream)
+    barrier()
+    plain_ms = s3.elapsed_time(e3)
+    plain_qps = len(sample_q) / (plain_ms / 1000)
+
+    nq = len(queries) * world
+    ms_per_step = dev_ms / args.steps
+    value = nq / (ms_per_step / 1000)
+    e2e_value = nq / (e2e_ms / args.steps / 1000)
+    kernel_avg = float(np.mean(kernel_ms))
+    F, S, Pp, L, N = (work[k] for k in ("entries", "records", "active_pairs", "relaxations", "claims"))
+    alg_bytes = 16 * F + 12 * S + 8 * Pp + 16 * L + 8 * N
+    peaks_path = REPO / "MEASURED_PEAKS.json"
+    if peaks_path.exists():
+        peak = json.loads(peaks_path.read_text())["hbm_gbs"]
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = alg_bytes / (kernel_avg / 1000) / 1e9
+    traffic = None
+    tpath = REPO / "profiles" / "frontier_push_c2_traffic.txt"
+    if tpath.exists():
+        for line in tpath.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch:"):
+                traffic = int(float(line.split(":")[1]))
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "c2: 256 uneven regional queries (box side U[4,64] tiles) on 128x128 tiles x 128 "
+                               "nodes, 2,097,152 V / 16,777,216 E, f32 lognormal costs",
+                   "queries_per_gpu": len(queries), "batches": plan.batch_count,
+                   "lane_widths": sorted({d.lane_width for d in descs}), "engine": args.engine,
+                   "control": "persistent_cooperative", "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (graph 0.54 GB + labels), no flush"},
+        "gteps": lane_edges * world / (ms_per_step / 1000) / 1e9,
+        "reached_lanes": reached,
+        "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "plain_per_query": {"value": plain_qps, "unit": "queries/s", "sample": len(sample_q),
+                            "batched_speedup": value / world / plain_qps},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_src, "kernel": "persistent_kernel<false> (frontier)",
+                     "kernel_ms": kernel_avg, "algorithmic_bytes_per_launch": alg_bytes, "work": work},
+        "clocks": clocks.summary(),
+        "gpu_launches": launches_per_step * args.steps,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        try:
+            cb = cpu_reference_baseline(g, order, queries, 32, threads)
+        except Exception as exc:  # reference build unusable here
+            log(f"[bench] reference baseline failed: {exc}")
+            cb = None
+        line["cpu_baseline"] = cb or cpu_port_baseline(layout, queries, 32, threads)
+    if rank == 0:
+        print(json.dumps(line))
+    ws.close()
+    resident.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

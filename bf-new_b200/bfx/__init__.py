@@ -530,6 +530,25 @@ class Workspace:
         _check(load().bfx_last_launch_count(self._h, C.byref(n)))
         return n.value
 
+    def last_execute_timing(self) -> tuple[float, float]:
+        """(relaxation kernels ms, whole execute ms) from the library's CUDA events."""
+        out = (f32 * 2)()
+        _check(load().bfx_last_execute_timing(self._h, out))
+        return float(out[0]), float(out[1])
+
+    def transfer_bytes(self) -> tuple[int, int]:
+        out = (u64 * 2)()
+        _check(load().bfx_workspace_transfer_bytes(self._h, out))
+        return int(out[0]), int(out[1])
+
+    WORK_KEYS = ("entries", "records", "active_pairs", "relaxations", "claims", "decreases", "min_reductions",
+                 "rounds")
+
+    def work_counters(self) -> dict:
+        out = (u64 * 8)()
+        _check(load().bfx_fetch_work_statistics(self._h, None, out))
+        return dict(zip(self.WORK_KEYS, (int(x) for x in out)))
+
     def run_query(self, sources, targets, selected_tiles, options: GpuRunOptions) -> DeviceRunStatus:
         s = np.ascontiguousarray(np.unique(np.asarray(sources, np.uint32)))
         t = np.ascontiguousarray(np.unique(np.asarray(targets, np.uint32)))

@@ -104,6 +104,18 @@ struct DRun {
   u32 abort;       // device failure seen
   u64 max_rounds;
   u64 launches;
+  u64 work[8];     // launch-wide work counters (instrumented runs)
+};
+
+// Work counters of an instrumented run (instrumentation >= 1):
+// 0 queue entries processed, 1 edge records read, 2 active (vertex, lane)
+// source reads, 3 lane-edge relaxations, 4 queue claims, 5 distance
+// decreases, 6 min-reductions issued, 7 rounds executed.
+struct Work {
+  u64 c[7];
+  __device__ void zero() {
+    for (int i = 0; i < 7; ++i) c[i] = 0;
+  }
 };
 
 constexpr u32 kMaxBatchesPerLaunch = 4096;
@@ -254,6 +266,7 @@ __global__ void init_kernel(LaunchParams p) {
     p.run->done = 0u;
     p.run->stop = 0u;
     p.run->abort = 0u;
+    for (int i = 0; i < 8; ++i) p.run->work[i] = 0u;
   }
 }
 
@@ -295,8 +308,9 @@ __global__ void seed_kernel(LaunchParams p, const u32* src_base) {
 // Frontier push: one warp per (batch, vertex) queue entry.
 // ---------------------------------------------------------------------------
 
+template <bool kCount>
 __device__ __forceinline__ void frontier_entry(const LaunchParams& p, const DBatch& B, DCtl& C, u32 v, u32 rd,
-                                               u32 widx) {
+                                               u32 widx, Work& wk) {
   const u32 lane = lane_id();
   const u32 st = __ldg(p.g.owner + v);
   const uint2 sti = B.tiles[st];
@@ -306,6 +320,12 @@ __device__ __forceinline__ void frontier_entry(const LaunchParams& p, const DBat
   m = __shfl_sync(0xFFFFFFFFu, m, 0) & sti.x;
   if (m == 0u) return;
   const u32 k = __popc(m);
+  const u32 rb = __ldg(p.g.csr_off + v), re = __ldg(p.g.csr_off + v + 1);
+  if (kCount && lane == 0) {
+    wk.c[0] += 1;
+    wk.c[1] += re - rb;
+    wk.c[2] += k;
+  }
   const u32 s = k <= 1u ? 0u : 32u - __clz(k - 1u);  // group = 2^s lanes per edge
   const u32 kp = 1u << s;
   const u32 slot = lane >> s;
@@ -321,7 +341,6 @@ __device__ __forceinline__ void frontier_entry(const LaunchParams& p, const DBat
   }
   u32* const mask_w = B.mask[rd ^ 1u];
   u32* const queue_w = B.queue[rd ^ 1u];
-  const u32 rb = __ldg(p.g.csr_off + v), re = __ldg(p.g.csr_off + v + 1);
   for (u32 base = rb; base < re; base += G) {
     const u32 e = base + slot;
     u32 bits = 0u, cdst = 0u, dstv = 0u;
@@ -334,9 +353,14 @@ __device__ __forceinline__ void frontier_entry(const LaunchParams& p, const DBat
         const u64 cand = dev::candidate(src_bits, rec.y, rec.z);
         u64* const target = B.dist[0] + ((static_cast<u64>(cdst) << B.shift) + ql);
         const u64 cur = dev::ld_cg(target);
+        if (kCount) wk.c[3] += 1;
         if (cand < cur) {
           dev::red_min(target, cand);
           if (dev::hi(cand) < dev::hi(cur)) bits = 1u << ql;
+          if (kCount) {
+            wk.c[6] += 1;
+            wk.c[5] += bits != 0u;
+          }
         }
       }
     }
@@ -353,6 +377,7 @@ __device__ __forceinline__ void frontier_entry(const LaunchParams& p, const DBat
       if (lane == leader) pos = atomicAdd(&C.count[widx], static_cast<u32>(__popc(cm)));
       pos = __shfl_sync(0xFFFFFFFFu, pos, static_cast<int>(leader));
       if (claim) {
+        if (kCount) wk.c[4] += 1;
         const u32 at = pos + __popc(cm & ((1u << lane) - 1u));
         if (at < B.U) {
           queue_w[at] = dstv;
@@ -369,8 +394,9 @@ __device__ __forceinline__ void frontier_entry(const LaunchParams& p, const DBat
 // d_next[v,l] = min(d[v,l], min over admitted in-edges of d[u,l] + w).
 // ---------------------------------------------------------------------------
 
+template <bool kCount>
 __device__ __forceinline__ void jacobi_item(const LaunchParams& p, const DBatch& B, DCtl& C, u32 item, u32 r,
-                                            u32 widx) {
+                                            u32 widx, Work& wk) {
   const u32 lane = lane_id();
   const u32 sub = lane >> B.shift;
   const u32 ql = lane & (B.W - 1u);
@@ -387,6 +413,11 @@ __device__ __forceinline__ void jacobi_item(const LaunchParams& p, const DBatch&
     u64 best = old;
     if ((vt.x >> ql) & 1u) {
       const u32 cb = __ldg(p.g.csc_off + v), ce = __ldg(p.g.csc_off + v + 1);
+      if (kCount) {
+        wk.c[0] += 1;
+        wk.c[1] += ce - cb;
+        wk.c[2] += 1;
+      }
       for (u32 e = cb; e < ce; ++e) {
         const uint4 rec = __ldg(p.g.csc + e);
         const uint2 su = B.tiles[rec.w];
@@ -395,10 +426,12 @@ __device__ __forceinline__ void jacobi_item(const LaunchParams& p, const DBatch&
           if (sb != dev::kInfBits) {
             const u64 cand = dev::candidate(sb, rec.y, rec.z);
             best = cand < best ? cand : best;
+            if (kCount) wk.c[3] += 1;
           }
         }
       }
       if (dev::hi(best) != dev::hi(old)) changed = 1u << ql;
+      if (kCount) wk.c[5] += changed != 0u;
     }
     dw[idx] = best;
   }
@@ -411,8 +444,9 @@ __device__ __forceinline__ void jacobi_item(const LaunchParams& p, const DBatch&
 // admitted out-edges in place each round.
 // ---------------------------------------------------------------------------
 
+template <bool kCount>
 __device__ __forceinline__ void dense_item(const LaunchParams& p, const DBatch& B, DCtl& C, u32 item, u32 exec,
-                                           u32 widx) {
+                                           u32 widx, Work& wk) {
   const u32 lane = lane_id();
   const u32 sub = lane >> B.shift;
   const u32 ql = lane & (B.W - 1u);
@@ -426,6 +460,11 @@ __device__ __forceinline__ void dense_item(const LaunchParams& p, const DBatch& 
       const u32 sb = dev::hi(dev::ld_cg(B.dist[0] + ((static_cast<u64>(cu) << B.shift) + ql)));
       if (sb != dev::kInfBits) {
         const u32 rb = __ldg(p.g.csr_off + u), re = __ldg(p.g.csr_off + u + 1);
+        if (kCount) {
+          wk.c[0] += 1;
+          wk.c[1] += re - rb;
+          wk.c[2] += 1;
+        }
         for (u32 e = rb; e < re; ++e) {
           const uint4 rec = __ldg(p.g.csr + e);
           const uint2 dt = B.tiles[rec.w];
@@ -433,9 +472,15 @@ __device__ __forceinline__ void dense_item(const LaunchParams& p, const DBatch& 
             const u64 cand = dev::candidate(sb, rec.y, rec.z);
             u64* const target = B.dist[0] + ((static_cast<u64>(rec.x - dt.y) << B.shift) + ql);
             const u64 cur = dev::ld_cg(target);
+            if (kCount) wk.c[3] += 1;
             if (cand < cur) {
               dev::red_min(target, cand);
-              if (dev::hi(cand) < dev::hi(cur)) changed = 1u << ql;
+              const bool dec = dev::hi(cand) < dev::hi(cur);
+              if (dec) changed = 1u << ql;
+              if (kCount) {
+                wk.c[6] += 1;
+                wk.c[5] += dec;
+              }
             }
           }
         }
@@ -471,7 +516,8 @@ __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
   return prefix[p.nb];
 }
 
-__device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix) {
+template <bool kCount>
+__device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work& wk) {
   const u32 ridx = r % 3u, widx = (r + 1u) % 3u;
   const u32 total = prefix[p.nb];
   const u32 warps_per_block = blockDim.x >> 5;
@@ -484,11 +530,11 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix) {
     const u32 item = w - prefix[b];
     if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
       const u32 v = dev::ld_cg(B.queue[r & 1u] + item);
-      frontier_entry(p, B, C, v, r & 1u, widx);
+      frontier_entry<kCount>(p, B, C, v, r & 1u, widx, wk);
     } else if (p.engine == BFX_ENGINE_JACOBI_PULL) {
-      jacobi_item(p, B, C, item, r, widx);
+      jacobi_item<kCount>(p, B, C, item, r, widx, wk);
     } else {
-      dense_item(p, B, C, item, batch_exec(p, b, ridx), widx);
+      dense_item<kCount>(p, B, C, item, batch_exec(p, b, ridx), widx, wk);
     }
   }
 }
@@ -507,34 +553,52 @@ __device__ void round_bookkeeping(const LaunchParams& p, u32 r) {
   }
 }
 
+// Adds each thread's counters into the launch-wide totals.
+__device__ void flush_work(const LaunchParams& p, Work& wk) {
+  for (int i = 0; i < 7; ++i) {
+    u64 x = wk.c[i];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xFFFFFFFFu, x, o);
+    if (lane_id() == 0 && x) atomicAdd(reinterpret_cast<unsigned long long*>(&p.run->work[i]), x);
+  }
+}
+
+template <bool kCount>
 __global__ void __launch_bounds__(1024) persistent_kernel(LaunchParams p) {
   extern __shared__ u32 prefix[];
   const u32 nblocks = gridDim.x;
+  Work wk;
+  wk.zero();
   u32 r = 0;
   for (;; ++r) {
     const u32 total = round_work(p, r, prefix);
     if (total == 0u || r >= p.max_rounds) break;
     if (blockIdx.x == 0) round_bookkeeping(p, r);
-    round_body(p, r, prefix);
+    round_body<kCount>(p, r, prefix, wk);
     if (!dev::grid_barrier(&p.run->sync, nblocks, kBarrierTimeoutNs)) {
       if (threadIdx.x == 0) atomicExch(&p.run->abort, 1u);
       break;
     }
   }
+  if (kCount) flush_work(p, wk);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     p.run->round = r;
     p.run->done = 1u;
+    p.run->work[7] = r;
   }
 }
 
 // Host-poll modes: one round per launch over a fixed grid ...
+template <bool kCount>
 __global__ void __launch_bounds__(1024) round_kernel(LaunchParams p) {
   extern __shared__ u32 prefix[];
   if (dev::ld_cg(&p.run->done) != 0u) return;
   const u32 r = dev::ld_cg(&p.run->round);
   const u32 total = round_work(p, r, prefix);
   if (total == 0u) return;
-  round_body(p, r, prefix);
+  Work wk;
+  wk.zero();
+  round_body<kCount>(p, r, prefix, wk);
+  if (kCount) flush_work(p, wk);
 }
 
 // ... followed by a one-block advance: stop test, bookkeeping, next round.
@@ -549,6 +613,7 @@ __global__ void advance_kernel(LaunchParams p) {
   const u32 next_total = round_work(p, r + 1u, prefix);
   if (threadIdx.x == 0) {
     p.run->round = r + 1u;
+    p.run->work[7] = r + 1u;
     if (next_total == 0u || static_cast<u64>(r + 1u) >= p.max_rounds) p.run->done = 1u;
   }
 }
@@ -767,12 +832,16 @@ struct bfx_workspace {
   bfx_device_run_status* d_status{nullptr};
   bfx_device_controller* d_ctrl{nullptr};
   std::uint64_t last_launches{0};
+  std::uint64_t last_host_checks{0};
+  std::uint64_t last_h2d{0}, last_d2h{0};
+  cudaEvent_t ev[4]{};  // execute start, relaxation start, relaxation end, execute end
   bool executed{false};
   // Host-poll graph cache, keyed by the exact launch parameters.
   cudaGraphExec_t chunk_exec{nullptr};
   std::uint32_t chunk_rounds{0};
   int chunk_grid{0};
   int chunk_block{0};
+  std::uint32_t chunk_instr{0};
   bfx::LaunchParams chunk_params{};
   std::uint64_t generation{0};
 };
@@ -948,6 +1017,7 @@ int bfx_workspace_create(bfx_resident_graph* graph, bfx_workspace** out) {
     auto ws = std::make_unique<bfx_workspace>();
     ws->graph = graph;
     BFX_CUDA(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
+    for (auto& e : ws->ev) BFX_CUDA(cudaEventCreate(&e));
     BFX_CUDA(cudaDeviceGetAttribute(&ws->sm_count, cudaDevAttrMultiProcessorCount, graph->device));
     *out = ws.release();
   });
@@ -959,6 +1029,9 @@ int bfx_workspace_destroy(bfx_workspace* ws) {
     cudaSetDevice(ws->graph->device);
     if (ws->stream) cudaStreamSynchronize(ws->stream);
     if (ws->chunk_exec) cudaGraphExecDestroy(ws->chunk_exec);
+    for (auto& e : ws->ev) {
+      if (e) cudaEventDestroy(e);
+    }
     if (ws->stream) cudaStreamDestroy(ws->stream);
     delete ws;
   });
@@ -1151,6 +1224,7 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
     sbase[count] = static_cast<std::uint32_t>(ssum);
     std::memcpy(hb + o_batch, ws->batches.data(), count * sizeof(bfx::DBatch));
     bfx::upload(db, hb, meta_total, ws->stream);
+    ws->last_h2d = meta_total;
     // Tile tables must read 0 outside the union.
     for (std::uint32_t b = 0; b < count; ++b) {
       BFX_CUDA(cudaMemsetAsync(ws->batches[b].tiles, 0, size_t{g.T} * 8, ws->stream));
@@ -1216,6 +1290,8 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   const int block = static_cast<int>(o.block_size);
   const size_t smem = (size_t{ws->nb} + 1) * 4;
   std::uint64_t launches = 0;
+  ws->last_host_checks = 0;
+  BFX_CUDA(cudaEventRecord(ws->ev[0], ws->stream));
   // init + seed with a wide ordinary grid
   const int wide = ws->sm_count * 8;
   init_kernel<<<wide, 256, 0, ws->stream>>>(p);
@@ -1226,20 +1302,25 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   seed_kernel<<<seed_blocks, 256, 0, ws->stream>>>(p, ws->src_base);
   ++launches;
   BFX_CUDA(cudaGetLastError());
+  BFX_CUDA(cudaEventRecord(ws->ev[1], ws->stream));
   if (o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
-    const int grid = grid_blocks(ws, reinterpret_cast<const void*>(persistent_kernel), block, smem, o);
+    const void* kfn = o.instrumentation ? reinterpret_cast<const void*>(persistent_kernel<true>)
+                                        : reinterpret_cast<const void*>(persistent_kernel<false>);
+    const int grid = grid_blocks(ws, kfn, block, smem, o);
     void* args[] = {&p};
-    BFX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(persistent_kernel), grid, block, args, smem,
-                                         ws->stream));
+    BFX_CUDA(cudaLaunchCooperativeKernel(kfn, grid, block, args, smem, ws->stream));
     ++launches;
   } else {
     const std::uint32_t K = o.control_mode == BFX_CONTROL_PER_ROUND_HOST_POLL ? 1u : o.rounds_per_chunk;
-    const int grid = grid_blocks(ws, reinterpret_cast<const void*>(round_kernel), block, smem, o);
+    const void* kfn = o.instrumentation ? reinterpret_cast<const void*>(round_kernel<true>)
+                                        : reinterpret_cast<const void*>(round_kernel<false>);
+    const int grid = grid_blocks(ws, kfn, block, smem, o);
     start_kernel<<<1, 1024, smem, ws->stream>>>(p);
     ++launches;
     BFX_CUDA(cudaGetLastError());
     // Capture K x (round, advance) once per workspace generation / K / engine.
     const bool reuse = ws->chunk_exec && ws->chunk_rounds == K && ws->chunk_grid == grid &&
+                       ws->chunk_instr == o.instrumentation &&
                        ws->chunk_block == block && std::memcmp(&ws->chunk_params, &p, sizeof(p)) == 0;
     if (!reuse) {
       if (ws->chunk_exec) cudaGraphExecDestroy(ws->chunk_exec);
@@ -1247,7 +1328,11 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
       cudaGraph_t graph;
       BFX_CUDA(cudaStreamBeginCapture(ws->stream, cudaStreamCaptureModeThreadLocal));
       for (std::uint32_t k = 0; k < K; ++k) {
-        round_kernel<<<grid, block, smem, ws->stream>>>(p);
+        if (o.instrumentation) {
+          round_kernel<true><<<grid, block, smem, ws->stream>>>(p);
+        } else {
+          round_kernel<false><<<grid, block, smem, ws->stream>>>(p);
+        }
         advance_kernel<<<1, 1024, smem, ws->stream>>>(p);
       }
       BFX_CUDA(cudaStreamEndCapture(ws->stream, &graph));
@@ -1257,6 +1342,7 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
       ws->chunk_rounds = K;
       ws->chunk_grid = grid;
       ws->chunk_block = block;
+      ws->chunk_instr = o.instrumentation;
       ws->chunk_params = p;
     }
     // Poll the device controller after every chunk, as the reference's
@@ -1264,18 +1350,22 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
     ws->status_host.reserve(256);
     std::uint32_t* const done_host = static_cast<std::uint32_t*>(ws->status_host.ptr);
     const std::uint64_t max_chunks = (o.maximum_rounds + K - 1) / K + 1;
+    ws->last_host_checks = 0;
     for (std::uint64_t c = 0; c < max_chunks; ++c) {
       BFX_CUDA(cudaMemcpyAsync(done_host, &p.run->done, 4, cudaMemcpyDeviceToHost, ws->stream));
       BFX_CUDA(cudaStreamSynchronize(ws->stream));
+      ++ws->last_host_checks;
       if (*done_host) break;
       BFX_CUDA(cudaGraphLaunch(ws->chunk_exec, ws->stream));
       launches += 2ull * K;
     }
   }
   BFX_CUDA(cudaGetLastError());
+  BFX_CUDA(cudaEventRecord(ws->ev[2], ws->stream));
   finalize_kernel<<<ws->nb, 256, 0, ws->stream>>>(p, ws->d_ctrl, ws->d_status);
   ++launches;
   BFX_CUDA(cudaGetLastError());
+  BFX_CUDA(cudaEventRecord(ws->ev[3], ws->stream));
   ws->last_launches = launches;
   ws->executed = true;
   ws->params.engine = o.engine;
@@ -1308,6 +1398,7 @@ int bfx_fetch_statuses(bfx_workspace* ws, bfx_device_run_status* statuses, bfx_d
     BFX_CUDA(cudaStreamSynchronize(ws->stream));
     if (statuses) std::memcpy(statuses, h, sb);
     if (controllers) std::memcpy(controllers, h + sb, cb);
+    ws->last_d2h = (statuses ? sb : 0) + (controllers ? cb : 0);
   });
 }
 
@@ -1345,6 +1436,52 @@ int bfx_download_labels(bfx_workspace* ws, uint32_t batch, uint32_t* distance_bi
     cudaFreeAsync(d_out, ws->stream);
     BFX_CUDA(le);
     BFX_CUDA(cudaStreamSynchronize(ws->stream));
+  });
+}
+
+int bfx_fetch_work_statistics(bfx_workspace* ws, bfx_device_work_statistics* stats, uint64_t counters[8]) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null workspace");
+    bfx::require(ws->executed, "no executed batches");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    std::uint64_t w[8];
+    BFX_CUDA(cudaMemcpyAsync(w, ws->params.run->work, sizeof(w), cudaMemcpyDeviceToHost, ws->stream));
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    if (counters) std::memcpy(counters, w, sizeof(w));
+    if (stats) {
+      std::memset(stats, 0, sizeof(*stats));
+      stats->edges_examined = w[3];
+      stats->successful_decreases = w[5];
+      stats->active_vertices = w[0];
+      stats->active_lane_rounds = w[2];
+      stats->kernel_dispatches = ws->last_launches;
+      stats->atomic_attempts = w[6];
+      stats->successful_atomic_updates = w[5];
+      stats->queue_claims = w[4];
+      stats->full_edge_rounds = ws->params.engine == BFX_ENGINE_FRONTIER_PUSH ? 0u : w[7];
+      stats->host_checks = ws->last_host_checks;
+      stats->host_synchronizations = ws->last_host_checks;
+      stats->controller_copies = ws->last_host_checks;
+    }
+  });
+}
+
+int bfx_last_execute_timing(bfx_workspace* ws, float out[2]) {
+  return bfx::guarded([&] {
+    bfx::require(ws && out, "null argument");
+    bfx::require(ws->executed, "no executed batches");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    BFX_CUDA(cudaEventSynchronize(ws->ev[3]));
+    BFX_CUDA(cudaEventElapsedTime(&out[0], ws->ev[1], ws->ev[2]));
+    BFX_CUDA(cudaEventElapsedTime(&out[1], ws->ev[0], ws->ev[3]));
+  });
+}
+
+int bfx_workspace_transfer_bytes(bfx_workspace* ws, uint64_t out[2]) {
+  return bfx::guarded([&] {
+    bfx::require(ws && out, "null argument");
+    out[0] = ws->last_h2d;
+    out[1] = ws->last_d2h;
   });
 }
 

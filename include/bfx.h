@@ -87,6 +87,16 @@ typedef struct bfx_device_run_status {
   uint32_t reserved0;
 } bfx_device_run_status;
 
+/* Mirrors bfnew::DeviceWorkStatistics (gpu_api.hpp:122-150), 168 bytes. */
+typedef struct bfx_device_work_statistics {
+  uint64_t edges_examined, successful_decreases, active_vertices, active_lane_rounds;
+  uint64_t maximum_queue_size, host_checks, host_synchronizations, controller_copies;
+  uint64_t kernel_dispatches, expansion_count, atomic_attempts, successful_atomic_updates;
+  uint64_t queue_claims, duplicate_suppressions, mask_operations, overflow_events;
+  uint64_t high_contention_destinations, changed_flag_updates, full_edge_rounds;
+  uint64_t empty_frontier_rounds, small_frontier_rounds;
+} bfx_device_work_statistics;
+
 /* Flattened bfnew::DeviceGraphLayout32 (include/bfnew/device_layout.hpp:72-93)
  * plus csr_edge_ids, the stable EdgeId of every CSR position
  * (WeightedGraph::outgoing().edge_ids); NULL derives it from the CSC image.
@@ -198,8 +208,25 @@ int bfx_run_batches(bfx_workspace *ws, uint32_t count, const bfx_batch_descripti
 int bfx_download_labels(bfx_workspace *ws, uint32_t batch, uint32_t *distance_bits,
                         uint32_t *predecessor_edges);
 
+/* Device time of the most recent bfx_execute, measured by CUDA events the
+ * library records on the workspace stream: out[0] = relaxation kernels
+ * (the persistent launch, or all round/advance launches of a host-poll run),
+ * out[1] = the whole execute (init, seed, relaxation, finalize), in ms. */
+int bfx_last_execute_timing(bfx_workspace *ws, float out[2]);
+/* Bytes moved by the most recent bfx_prepare_batches (H2D) and
+ * bfx_fetch_statuses (D2H). */
+int bfx_workspace_transfer_bytes(bfx_workspace *ws, uint64_t out[2]);
+
 /* Kernels launched by the most recent bfx_execute (its own kernels only). */
 int bfx_last_launch_count(bfx_workspace *ws, uint64_t *launches);
+
+/* Work counters of the most recent bfx_execute run with instrumentation >= 1
+ * (the reference's Light level, gpu_api.hpp:40-44): stats in the reference's
+ * DeviceWorkStatistics layout; counters (may be NULL) = {queue entries
+ * processed, edge records read, active (vertex, lane) source reads, lane-edge
+ * relaxations, queue claims, distance decreases, min-reductions issued,
+ * rounds}.  Without instrumentation the counters read zero. */
+int bfx_fetch_work_statistics(bfx_workspace *ws, bfx_device_work_statistics *stats, uint64_t counters[8]);
 
 /* ---- plain per-query engine ----------------------------------------------
  * Replaces GpuSsspEngine::run(RouteQuery, GpuRunOptions) (gpu_api.hpp:203-211)
