@@ -165,6 +165,32 @@ def test_round_limit_stops_without_result_masks(gpu, c1, engine):
     res.close()
 
 
+@pytest.mark.parametrize("engine", ENGINES, ids=["frontier", "jacobi", "dense"])
+def test_instrumented_counters_and_timing(gpu, c1, engine):
+    """Light instrumentation fills the work counters without changing labels;
+    the library's event timing brackets the relaxation launch."""
+    d = bfx.make_description(c1.layout, c1.queries, 8)
+    res = bfx.ResidentDeviceGraph.upload_once(c1.layout)
+    ws = bfx.Workspace(res)
+    eng = ENGINE_CLASS[engine](res, ws)
+    st, labels = eng.run_with_distances([d], bfx.GpuRunOptions(instrumentation=1))
+    w = ws.work_counters()
+    k_ms, x_ms = ws.last_execute_timing()
+    assert 0 < k_ms <= x_ms
+    assert w["rounds"] == st[0].rounds_completed
+    assert w["relaxations"] >= w["decreases"] > 0 and w["records"] > 0 and w["entries"] > 0
+    if engine == bfx.ENGINE_FRONTIER_PUSH:
+        # every (vertex, lane) improvement that activated a vertex was claimed once per round
+        assert w["claims"] <= w["decreases"] and w["entries"] >= w["claims"]
+    plain, plabels = eng.run_with_distances([d], bfx.GpuRunOptions())
+    np.testing.assert_array_equal(labels[0][0], plabels[0][0])
+    np.testing.assert_array_equal(labels[0][1], plabels[0][1])
+    h2d, d2h = ws.transfer_bytes()
+    assert h2d > 0 and d2h == 48
+    ws.close()
+    res.close()
+
+
 def test_invalid_options_and_descriptions_rejected(gpu, c1):
     res = bfx.ResidentDeviceGraph.upload_once(c1.layout)
     ws = bfx.Workspace(res)
