@@ -80,6 +80,12 @@ class DeviceRunStatus(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("reserved")}
 
 
+class CompactTargetSummary(C.Structure):
+    """bfnew::CompactTargetSummary (include/bfnew/compact_path_types.hpp:31-47), 28 bytes."""
+    _fields_ = [("target", u32), ("selected_source", u32), ("distance", f32), ("path_length", u32),
+                ("reached", u32), ("reconstruction", u32), ("has_selected_source", u32)]
+
+
 class DeviceGraphLayout32View(C.Structure):
     _fields_ = [("vertex_count", u32), ("edge_count", u32), ("tile_count", u32), ("csr_run_count", u32),
                 ("csc_run_count", u32), ("reserved0", u32),
@@ -540,6 +546,41 @@ class Workspace:
         out = (u64 * 2)()
         _check(load().bfx_workspace_transfer_bytes(self._h, out))
         return int(out[0]), int(out[1])
+
+    def compact_paths(self, first_batch: int = 0, batch_count: int | None = None) -> list:
+        """ReusableCompactPathWorkspace::reconstruct: per target (description
+        order, batches [first_batch, first_batch+batch_count)) a dict with the
+        summary fields and, for complete targets, vertices (source first),
+        distance labels and stable edge ids."""
+        lib = load()
+        n = (self.batch_count - first_batch) if batch_count is None else batch_count
+        total = sum(self._keep[b].targets.shape[0] for b in range(first_batch, first_batch + n)) \
+            if hasattr(self, "_keep") and self._keep is not None else None
+        if total is None:
+            raise RuntimeError("compact paths need batches prepared through this workspace")
+        summ = (CompactTargetSummary * max(total, 1))()
+        sizes = (u64 * 3)()
+        _check(lib.bfx_compact_path_summaries(self._h, u32(first_batch), u32(n), summ, sizes))
+        nv, ne = int(sizes[1]), int(sizes[2])
+        verts = np.zeros(max(nv, 1), np.uint32)
+        labels = np.zeros(max(nv, 1), np.float32)
+        edges = np.zeros(max(ne, 1), np.uint32)
+        _check(lib.bfx_compact_path_payload(self._h, _ptr(verts), _ptr(labels, f32), _ptr(edges)))
+        out, vo, eo = [], 0, 0
+        for i in range(total):
+            s = summ[i]
+            d = {"target": s.target, "selected_source": s.selected_source, "distance": s.distance,
+                 "path_length": s.path_length, "reached": s.reached, "reconstruction": s.reconstruction,
+                 "has_selected_source": s.has_selected_source}
+            if s.reconstruction == 0:
+                L = s.path_length
+                d["vertices"] = verts[vo:vo + L + 1].copy()
+                d["labels"] = labels[vo:vo + L + 1].copy()
+                d["edges"] = edges[eo:eo + L].copy()
+                vo += L + 1
+                eo += L
+            out.append(d)
+        return out
 
     WORK_KEYS = ("entries", "records", "active_pairs", "relaxations", "claims", "decreases", "min_reductions",
                  "rounds")

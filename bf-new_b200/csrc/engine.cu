@@ -28,6 +28,7 @@
 #include "bfx.h"
 #include "bfx_internal.hpp"
 #include "device_common.cuh"
+#include "engine_types.cuh"
 
 #include <cuda_runtime.h>
 
@@ -46,93 +47,6 @@ thread_local std::string g_last_error;
 
 void set_last_error(const std::string& message) { g_last_error = message; }
 
-#define BFX_CUDA(call)                                                                          \
-  do {                                                                                          \
-    cudaError_t err_ = (call);                                                                  \
-    if (err_ != cudaSuccess) {                                                                  \
-      throw ::bfx::Error(err_ == cudaErrorMemoryAllocation ? BFX_ERR_OUT_OF_MEMORY : BFX_ERR_CUDA, \
-                         std::string(#call) + ": " + cudaGetErrorString(err_));                \
-    }                                                                                           \
-  } while (0)
-
-using dev::u32;
-using dev::u64;
-
-// ---------------------------------------------------------------------------
-// Device structures
-// ---------------------------------------------------------------------------
-
-struct DGraph {
-  u32 V, E, T, reserved;
-  const u32* owner;    // [V]
-  const u32* csr_off;  // [V+1]
-  const uint4* csr;    // [E] {dst, weight bits, eid+1, dst tile}
-  const u32* csc_off;  // [V+1]
-  const uint4* csc;    // [E] {src, weight bits, eid+1, src tile}
-};
-
-struct DBatch {
-  u32 W, shift, valid, U;
-  u32 src_count, tgt_count, range_count, reserved;
-  u64* dist[2];        // [U*W] labels (slot 1 only for Jacobi)
-  u32* mask[2];        // [U] pending lane masks (frontier)
-  u32* queue[2];       // [U] frontier vertices (global ids)
-  u32* c2g;            // [U] compact -> global vertex
-  uint2* tiles;        // [T] {lane mask, compact bias}
-  const u32* src_off;  // [W+1]
-  const u32* src;
-  const u32* tgt_off;  // [W+1]
-  const u32* tgt;
-  const uint4* ranges;    // [R] {tile, begin, end, lane mask}
-  const u32* range_off;   // [R+1] compact offsets
-};
-
-struct DCtl {
-  u32 count[3];    // frontier sizes, rotating by round
-  u32 changed[3];  // Jacobi/dense: lanes whose distance changed, rotating
-  u32 rounds;      // rounds executed with work
-  u32 missing;     // finalize: lanes with an unreached target
-  u32 active;      // finalize: lanes still pending at the stop
-  u32 error_bits;
-};
-
-struct DRun {
-  dev::GridSync sync;
-  u32 round;       // next round (host-poll modes)
-  u32 done;        // all batches stopped
-  u32 stop;        // launch-wide stop reason
-  u32 abort;       // device failure seen
-  u64 max_rounds;
-  u64 launches;
-  u64 work[8];     // launch-wide work counters (instrumented runs)
-};
-
-// Work counters of an instrumented run (instrumentation >= 1):
-// 0 queue entries processed, 1 edge records read, 2 active (vertex, lane)
-// source reads, 3 lane-edge relaxations, 4 queue claims, 5 distance
-// decreases, 6 min-reductions issued, 7 rounds executed.
-struct Work {
-  u64 c[7];
-  __device__ void zero() {
-    for (int i = 0; i < 7; ++i) c[i] = 0;
-  }
-};
-
-constexpr u32 kMaxBatchesPerLaunch = 4096;
-constexpr u64 kBarrierTimeoutNs = 2000000000ull;  // 2 s per barrier wait
-
-struct LaunchParams {
-  DGraph g;
-  const DBatch* batches;
-  DCtl* ctl;
-  DRun* run;
-  const u32* unit_base;  // [nb+1] prefix of U (init / finalize)
-  u32 nb;
-  u32 engine;
-  u32 per_lane;
-  u32 reserved;
-  u64 max_rounds;
-};
 
 // ---------------------------------------------------------------------------
 // Small device helpers
@@ -751,107 +665,13 @@ __global__ void expand_kernel(DGraph g, DBatch B, u32 slot, u32* bits, u32* pred
 }
 
 // ---------------------------------------------------------------------------
-// Host side
-// ---------------------------------------------------------------------------
-
-struct DeviceBuffer {
-  void* ptr{nullptr};
-  size_t bytes{0};
-  int device{0};
-  DeviceBuffer() = default;
-  DeviceBuffer(const DeviceBuffer&) = delete;
-  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-  ~DeviceBuffer() { release(); }
-  void release() {
-    if (ptr) {
-      cudaSetDevice(device);
-      cudaFree(ptr);
-    }
-    ptr = nullptr;
-    bytes = 0;
-  }
-  // Grows geometrically; contents are not preserved.
-  void reserve(size_t need, int dev) {
-    if (need <= bytes && ptr) return;
-    release();
-    device = dev;
-    size_t cap = std::max(need, bytes + bytes / 2);
-    cap = (cap + 255) & ~size_t{255};
-    BFX_CUDA(cudaMalloc(&ptr, cap));
-    bytes = cap;
-  }
-};
-
-struct PinnedBuffer {
-  void* ptr{nullptr};
-  size_t bytes{0};
-  PinnedBuffer() = default;
-  PinnedBuffer(const PinnedBuffer&) = delete;
-  PinnedBuffer& operator=(const PinnedBuffer&) = delete;
-  ~PinnedBuffer() {
-    if (ptr) cudaFreeHost(ptr);
-  }
-  void reserve(size_t need) {
-    if (need <= bytes && ptr) return;
-    if (ptr) cudaFreeHost(ptr);
-    ptr = nullptr;
-    size_t cap = std::max(need, bytes + bytes / 2);
-    cap = (cap + 255) & ~size_t{255};
-    BFX_CUDA(cudaHostAlloc(&ptr, cap, cudaHostAllocDefault));
-    bytes = cap;
-  }
-};
-
 }  // namespace bfx
-
-struct bfx_resident_graph {
-  int device{0};
-  bfx::DGraph g{};
-  bfx::DeviceBuffer mem;
-  std::vector<std::uint32_t> tile_vertex_offsets;  // host copy, [T+1]
-  std::uint64_t bytes{0};
-};
-
-struct bfx_workspace {
-  bfx_resident_graph* graph{nullptr};
-  cudaStream_t stream{nullptr};
-  int sm_count{0};
-  // Prepared batch set.
-  std::uint32_t nb{0};
-  std::uint64_t src_total{0};
-  std::vector<bfx::DBatch> batches;
-  bfx::DeviceBuffer meta;   // DBatch[], DCtl[], DRun, unit_base, src_base, uploaded descriptions
-  bfx::DeviceBuffer arena;  // labels, masks, queues, c2g, tile tables
-  bfx::PinnedBuffer staging;
-  bfx::PinnedBuffer status_host;
-  size_t meta_bytes{0};
-  size_t arena_bytes{0};
-  bool needs_slot2{false};
-  bfx::LaunchParams params{};
-  bfx::u32* src_base{nullptr};
-  bfx_device_run_status* d_status{nullptr};
-  bfx_device_controller* d_ctrl{nullptr};
-  std::uint64_t last_launches{0};
-  std::uint64_t last_host_checks{0};
-  std::uint64_t last_h2d{0}, last_d2h{0};
-  cudaEvent_t ev[4]{};  // execute start, relaxation start, relaxation end, execute end
-  bool executed{false};
-  // Host-poll graph cache, keyed by the exact launch parameters.
-  cudaGraphExec_t chunk_exec{nullptr};
-  std::uint32_t chunk_rounds{0};
-  int chunk_grid{0};
-  int chunk_block{0};
-  std::uint32_t chunk_instr{0};
-  bfx::LaunchParams chunk_params{};
-  std::uint64_t generation{0};
-};
 
 namespace bfx {
 namespace {
 
 std::mutex g_graph_mutex;
 
-size_t align256(size_t x) { return (x + 255) & ~size_t{255}; }
 
 void upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   if (bytes) BFX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
@@ -953,6 +773,7 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
     for (std::uint32_t t = 0; t < T; ++t) G->tile_vertex_offsets[t + 1] += G->tile_vertex_offsets[t];
 
     std::vector<uint4> csr(E), csc(E);
+    std::vector<std::uint32_t> eid_src(E, 0U);
     bfx::parallel_for(V, 0, [&](std::uint64_t b, std::uint64_t e) {
       for (std::uint64_t v = b; v < e; ++v) {
         for (std::uint32_t p = L.csr_row_offsets[v]; p < L.csr_row_offsets[v + 1]; ++p) {
@@ -960,6 +781,8 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
           std::uint32_t wb;
           std::memcpy(&wb, &L.csr_weights[p], 4);
           csr[p] = make_uint4(d, wb, eids[p] + 1U, L.owner_tiles[d]);
+          if (eids[p] >= E) throw std::out_of_range("csr edge id out of range");
+          eid_src[eids[p]] = static_cast<std::uint32_t>(v);
         }
         for (std::uint32_t q = L.csc_column_offsets[v]; q < L.csc_column_offsets[v + 1]; ++q) {
           const std::uint32_t s = L.csc_sources[q];
@@ -974,7 +797,8 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
     const size_t o_csc_off = bfx::align256(o_csr_off + (size_t{V} + 1) * 4);
     const size_t o_csr = bfx::align256(o_csc_off + (size_t{V} + 1) * 4);
     const size_t o_csc = bfx::align256(o_csr + size_t{E} * 16);
-    const size_t total = bfx::align256(o_csc + size_t{E} * 16);
+    const size_t o_eid_src = bfx::align256(o_csc + size_t{E} * 16);
+    const size_t total = bfx::align256(o_eid_src + size_t{E} * 4);
     G->mem.reserve(total, device);
     char* base = static_cast<char*>(G->mem.ptr);
     BFX_CUDA(cudaMemcpy(base + o_owner, L.owner_tiles, size_t{V} * 4, cudaMemcpyHostToDevice));
@@ -982,6 +806,7 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
     BFX_CUDA(cudaMemcpy(base + o_csc_off, L.csc_column_offsets, (size_t{V} + 1) * 4, cudaMemcpyHostToDevice));
     BFX_CUDA(cudaMemcpy(base + o_csr, csr.data(), size_t{E} * 16, cudaMemcpyHostToDevice));
     BFX_CUDA(cudaMemcpy(base + o_csc, csc.data(), size_t{E} * 16, cudaMemcpyHostToDevice));
+    BFX_CUDA(cudaMemcpy(base + o_eid_src, eid_src.data(), size_t{E} * 4, cudaMemcpyHostToDevice));
     G->g.V = V;
     G->g.E = E;
     G->g.T = T;
@@ -990,6 +815,7 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
     G->g.csc_off = reinterpret_cast<const std::uint32_t*>(base + o_csc_off);
     G->g.csr = reinterpret_cast<const uint4*>(base + o_csr);
     G->g.csc = reinterpret_cast<const uint4*>(base + o_csc);
+    G->g.eid_src = reinterpret_cast<const std::uint32_t*>(base + o_eid_src);
     G->bytes = total;
     *out = G.release();
   });
@@ -1368,6 +1194,7 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   BFX_CUDA(cudaEventRecord(ws->ev[3], ws->stream));
   ws->last_launches = launches;
   ws->executed = true;
+  ws->paths_ready = false;
   ws->params.engine = o.engine;
   ws->params.per_lane = o.enable_per_lane_convergence;
 }

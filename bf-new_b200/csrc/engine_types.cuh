@@ -1,0 +1,213 @@
+// Shared declarations of the CUDA translation units: device records of the
+// resident graph, batches and launch state, and the host-side resident
+// graph / workspace objects behind the C ABI handles.
+#pragma once
+
+#include "bfx.h"
+#include "bfx_internal.hpp"
+#include "device_common.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace bfx {
+
+#define BFX_CUDA(call)                                                                          \
+  do {                                                                                          \
+    cudaError_t err_ = (call);                                                                  \
+    if (err_ != cudaSuccess) {                                                                  \
+      throw ::bfx::Error(err_ == cudaErrorMemoryAllocation ? BFX_ERR_OUT_OF_MEMORY : BFX_ERR_CUDA, \
+                         std::string(#call) + ": " + cudaGetErrorString(err_));                \
+    }                                                                                           \
+  } while (0)
+
+using dev::u32;
+using dev::u64;
+
+// ---------------------------------------------------------------------------
+// Device structures
+// ---------------------------------------------------------------------------
+
+struct DGraph {
+  u32 V, E, T, reserved;
+  const u32* owner;    // [V]
+  const u32* csr_off;  // [V+1]
+  const uint4* csr;    // [E] {dst, weight bits, eid+1, dst tile}
+  const u32* csc_off;  // [V+1]
+  const uint4* csc;    // [E] {src, weight bits, eid+1, src tile}
+  const u32* eid_src;  // [E] source vertex of each stable edge id
+};
+
+struct DBatch {
+  u32 W, shift, valid, U;
+  u32 src_count, tgt_count, range_count, reserved;
+  u64* dist[2];        // [U*W] labels (slot 1 only for Jacobi)
+  u32* mask[2];        // [U] pending lane masks (frontier)
+  u32* queue[2];       // [U] frontier vertices (global ids)
+  u32* c2g;            // [U] compact -> global vertex
+  uint2* tiles;        // [T] {lane mask, compact bias}
+  const u32* src_off;  // [W+1]
+  const u32* src;
+  const u32* tgt_off;  // [W+1]
+  const u32* tgt;
+  const uint4* ranges;    // [R] {tile, begin, end, lane mask}
+  const u32* range_off;   // [R+1] compact offsets
+};
+
+struct DCtl {
+  u32 count[3];    // frontier sizes, rotating by round
+  u32 changed[3];  // Jacobi/dense: lanes whose distance changed, rotating
+  u32 rounds;      // rounds executed with work
+  u32 missing;     // finalize: lanes with an unreached target
+  u32 active;      // finalize: lanes still pending at the stop
+  u32 error_bits;
+};
+
+struct DRun {
+  dev::GridSync sync;
+  u32 round;       // next round (host-poll modes)
+  u32 done;        // all batches stopped
+  u32 stop;        // launch-wide stop reason
+  u32 abort;       // device failure seen
+  u64 max_rounds;
+  u64 launches;
+  u64 work[8];     // launch-wide work counters (instrumented runs)
+};
+
+// Work counters of an instrumented run (instrumentation >= 1):
+// 0 queue entries processed, 1 edge records read, 2 active (vertex, lane)
+// source reads, 3 lane-edge relaxations, 4 queue claims, 5 distance
+// decreases, 6 min-reductions issued, 7 rounds executed.
+struct Work {
+  u64 c[7];
+  __device__ void zero() {
+    for (int i = 0; i < 7; ++i) c[i] = 0;
+  }
+};
+
+constexpr u32 kMaxBatchesPerLaunch = 4096;
+constexpr u64 kBarrierTimeoutNs = 2000000000ull;  // 2 s per barrier wait
+
+struct LaunchParams {
+  DGraph g;
+  const DBatch* batches;
+  DCtl* ctl;
+  DRun* run;
+  const u32* unit_base;  // [nb+1] prefix of U (init / finalize)
+  u32 nb;
+  u32 engine;
+  u32 per_lane;
+  u32 reserved;
+  u64 max_rounds;
+};
+
+// Host side
+// ---------------------------------------------------------------------------
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t{255}; }
+
+struct DeviceBuffer {
+  void* ptr{nullptr};
+  size_t bytes{0};
+  int device{0};
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer() { release(); }
+  void release() {
+    if (ptr) {
+      cudaSetDevice(device);
+      cudaFree(ptr);
+    }
+    ptr = nullptr;
+    bytes = 0;
+  }
+  // Grows geometrically; contents are not preserved.
+  void reserve(size_t need, int dev) {
+    if (need <= bytes && ptr) return;
+    release();
+    device = dev;
+    size_t cap = std::max(need, bytes + bytes / 2);
+    cap = (cap + 255) & ~size_t{255};
+    BFX_CUDA(cudaMalloc(&ptr, cap));
+    bytes = cap;
+  }
+};
+
+struct PinnedBuffer {
+  void* ptr{nullptr};
+  size_t bytes{0};
+  PinnedBuffer() = default;
+  PinnedBuffer(const PinnedBuffer&) = delete;
+  PinnedBuffer& operator=(const PinnedBuffer&) = delete;
+  ~PinnedBuffer() {
+    if (ptr) cudaFreeHost(ptr);
+  }
+  void reserve(size_t need) {
+    if (need <= bytes && ptr) return;
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    size_t cap = std::max(need, bytes + bytes / 2);
+    cap = (cap + 255) & ~size_t{255};
+    BFX_CUDA(cudaHostAlloc(&ptr, cap, cudaHostAllocDefault));
+    bytes = cap;
+  }
+};
+
+}  // namespace bfx
+
+struct bfx_resident_graph {
+  int device{0};
+  bfx::DGraph g{};
+  bfx::DeviceBuffer mem;
+  std::vector<std::uint32_t> tile_vertex_offsets;  // host copy, [T+1]
+  std::uint64_t bytes{0};
+};
+
+struct bfx_workspace {
+  bfx_resident_graph* graph{nullptr};
+  cudaStream_t stream{nullptr};
+  int sm_count{0};
+  // Prepared batch set.
+  std::uint32_t nb{0};
+  std::uint64_t src_total{0};
+  std::vector<bfx::DBatch> batches;
+  bfx::DeviceBuffer meta;   // DBatch[], DCtl[], DRun, unit_base, src_base, uploaded descriptions
+  bfx::DeviceBuffer arena;  // labels, masks, queues, c2g, tile tables
+  bfx::PinnedBuffer staging;
+  bfx::PinnedBuffer status_host;
+  size_t meta_bytes{0};
+  size_t arena_bytes{0};
+  bool needs_slot2{false};
+  bfx::LaunchParams params{};
+  bfx::u32* src_base{nullptr};
+  bfx_device_run_status* d_status{nullptr};
+  bfx_device_controller* d_ctrl{nullptr};
+  std::uint64_t last_launches{0};
+  std::uint64_t last_host_checks{0};
+  std::uint64_t last_h2d{0}, last_d2h{0};
+  cudaEvent_t ev[4]{};  // execute start, relaxation start, relaxation end, execute end
+  bool executed{false};
+  // Host-poll graph cache, keyed by the exact launch parameters.
+  cudaGraphExec_t chunk_exec{nullptr};
+  std::uint32_t chunk_rounds{0};
+  int chunk_grid{0};
+  int chunk_block{0};
+  std::uint32_t chunk_instr{0};
+  bfx::LaunchParams chunk_params{};
+  std::uint64_t generation{0};
+  // Compact path reconstruction state (summaries pass -> payload pass).
+  bfx::DeviceBuffer paths;       // summaries, offsets, flags, search scratch
+  bfx::PinnedBuffer paths_host;
+  std::uint32_t path_first_batch{0};
+  std::uint32_t path_batch_count{0};
+  std::uint64_t path_targets{0};
+  std::uint64_t path_vertices{0};  // payload sizes after the summaries pass
+  std::uint64_t path_edges{0};
+  bool paths_ready{false};
+};
+

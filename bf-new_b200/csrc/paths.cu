@@ -1,0 +1,444 @@
+// Compact path reconstruction on the device (the reference's
+// ReusableCompactPathWorkspace::reconstruct, include/bfnew/hip/compact_path_results.hpp:99-127,
+// whose kernel runs one serial depth-first search for every target on a
+// single thread, src/hip/compact_path_results.hip.cpp:251-271).
+//
+// The relaxation labels already carry, per (vertex, lane), the smallest
+// stable edge id among tight admitted in-edges -- the first candidate of the
+// reference's search (tight_choices, src/compact_paths.cpp:98-129).  So a
+// target's path is found by one thread walking predecessors, all targets of
+// all lanes in parallel.  The walk equals the reference's search whenever it
+// never revisits a vertex; a revisit needs an equal-distance (zero-weight)
+// step, so the walk tracks runs of equal distances and hands a target to the
+// exact backtracking search (reconstruct_target, src/compact_paths.cpp:131-211)
+// when a run revisits a vertex or grows long.  That search runs serially per
+// flagged target with scratch sized by the largest union.
+//
+// Two passes as in the reference: summaries (status, source, distance,
+// length), then, after a host prefix over the lengths, the payload (path
+// vertices source-first, their labels, stable edge ids).
+#include "bfx.h"
+#include "bfx_internal.hpp"
+#include "device_common.cuh"
+#include "engine_types.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <vector>
+
+namespace bfx {
+namespace {
+
+constexpr u32 kPlateau = 16;  // equal-distance run the walk checks itself
+constexpr u32 kFallback = 0x80000000u;
+
+struct PathArgs {
+  DGraph g;
+  const DBatch* batches;
+  const bfx_device_run_status* status;
+  u32 first_batch, batch_count;
+  const u32* target_base;  // [batch_count+1] prefix of target counts
+  bfx_compact_target_summary* summaries;
+  u32* lengths;            // walk result | kFallback
+  const u64* vertex_offsets;  // payload pass
+  const u64* edge_offsets;
+  u32* out_vertices;
+  float* out_labels;
+  u32* out_edges;
+  // search scratch
+  u32* stack_v;
+  u32* stack_c;
+  u32* stack_e;
+  u32* on_path;  // bitmap over compact vertices
+  u32 max_union;
+};
+
+__device__ __forceinline__ u32 lane_of(const u32* offsets, u32 W, u32 pos) {
+  u32 lo = 0, hi = W;
+  while (hi - lo > 1u) {
+    const u32 mid = (lo + hi) >> 1;
+    if (offsets[mid] <= pos) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ u32 find_b(const u32* prefix, u32 n, u32 x) {
+  u32 lo = 0, hi = n;
+  while (hi - lo > 1u) {
+    const u32 mid = (lo + hi) >> 1;
+    if (prefix[mid] <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ u64 label(const DGraph& g, const DBatch& B, const u64* d, u32 v, u32 lane) {
+  const uint2 t = B.tiles[g.owner[v]];
+  if (((t.x >> lane) & 1u) == 0u) return dev::kUnreached;
+  return d[(static_cast<u64>(v - t.y) << B.shift) + lane];
+}
+
+__device__ __forceinline__ bool clean(const bfx_device_run_status& s) {
+  return s.stop_reason == BFX_STOP_CONVERGED && s.error_bits == 0u;
+}
+
+// Pass 1: one thread per target of the selected batches.
+__global__ void summaries_kernel(PathArgs a) {
+  const u32 total = a.target_base[a.batch_count];
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const u32 bi = find_b(a.target_base, a.batch_count, i);
+    const u32 b = a.first_batch + bi;
+    const DBatch& B = a.batches[b];
+    const bfx_device_run_status& st = a.status[b];
+    const u32 pos = i - a.target_base[bi];
+    const u32 lane = lane_of(B.tgt_off, B.W, pos);
+    const u32 t = B.tgt[pos];
+    bfx_compact_target_summary s;
+    s.target = t;
+    s.selected_source = 0u;
+    s.distance = __uint_as_float(dev::kInfBits);
+    s.path_length = 0u;
+    s.reached = 0u;
+    s.reconstruction = 2u;  // query_terminal_failure
+    s.has_selected_source = 0u;
+    u32 len = 0u;
+    if (clean(st)) {
+      const u64* d = B.dist[st.final_distance_slot];
+      u64 w = label(a.g, B, d, t, lane);
+      if (dev::hi(w) == dev::kInfBits) {
+        s.reconstruction = 1u;  // unreachable
+      } else {
+        s.reached = 1u;
+        s.distance = __uint_as_float(dev::hi(w));
+        u32 v = t, pn = 0;
+        u32 plateau[kPlateau];
+        bool fallback = false;
+        while (static_cast<u32>(w) != 0u) {
+          const u32 e = static_cast<u32>(w) - 1u;
+          if (e >= a.g.E) {
+            fallback = true;
+            break;
+          }
+          const u32 u = a.g.eid_src[e];
+          const u64 wu = label(a.g, B, d, u, lane);
+          if (dev::hi(wu) == dev::kInfBits) {  // inconsistent chain: let the search decide
+            fallback = true;
+            break;
+          }
+          if (dev::hi(wu) == dev::hi(w)) {
+            if (pn == 0u) plateau[pn++] = v;
+            for (u32 k = 0; k < pn; ++k) fallback |= plateau[k] == u;
+            if (fallback || pn == kPlateau) {
+              fallback = true;
+              break;
+            }
+            plateau[pn++] = u;
+          } else {
+            pn = 0u;
+          }
+          ++len;
+          if (len > B.U) {
+            fallback = true;
+            break;
+          }
+          v = u;
+          w = wu;
+        }
+        if (fallback) {
+          len = kFallback;
+        } else {
+          s.reconstruction = 0u;  // complete
+          s.path_length = len;
+          s.selected_source = v;
+          s.has_selected_source = 1u;
+        }
+      }
+    }
+    a.lengths[i] = len;
+    a.summaries[i] = s;
+  }
+}
+
+// The reference's backtracking search for one target (reconstruct_target):
+// candidates in stable-edge-id order, predecessors on the current path
+// skipped, dead ends popped.  Returns the edge count (or ~0u if no path) and
+// leaves the path on the stacks (stack_v[0] = target).
+__device__ u32 search_target(const PathArgs& a, const DBatch& B, const u64* d, u32 t, u32 lane) {
+  auto cv = [&](u32 v) { return v - B.tiles[a.g.owner[v]].y; };
+  auto mark = [&](u32 v, bool on) {
+    const u32 c = cv(v);
+    if (on) a.on_path[c >> 5] |= 1u << (c & 31u); else a.on_path[c >> 5] &= ~(1u << (c & 31u));
+  };
+  auto marked = [&](u32 v) {
+    const u32 c = cv(v);
+    return (a.on_path[c >> 5] >> (c & 31u)) & 1u;
+  };
+  int depth = 0;
+  a.stack_v[0] = t;
+  a.stack_c[0] = 0u;
+  mark(t, true);
+  u32 found = 0xFFFFFFFFu;
+  while (depth >= 0) {
+    const u32 v = a.stack_v[depth];
+    const u64 wv = label(a.g, B, d, v, lane);
+    if (static_cast<u32>(wv) == 0u) {  // a source of this lane
+      found = static_cast<u32>(depth);
+      break;
+    }
+    const u32 dv = dev::hi(wv);
+    u32 best = 0xFFFFFFFFu, bu = 0u;
+    for (u32 q = a.g.csc_off[v]; q < a.g.csc_off[v + 1]; ++q) {
+      const uint4 rec = a.g.csc[q];
+      if (rec.z <= a.stack_c[depth] || rec.z >= best) continue;
+      const uint2 su = B.tiles[rec.w];
+      if (((su.x >> lane) & 1u) == 0u) continue;
+      const u32 du = dev::hi(d[(static_cast<u64>(rec.x - su.y) << B.shift) + lane]);
+      if (du == dev::kInfBits) continue;
+      if (__float_as_uint(__fadd_rn(__uint_as_float(du), __uint_as_float(rec.y))) != dv) continue;
+      best = rec.z;
+      bu = rec.x;
+    }
+    if (best == 0xFFFFFFFFu) {
+      mark(v, false);
+      --depth;
+      continue;
+    }
+    a.stack_c[depth] = best;
+    if (marked(bu)) continue;
+    ++depth;
+    a.stack_v[depth] = bu;
+    a.stack_c[depth] = 0u;
+    a.stack_e[depth] = best - 1u;
+    mark(bu, true);
+  }
+  // clear the marks of the path that remained (popped vertices are clear)
+  if (found != 0xFFFFFFFFu) {
+    for (u32 k = 0; k <= found; ++k) mark(a.stack_v[k], false);
+  }
+  return found;
+}
+
+// Serial pass over flagged targets (rare: zero-weight ties that revisit).
+// payload == false: fill summaries; true: write the payload.
+__global__ void search_kernel(PathArgs a, bool payload) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const u32 total = a.target_base[a.batch_count];
+  for (u32 i = 0; i < total; ++i) {
+    if ((a.lengths[i] & kFallback) == 0u) continue;
+    const u32 bi = find_b(a.target_base, a.batch_count, i);
+    const u32 b = a.first_batch + bi;
+    const DBatch& B = a.batches[b];
+    const u32 pos = i - a.target_base[bi];
+    const u32 lane = lane_of(B.tgt_off, B.W, pos);
+    const u64* d = B.dist[a.status[b].final_distance_slot];
+    const u32 n = search_target(a, B, d, B.tgt[pos], lane);
+    if (!payload) {
+      bfx_compact_target_summary& s = a.summaries[i];
+      if (n == 0xFFFFFFFFu) {
+        s.reconstruction = 3u;  // no_tight_path
+      } else {
+        s.reconstruction = 0u;
+        s.path_length = n;
+        s.selected_source = a.stack_v[n];
+        s.has_selected_source = 1u;
+      }
+    } else if (n != 0xFFFFFFFFu) {
+      const u64 vo = a.vertex_offsets[i], eo = a.edge_offsets[i];
+      for (u32 k = 0; k <= n; ++k) {
+        const u32 v = a.stack_v[n - k];
+        a.out_vertices[vo + k] = v;
+        a.out_labels[vo + k] = __uint_as_float(dev::hi(label(a.g, B, d, v, lane)));
+        if (k < n) a.out_edges[eo + k] = a.stack_e[n - k];
+      }
+    }
+  }
+}
+
+// Pass 2: one thread per complete, walkable target writes its payload.
+__global__ void payload_kernel(PathArgs a) {
+  const u32 total = a.target_base[a.batch_count];
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const u32 len = a.lengths[i];
+    if ((len & kFallback) != 0u || a.summaries[i].reconstruction != 0u) continue;
+    const u32 bi = find_b(a.target_base, a.batch_count, i);
+    const u32 b = a.first_batch + bi;
+    const DBatch& B = a.batches[b];
+    const u32 pos = i - a.target_base[bi];
+    const u32 lane = lane_of(B.tgt_off, B.W, pos);
+    const u64* d = B.dist[a.status[b].final_distance_slot];
+    const u64 vo = a.vertex_offsets[i], eo = a.edge_offsets[i];
+    u32 v = B.tgt[pos];
+    u64 w = label(a.g, B, d, v, lane);
+    for (u32 k = 0;; ++k) {
+      a.out_vertices[vo + len - k] = v;
+      a.out_labels[vo + len - k] = __uint_as_float(dev::hi(w));
+      if (k == len) break;
+      const u32 e = static_cast<u32>(w) - 1u;
+      a.out_edges[eo + len - 1u - k] = e;
+      v = a.g.eid_src[e];
+      w = label(a.g, B, d, v, lane);
+    }
+  }
+}
+
+void check_ready(bfx_workspace* ws) {
+  require(ws != nullptr, "null workspace");
+  require(ws->executed, "no executed batches");
+}
+
+}  // namespace
+}  // namespace bfx
+
+extern "C" {
+
+int bfx_compact_path_summaries(bfx_workspace* ws, uint32_t first_batch, uint32_t batch_count,
+                               bfx_compact_target_summary* summaries, uint64_t sizes[3]) {
+  return bfx::guarded([&] {
+    bfx::check_ready(ws);
+    bfx::require(summaries != nullptr, "null output");
+    if (batch_count == 0 || first_batch >= ws->nb || batch_count > ws->nb - first_batch)
+      throw std::out_of_range("batch range");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    std::vector<std::uint32_t> tbase(batch_count + 1, 0U);
+    std::uint32_t max_union = 0;
+    for (std::uint32_t i = 0; i < batch_count; ++i) {
+      const bfx::DBatch& B = ws->batches[first_batch + i];
+      tbase[i + 1] = tbase[i] + B.tgt_count;
+      max_union = std::max(max_union, B.U);
+    }
+    const std::uint64_t T = tbase[batch_count];
+    const size_t o_tb = 0;
+    const size_t o_sum = bfx::align256(o_tb + (batch_count + 1) * 4);
+    const size_t o_len = bfx::align256(o_sum + T * sizeof(bfx_compact_target_summary));
+    const size_t o_vo = bfx::align256(o_len + T * 4);
+    const size_t o_eo = bfx::align256(o_vo + T * 8);
+    const size_t o_sv = bfx::align256(o_eo + T * 8);
+    const size_t o_sc = bfx::align256(o_sv + (size_t{max_union} + 1) * 4);
+    const size_t o_se = bfx::align256(o_sc + (size_t{max_union} + 1) * 4);
+    const size_t o_op = bfx::align256(o_se + (size_t{max_union} + 1) * 4);
+    const size_t total = bfx::align256(o_op + (size_t{max_union} / 32 + 1) * 4);
+    ws->paths.reserve(total, ws->graph->device);
+    char* base = static_cast<char*>(ws->paths.ptr);
+    BFX_CUDA(cudaMemcpyAsync(base + o_tb, tbase.data(), (batch_count + 1) * 4, cudaMemcpyHostToDevice, ws->stream));
+    BFX_CUDA(cudaMemsetAsync(base + o_op, 0, (size_t{max_union} / 32 + 1) * 4, ws->stream));
+    bfx::PathArgs a{};
+    a.g = ws->graph->g;
+    a.batches = ws->params.batches;
+    a.status = ws->d_status;
+    a.first_batch = first_batch;
+    a.batch_count = batch_count;
+    a.target_base = reinterpret_cast<const std::uint32_t*>(base + o_tb);
+    a.summaries = reinterpret_cast<bfx_compact_target_summary*>(base + o_sum);
+    a.lengths = reinterpret_cast<std::uint32_t*>(base + o_len);
+    a.vertex_offsets = reinterpret_cast<const std::uint64_t*>(base + o_vo);
+    a.edge_offsets = reinterpret_cast<const std::uint64_t*>(base + o_eo);
+    a.stack_v = reinterpret_cast<std::uint32_t*>(base + o_sv);
+    a.stack_c = reinterpret_cast<std::uint32_t*>(base + o_sc);
+    a.stack_e = reinterpret_cast<std::uint32_t*>(base + o_se);
+    a.on_path = reinterpret_cast<std::uint32_t*>(base + o_op);
+    a.max_union = max_union;
+    if (T > 0) {
+      const int blocks = static_cast<int>(std::min<std::uint64_t>((T + 255) / 256, 4096));
+      bfx::summaries_kernel<<<blocks, 256, 0, ws->stream>>>(a);
+      BFX_CUDA(cudaGetLastError());
+      bfx::search_kernel<<<1, 1, 0, ws->stream>>>(a, false);
+      BFX_CUDA(cudaGetLastError());
+    }
+    ws->paths_host.reserve(T * sizeof(bfx_compact_target_summary) + 256);
+    BFX_CUDA(cudaMemcpyAsync(ws->paths_host.ptr, a.summaries, T * sizeof(bfx_compact_target_summary),
+                             cudaMemcpyDeviceToHost, ws->stream));
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    std::memcpy(summaries, ws->paths_host.ptr, T * sizeof(bfx_compact_target_summary));
+    // Payload offsets (checked host prefix, as the reference does).
+    std::vector<std::uint64_t> vo(T), eo(T);
+    std::uint64_t nv = 0, ne = 0;
+    for (std::uint64_t i = 0; i < T; ++i) {
+      vo[i] = nv;
+      eo[i] = ne;
+      if (summaries[i].reconstruction == 0u) {
+        nv += std::uint64_t{summaries[i].path_length} + 1U;
+        ne += summaries[i].path_length;
+      }
+    }
+    BFX_CUDA(cudaMemcpyAsync(base + o_vo, vo.data(), T * 8, cudaMemcpyHostToDevice, ws->stream));
+    BFX_CUDA(cudaMemcpyAsync(base + o_eo, eo.data(), T * 8, cudaMemcpyHostToDevice, ws->stream));
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    ws->path_first_batch = first_batch;
+    ws->path_batch_count = batch_count;
+    ws->path_targets = T;
+    ws->path_vertices = nv;
+    ws->path_edges = ne;
+    ws->paths_ready = true;
+    if (sizes) {
+      sizes[0] = T;
+      sizes[1] = nv;
+      sizes[2] = ne;
+    }
+  });
+}
+
+int bfx_compact_path_payload(bfx_workspace* ws, uint32_t* vertices, float* distance_labels, uint32_t* edge_ids) {
+  return bfx::guarded([&] {
+    bfx::check_ready(ws);
+    bfx::require(ws->paths_ready, "call bfx_compact_path_summaries first");
+    bfx::require(vertices && distance_labels && (edge_ids || ws->path_edges == 0), "null output");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    const std::uint64_t T = ws->path_targets, nv = ws->path_vertices, ne = ws->path_edges;
+    const std::uint32_t batch_count = ws->path_batch_count;
+    std::uint32_t max_union = 0;
+    for (std::uint32_t i = 0; i < batch_count; ++i) max_union = std::max(max_union, ws->batches[ws->path_first_batch + i].U);
+    char* base = static_cast<char*>(ws->paths.ptr);
+    const size_t o_tb = 0;
+    const size_t o_sum = bfx::align256(o_tb + (batch_count + 1) * 4);
+    const size_t o_len = bfx::align256(o_sum + T * sizeof(bfx_compact_target_summary));
+    const size_t o_vo = bfx::align256(o_len + T * 4);
+    const size_t o_eo = bfx::align256(o_vo + T * 8);
+    const size_t o_sv = bfx::align256(o_eo + T * 8);
+    const size_t o_sc = bfx::align256(o_sv + (size_t{max_union} + 1) * 4);
+    const size_t o_se = bfx::align256(o_sc + (size_t{max_union} + 1) * 4);
+    const size_t o_op = bfx::align256(o_se + (size_t{max_union} + 1) * 4);
+    // Output arena: vertices, labels, edges in one device allocation.
+    const size_t out_bytes = bfx::align256(nv * 4) * 2 + bfx::align256(ne * 4 + 4);
+    char* dout = nullptr;
+    BFX_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&dout), out_bytes, ws->stream));
+    bfx::PathArgs a{};
+    a.g = ws->graph->g;
+    a.batches = ws->params.batches;
+    a.status = ws->d_status;
+    a.first_batch = ws->path_first_batch;
+    a.batch_count = batch_count;
+    a.target_base = reinterpret_cast<const std::uint32_t*>(base + o_tb);
+    a.summaries = reinterpret_cast<bfx_compact_target_summary*>(base + o_sum);
+    a.lengths = reinterpret_cast<std::uint32_t*>(base + o_len);
+    a.vertex_offsets = reinterpret_cast<const std::uint64_t*>(base + o_vo);
+    a.edge_offsets = reinterpret_cast<const std::uint64_t*>(base + o_eo);
+    a.out_vertices = reinterpret_cast<std::uint32_t*>(dout);
+    a.out_labels = reinterpret_cast<float*>(dout + bfx::align256(nv * 4));
+    a.out_edges = reinterpret_cast<std::uint32_t*>(dout + 2 * bfx::align256(nv * 4));
+    a.stack_v = reinterpret_cast<std::uint32_t*>(base + o_sv);
+    a.stack_c = reinterpret_cast<std::uint32_t*>(base + o_sc);
+    a.stack_e = reinterpret_cast<std::uint32_t*>(base + o_se);
+    a.on_path = reinterpret_cast<std::uint32_t*>(base + o_op);
+    a.max_union = max_union;
+    cudaError_t err = cudaSuccess;
+    if (T > 0) {
+      const int blocks = static_cast<int>(std::min<std::uint64_t>((T + 255) / 256, 4096));
+      bfx::payload_kernel<<<blocks, 256, 0, ws->stream>>>(a);
+      err = cudaGetLastError();
+      if (err == cudaSuccess) {
+        bfx::search_kernel<<<1, 1, 0, ws->stream>>>(a, true);
+        err = cudaGetLastError();
+      }
+    }
+    if (err == cudaSuccess && nv) {
+      cudaMemcpyAsync(vertices, a.out_vertices, nv * 4, cudaMemcpyDeviceToHost, ws->stream);
+      cudaMemcpyAsync(distance_labels, a.out_labels, nv * 4, cudaMemcpyDeviceToHost, ws->stream);
+    }
+    if (err == cudaSuccess && ne) cudaMemcpyAsync(edge_ids, a.out_edges, ne * 4, cudaMemcpyDeviceToHost, ws->stream);
+    cudaFreeAsync(dout, ws->stream);
+    BFX_CUDA(err);
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+  });
+}
+
+}  // extern "C"

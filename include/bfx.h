@@ -217,6 +217,34 @@ int bfx_last_execute_timing(bfx_workspace *ws, float out[2]);
  * bfx_fetch_statuses (D2H). */
 int bfx_workspace_transfer_bytes(bfx_workspace *ws, uint64_t out[2]);
 
+/* ---- compact paths ---------------------------------------------------------
+ * Replace ReusableCompactPathWorkspace::reconstruct / run_compact_paths
+ * (include/bfnew/hip/compact_path_results.hpp:99-127,
+ * hip/batched_frontier_push.hpp:118-121).  Per target of batches
+ * [first_batch, first_batch + batch_count) of the last execute, in
+ * description order: a summary mirroring bfnew::CompactTargetSummary
+ * (include/bfnew/compact_path_types.hpp:31-47, 28 bytes; reached 0/1;
+ * reconstruction 0 complete, 1 unreachable, 2 query terminal failure (the
+ * lane's run did not converge cleanly), 3 no tight path).  Paths follow the
+ * reference's deterministic tight-edge search (src/compact_paths.cpp:131-211).
+ * sizes (may be NULL) = {targets, payload vertices, payload edges}. */
+typedef struct bfx_compact_target_summary {
+  uint32_t target;
+  uint32_t selected_source;
+  float distance;
+  uint32_t path_length;
+  uint32_t reached;
+  uint32_t reconstruction;
+  uint32_t has_selected_source;
+} bfx_compact_target_summary;
+
+int bfx_compact_path_summaries(bfx_workspace *ws, uint32_t first_batch, uint32_t batch_count,
+                               bfx_compact_target_summary *summaries, uint64_t sizes[3]);
+/* Second pass: complete targets' paths concatenated in summary order; per
+ * target path_length + 1 vertices (source first) with their final labels and
+ * path_length stable edge ids. */
+int bfx_compact_path_payload(bfx_workspace *ws, uint32_t *vertices, float *distance_labels, uint32_t *edge_ids);
+
 /* Kernels launched by the most recent bfx_execute (its own kernels only). */
 int bfx_last_launch_count(bfx_workspace *ws, uint64_t *launches);
 
