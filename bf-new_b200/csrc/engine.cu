@@ -1359,3 +1359,241 @@ int bfx_run_query(bfx_workspace* ws, uint32_t source_count, const uint32_t* sour
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Static-scratch single-query entry point (bfx_run_query_static).
+//
+// For callers that must not allocate device memory at call time: code that
+// runs while a CUDA graph is being captured (cudaMalloc is not allowed
+// there), processes whose device memory is carved up and owned by another
+// runtime, and latency-critical loops that cannot afford an allocation's
+// implicit synchronisation.  bfx_run_query allocates its workspace on first
+// use and grows it; this variant keeps every scratch buffer (labels, pending
+// masks, frontier queues, tile table, batch records, launch state) in one
+// file-scope device array of fixed size, so a call allocates nothing.
+// ---------------------------------------------------------------------------
+
+namespace bfx {
+namespace {
+constexpr size_t kStaticScratchBytes = size_t{32} << 20;  // 32 MiB per device
+constexpr int kMaxStaticDevices = 64;
+}  // namespace
+}  // namespace bfx
+
+// Every device that loads libbfx.so holds this array until the process exits.
+// All calls on a device share it, and each call leaves its contents behind:
+// the call re-initialises everything it reads (labels, masks, queues, tile
+// table, counters) before relaxing.
+static __device__ __align__(256) unsigned char bfx_static_scratch[bfx::kStaticScratchBytes];
+
+namespace bfx {
+namespace {
+
+std::mutex g_static_mutex;
+void* g_static_base[kMaxStaticDevices] = {};
+
+// Device address of bfx_static_scratch on the current device, resolved once
+// per device with cudaGetSymbolAddress (the host-side name is only a
+// stand-in; kernels must be given this address).
+cudaError_t static_scratch_base(int device, void** out) {
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (g_static_base[device] == nullptr) {
+    void* p = nullptr;
+    const cudaError_t rc = cudaGetSymbolAddress(&p, bfx_static_scratch);
+    if (rc != cudaSuccess) return rc;
+    g_static_base[device] = p;
+  }
+  *out = g_static_base[device];
+  return cudaSuccess;
+}
+
+// Final label of every target of a width-1 batch: distance bits and the
+// predecessor edge id (0xffffffff for sources and unreached targets).
+__global__ void gather_targets_kernel(DGraph g, const DBatch* batch, const bfx_device_run_status* status,
+                                      u32* out_bits, u32* out_pred) {
+  const DBatch& B = *batch;
+  const u32 slot = status->final_distance_slot;
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < B.tgt_count; i += gridDim.x * blockDim.x) {
+    const u32 v = B.tgt[i];
+    const uint2 t = B.tiles[g.owner[v]];
+    const u64 w = (t.x & 1u) ? B.dist[slot][v - t.y] : dev::kUnreached;
+    const u32 lo = static_cast<u32>(w);
+    out_bits[i] = dev::hi(w);
+    out_pred[i] = (lo == 0u || lo == 0xFFFFFFFFu) ? 0xFFFFFFFFu : lo - 1u;
+  }
+}
+
+void copy_in(char* base, size_t off, const void* src, size_t bytes) {
+  if (bytes) BFX_CUDA(cudaMemcpy(base + off, src, bytes, cudaMemcpyHostToDevice));
+}
+
+}  // namespace
+}  // namespace bfx
+
+extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t source_count, const uint32_t* sources,
+                                    uint32_t target_count, const uint32_t* targets, uint32_t selected_tile_count,
+                                    const uint32_t* selected_tiles, const bfx_gpu_run_options* options,
+                                    bfx_device_run_status* status, uint32_t* target_distance_bits,
+                                    uint32_t* target_predecessor_edges) {
+  return bfx::guarded([&] {
+    using bfx::u32;
+    using bfx::u64;
+    bfx::require(graph && options && status && target_distance_bits && target_predecessor_edges, "null argument");
+    bfx::require(source_count > 0 && target_count > 0, "route queries require sources and targets");
+    bfx::require(sources && targets && selected_tiles && selected_tile_count > 0, "null query array");
+    bfx::validate_options(*options);
+    if (graph->device < 0 || graph->device >= bfx::kMaxStaticDevices) throw std::out_of_range("device index");
+    const std::vector<std::uint32_t>& tvo = graph->tile_vertex_offsets;
+    const u32 T = graph->g.T, V = graph->g.V;
+    u64 U = 0;
+    for (u32 i = 0; i < selected_tile_count; ++i) {
+      const u32 t = selected_tiles[i];
+      if (t >= T) throw std::out_of_range("selected tile out of range");
+      bfx::require(i == 0 || t > selected_tiles[i - 1], "selected tiles must be strictly increasing");
+      U += tvo[t + 1] - tvo[t];
+    }
+    bfx::require(U > 0, "query selects no vertices");
+    auto selected = [&](u32 v) {
+      const u32 owner = static_cast<u32>(std::upper_bound(tvo.begin(), tvo.end(), v) - tvo.begin()) - 1U;
+      return std::binary_search(selected_tiles, selected_tiles + selected_tile_count, owner);
+    };
+    for (u32 i = 0; i < source_count; ++i) {
+      if (sources[i] >= V) throw std::out_of_range("source out of range");
+      bfx::require(i == 0 || sources[i] > sources[i - 1], "noncanonical sources");
+      bfx::require(selected(sources[i]), "terminal owner tile not selected");
+    }
+    for (u32 i = 0; i < target_count; ++i) {
+      if (targets[i] >= V) throw std::out_of_range("target out of range");
+      bfx::require(i == 0 || targets[i] > targets[i - 1], "noncanonical targets");
+      bfx::require(selected(targets[i]), "terminal owner tile not selected");
+    }
+    // Layout inside the static array.
+    const size_t S = source_count, Tg = target_count, R = selected_tile_count;
+    const size_t o_batch = 0;
+    const size_t o_ctl = bfx::align256(o_batch + sizeof(bfx::DBatch));
+    const size_t o_run = bfx::align256(o_ctl + sizeof(bfx::DCtl));
+    const size_t o_ubase = bfx::align256(o_run + sizeof(bfx::DRun));
+    const size_t o_sbase = bfx::align256(o_ubase + 8);
+    const size_t o_status = bfx::align256(o_sbase + 8);
+    const size_t o_ctrl = bfx::align256(o_status + sizeof(bfx_device_run_status));
+    const size_t o_soff = bfx::align256(o_ctrl + sizeof(bfx_device_controller));
+    const size_t o_src = bfx::align256(o_soff + 8);
+    const size_t o_toff = bfx::align256(o_src + S * 4);
+    const size_t o_tgt = bfx::align256(o_toff + 8);
+    const size_t o_ranges = bfx::align256(o_tgt + Tg * 4);
+    const size_t o_roff = bfx::align256(o_ranges + R * 16);
+    const size_t o_out = bfx::align256(o_roff + (R + 1) * 4);
+    const size_t o_dist0 = bfx::align256(o_out + Tg * 8);
+    const size_t o_dist1 = bfx::align256(o_dist0 + U * 8);
+    const size_t o_mask0 = bfx::align256(o_dist1 + U * 8);
+    const size_t o_mask1 = bfx::align256(o_mask0 + U * 4);
+    const size_t o_q0 = bfx::align256(o_mask1 + U * 4);
+    const size_t o_q1 = bfx::align256(o_q0 + U * 4);
+    const size_t o_c2g = bfx::align256(o_q1 + U * 4);
+    const size_t o_tiles = bfx::align256(o_c2g + U * 4);
+    const size_t total = bfx::align256(o_tiles + size_t{T} * 8);
+    if (total > bfx::kStaticScratchBytes) {
+      throw std::overflow_error("query needs more than the 32 MiB static scratch (union of " + std::to_string(U) +
+                                " vertices); use bfx_run_query");
+    }
+    BFX_CUDA(cudaSetDevice(graph->device));
+    void* vbase = nullptr;
+    BFX_CUDA(bfx::static_scratch_base(graph->device, &vbase));
+    char* base = static_cast<char*>(vbase);
+    // Batch record (width 1) pointing into the array.
+    bfx::DBatch B{};
+    B.W = 1;
+    B.shift = 0;
+    B.valid = 1;
+    B.U = static_cast<u32>(U);
+    B.src_count = static_cast<u32>(S);
+    B.tgt_count = static_cast<u32>(Tg);
+    B.range_count = static_cast<u32>(R);
+    B.dist[0] = reinterpret_cast<u64*>(base + o_dist0);
+    B.dist[1] = reinterpret_cast<u64*>(base + o_dist1);
+    B.mask[0] = reinterpret_cast<u32*>(base + o_mask0);
+    B.mask[1] = reinterpret_cast<u32*>(base + o_mask1);
+    B.queue[0] = reinterpret_cast<u32*>(base + o_q0);
+    B.queue[1] = reinterpret_cast<u32*>(base + o_q1);
+    B.c2g = reinterpret_cast<u32*>(base + o_c2g);
+    B.tiles = reinterpret_cast<uint2*>(base + o_tiles);
+    B.src_off = reinterpret_cast<const u32*>(base + o_soff);
+    B.src = reinterpret_cast<const u32*>(base + o_src);
+    B.tgt_off = reinterpret_cast<const u32*>(base + o_toff);
+    B.tgt = reinterpret_cast<const u32*>(base + o_tgt);
+    B.ranges = reinterpret_cast<const uint4*>(base + o_ranges);
+    B.range_off = reinterpret_cast<const u32*>(base + o_roff);
+    const u32 ubase[2] = {0U, static_cast<u32>(U)};
+    const u32 soff[2] = {0U, source_count};
+    const u32 toff[2] = {0U, target_count};
+    bfx::copy_in(base, o_batch, &B, sizeof(B));
+    bfx::copy_in(base, o_ubase, ubase, 8);
+    bfx::copy_in(base, o_sbase, soff, 8);
+    bfx::copy_in(base, o_soff, soff, 8);
+    bfx::copy_in(base, o_src, sources, S * 4);
+    bfx::copy_in(base, o_toff, toff, 8);
+    bfx::copy_in(base, o_tgt, targets, Tg * 4);
+    // Vertex ranges and their compact offsets, streamed through a stack buffer.
+    {
+      constexpr u32 kChunk = 256;
+      uint4 rbuf[kChunk];
+      u32 obuf[kChunk];
+      u32 acc = 0;
+      for (u32 i0 = 0; i0 < R; i0 += kChunk) {
+        const u32 n = std::min<u32>(kChunk, static_cast<u32>(R) - i0);
+        for (u32 k = 0; k < n; ++k) {
+          const u32 t = selected_tiles[i0 + k];
+          rbuf[k] = make_uint4(t, tvo[t], tvo[t + 1], 1U);
+          obuf[k] = acc;
+          acc += tvo[t + 1] - tvo[t];
+        }
+        bfx::copy_in(base, o_ranges + size_t{i0} * 16, rbuf, size_t{n} * 16);
+        bfx::copy_in(base, o_roff + size_t{i0} * 4, obuf, size_t{n} * 4);
+      }
+      bfx::copy_in(base, o_roff + R * 4, &acc, 4);
+    }
+    // The tile table must read 0 outside the selection (the previous call's
+    // entries are still there); everything else is reset by init_kernel.
+    BFX_CUDA(cudaMemset(base + o_tiles, 0, size_t{T} * 8));
+    bfx::LaunchParams p{};
+    p.g = graph->g;
+    p.batches = reinterpret_cast<const bfx::DBatch*>(base + o_batch);
+    p.ctl = reinterpret_cast<bfx::DCtl*>(base + o_ctl);
+    p.run = reinterpret_cast<bfx::DRun*>(base + o_run);
+    p.unit_base = reinterpret_cast<const u32*>(base + o_ubase);
+    p.nb = 1;
+    p.engine = options->engine;
+    p.per_lane = options->enable_per_lane_convergence;
+    p.max_rounds = options->maximum_rounds;
+    int sms = 0;
+    BFX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, graph->device));
+    bfx::init_kernel<<<sms * 8, 256>>>(p);
+    BFX_CUDA(cudaGetLastError());
+    bfx::seed_kernel<<<static_cast<int>((S + 255) / 256), 256>>>(p, reinterpret_cast<const u32*>(base + o_sbase));
+    BFX_CUDA(cudaGetLastError());
+    const int block = static_cast<int>(options->block_size);
+    const size_t smem = 8;
+    int per_sm = 0;
+    BFX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, reinterpret_cast<const void*>(bfx::persistent_kernel<false>), block, smem));
+    if (per_sm <= 0) throw bfx::Error(BFX_ERR_CUDA, "kernel cannot be resident with this block size");
+    if (options->grid_policy == 1u) {
+      if (static_cast<int>(options->blocks_per_wgp) > per_sm)
+        throw std::invalid_argument("blocks per SM exceed the cooperative residency limit");
+      per_sm = static_cast<int>(options->blocks_per_wgp);
+    }
+    void* args[] = {&p};
+    BFX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(bfx::persistent_kernel<false>),
+                                         per_sm * sms, block, args, smem, 0));
+    auto* d_status = reinterpret_cast<bfx_device_run_status*>(base + o_status);
+    bfx::finalize_kernel<<<1, 256>>>(p, reinterpret_cast<bfx_device_controller*>(base + o_ctrl), d_status);
+    BFX_CUDA(cudaGetLastError());
+    u32* out = reinterpret_cast<u32*>(base + o_out);
+    bfx::gather_targets_kernel<<<static_cast<int>((Tg + 255) / 256), 256>>>(graph->g, p.batches, d_status, out,
+                                                                          out + Tg);
+    BFX_CUDA(cudaGetLastError());
+    BFX_CUDA(cudaMemcpy(status, d_status, sizeof(*status), cudaMemcpyDeviceToHost));
+    BFX_CUDA(cudaMemcpy(target_distance_bits, out, Tg * 4, cudaMemcpyDeviceToHost));
+    BFX_CUDA(cudaMemcpy(target_predecessor_edges, out + Tg, Tg * 4, cudaMemcpyDeviceToHost));
+  });
+}

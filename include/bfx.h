@@ -265,6 +265,37 @@ int bfx_run_query(bfx_workspace *ws, uint32_t source_count, const uint32_t *sour
                   uint32_t selected_tile_count, const uint32_t *selected_tiles,
                   const bfx_gpu_run_options *options, bfx_device_run_status *status);
 
+/* ---- single query without device allocation --------------------------------
+ * No counterpart in the reference: a libbfx addition for callers that cannot
+ * allocate device memory when they run a query -- code running inside CUDA
+ * graph capture (cudaMalloc is not permitted there), processes whose device
+ * memory is owned and carved up by another runtime, and latency-critical
+ * loops that cannot afford an allocation's implicit synchronisation.
+ *
+ * Same query semantics and status as bfx_run_query, but every scratch buffer
+ * (labels, pending masks, frontier queues, tile table, batch records, launch
+ * state) lives in one fixed 32 MiB array in the library's device memory, so
+ * the call allocates nothing.  Limits and rules:
+ *  - the whole query image must fit in 32 MiB (about 36 bytes per selected
+ *    vertex plus 8 bytes per graph tile); larger queries fail with
+ *    BFX_ERR_OVERFLOW and a message -- use bfx_run_query for them;
+ *  - every GPU that loads libbfx.so holds the 32 MiB array until exit;
+ *  - the first call on a device resolves the array's device address once
+ *    (cudaGetSymbolAddress); make that first call before any stream capture;
+ *  - all calls on a device share the array and leave their data in it (each
+ *    call re-initialises what it reads); calls that overlap on the GPU --
+ *    from several host threads at once -- race and must be serialised by the
+ *    caller;
+ *  - work runs on the legacy default stream and the call returns after the
+ *    results are on the host.
+ * Outputs: the status, and per target (canonical order) its distance bits and
+ * predecessor stable edge id (0xffffffff for sources and unreached targets). */
+int bfx_run_query_static(const bfx_resident_graph *graph, uint32_t source_count, const uint32_t *sources,
+                         uint32_t target_count, const uint32_t *targets, uint32_t selected_tile_count,
+                         const uint32_t *selected_tiles, const bfx_gpu_run_options *options,
+                         bfx_device_run_status *status, uint32_t *target_distance_bits,
+                         uint32_t *target_predecessor_edges);
+
 #ifdef __cplusplus
 }
 #endif
