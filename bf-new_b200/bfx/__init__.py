@@ -474,6 +474,13 @@ class ResidentDeviceGraph:
         _check(load().bfx_resident_graph_upload(C.byref(v), C.c_int(device), C.byref(h)))
         return cls(h, layout)
 
+    def set_weights(self, weights_by_edge_id) -> None:
+        """Replaces every edge weight on the device (array indexed by stable edge id)."""
+        w = np.ascontiguousarray(weights_by_edge_id, np.float32)
+        if w.shape[0] != self.layout.edge_count:
+            raise ValueError("one weight per edge is required")
+        _check(load().bfx_resident_graph_set_weights(self._h, _ptr(w, f32)))
+
     def info(self) -> dict:
         out = (u64 * 4)()
         _check(load().bfx_resident_graph_info(self._h, out))
@@ -580,6 +587,14 @@ class Workspace:
                 vo += L + 1
                 eo += L
             out.append(d)
+        return out
+
+    def edge_usage_adjoint(self, target_grads) -> np.ndarray:
+        """dL/dw (by stable edge id) for L = sum_t g_t * dist_t over the targets
+        of the last compact_paths() call, in its target order."""
+        g = np.ascontiguousarray(target_grads, np.float32)
+        out = np.zeros(self.graph.layout.edge_count, np.float32)
+        _check(load().bfx_edge_usage_adjoint(self._h, _ptr(g, f32), _ptr(out, f32)))
         return out
 
     WORK_KEYS = ("entries", "records", "active_pairs", "relaxations", "claims", "decreases", "min_reductions",

@@ -150,3 +150,18 @@ def sequential_batches(layout, queries, lane_width: int = 32):
     for i in range(0, len(queries), lane_width):
         out.append(make_description(layout, queries[i:i + lane_width], lane_width))
     return out
+
+
+def shard_batches(lane_edge_estimates, world: int) -> list:
+    """Replica sharding: every rank holds the whole graph, batches are split
+    so each rank gets a near-equal share of estimated lane-edges (greedy
+    longest-first onto the least-loaded rank; ties by rank).  Deterministic,
+    so every rank computes the same assignment without communicating."""
+    order = sorted(range(len(lane_edge_estimates)), key=lambda b: (-int(lane_edge_estimates[b]), b))
+    loads = [0] * world
+    shards = [[] for _ in range(world)]
+    for b in order:
+        r = min(range(world), key=lambda i: (loads[i], i))
+        shards[r].append(b)
+        loads[r] += int(lane_edge_estimates[b])
+    return [sorted(s) for s in shards]

@@ -209,5 +209,6 @@ struct bfx_workspace {
   std::uint64_t path_vertices{0};  // payload sizes after the summaries pass
   std::uint64_t path_edges{0};
   bool paths_ready{false};
+  bfx::DeviceBuffer adjoint;     // per-edge exact accumulators, upstream values, result
 };
 

@@ -1,0 +1,112 @@
+// Frontier push round body (included by engine.cu after the device records).
+//
+// One warp item covers EPW = 32 / S queue entries of one batch: a group of S
+// threads per entry (S = 8 for batches of <= 8 lanes, 32 otherwise).  Within
+// a group the entry's k active lanes are spread over aligned sub-groups of
+// kp = 2^ceil(log2 k) threads, so a group relaxes S / kp edges per step and
+// all groups of the warp step together (the step count is the warp's
+// maximum, so every shuffle has the full warp).
+//
+// Per entry the dependent chain is short: the group leader loads the queue
+// word {vertex, compact index}, the pending lanes and the row bounds in one
+// go and clears the pending lanes with a plain store -- the read slot is
+// only written in the previous round, and every vertex is queued at most
+// once per round, so no atomic is needed.  Each thread pre-reads its
+// destination label and issues a non-returning 64-bit min only for a smaller
+// candidate; success bits are OR-combined per edge; the first lane of the
+// edge ORs them into the next round's pending lanes and the warp claims
+// queue slots with one atomicAdd.
+#pragma once
+
+template <bool kCount, u32 S>
+__device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBatch& B, DCtl& C, u32 item, u32 count,
+                                               u32 rd, u32 widx, Work& wk) {
+  constexpr u32 EPW = 32u / S;
+  const u32 lane = lane_id();
+  const u32 sl = lane & (S - 1u);
+  const u32 leader = lane & ~(S - 1u);
+  const u32 entry = item * EPW + (lane / S);
+  const bool live = entry < count;
+  u32* const mask_r = B.mask[rd];
+  u32 v = 0u, cv = 0u, m = 0u, rb = 0u, re = 0u;
+  if (live && sl == 0u) {
+    const u64 q = dev::ld_cg(B.queue[rd] + entry);
+    v = static_cast<u32>(q);
+    cv = static_cast<u32>(q >> 32);
+    m = dev::ld_cg(mask_r + cv);
+    rb = __ldg(p.g.csr_off + v);
+    re = __ldg(p.g.csr_off + v + 1u);
+    mask_r[cv] = 0u;
+  }
+  v = __shfl_sync(0xFFFFFFFFu, v, static_cast<int>(leader));
+  cv = __shfl_sync(0xFFFFFFFFu, cv, static_cast<int>(leader));
+  m = __shfl_sync(0xFFFFFFFFu, m, static_cast<int>(leader));
+  rb = __shfl_sync(0xFFFFFFFFu, rb, static_cast<int>(leader));
+  re = __shfl_sync(0xFFFFFFFFu, re, static_cast<int>(leader));
+  const u32 k = __popc(m);
+  const u32 s = k <= 1u ? 0u : 32u - __clz(k - 1u);
+  const u32 kp = 1u << s;  // <= S by construction (k <= W <= S)
+  const u32 G = S >> s;    // edges per step for this entry
+  const u32 slot = sl >> s;
+  const u32 j = sl & (kp - 1u);
+  const bool has_lane = live && j < k;
+  if (kCount && live && sl == 0u) {
+    wk.c[0] += 1;
+    wk.c[1] += re - rb;
+    wk.c[2] += k;
+  }
+  u32 ql = 0u, src_bits = dev::kInfBits;
+  if (has_lane) {
+    u32 mm = m;
+    for (u32 t = 0; t < j; ++t) mm &= mm - 1u;  // drop the j lowest active lanes
+    ql = __ffs(mm) - 1u;
+    src_bits = dev::hi(dev::ld_cg(B.dist[0] + ((static_cast<u64>(cv) << B.shift) + ql)));
+  }
+  const u32 steps_mine = live ? (re - rb + G - 1u) / G : 0u;
+  const u32 steps = __reduce_max_sync(0xFFFFFFFFu, steps_mine);
+  u32* const mask_w = B.mask[rd ^ 1u];
+  u64* const queue_w = B.queue[rd ^ 1u];
+  for (u32 st = 0; st < steps; ++st) {
+    const u32 e = rb + st * G + slot;
+    u32 bits = 0u, cdst = 0u, dstv = 0u;
+    if (has_lane && e < re) {
+      const uint4 rec = __ldg(p.g.csr + e);
+      const uint2 dt = B.tiles[rec.w];
+      cdst = rec.x - dt.y;
+      dstv = rec.x;
+      if (((dt.x >> ql) & 1u) && src_bits != dev::kInfBits) {
+        const u64 cand = dev::candidate(src_bits, rec.y, rec.z);
+        u64* const target = B.dist[0] + ((static_cast<u64>(cdst) << B.shift) + ql);
+        const u64 cur = dev::ld_cg(target);
+        if (kCount) wk.c[3] += 1;
+        if (cand < cur) {
+          dev::red_min(target, cand);
+          if (dev::hi(cand) < dev::hi(cur)) bits = 1u << ql;
+          if (kCount) {
+            wk.c[6] += 1;
+            wk.c[5] += bits != 0u;
+          }
+        }
+      }
+    }
+    for (u32 o = 1; o < kp; o <<= 1) bits |= __shfl_xor_sync(0xFFFFFFFFu, bits, o);
+    bool claim = false;
+    if (j == 0u && bits != 0u) claim = atomicOr(mask_w + cdst, bits) == 0u;
+    const u32 cm = __ballot_sync(0xFFFFFFFFu, claim);
+    if (cm != 0u) {
+      const u32 first = __ffs(cm) - 1u;
+      u32 pos = 0u;
+      if (lane == first) pos = atomicAdd(&C.count[widx], static_cast<u32>(__popc(cm)));
+      pos = __shfl_sync(0xFFFFFFFFu, pos, static_cast<int>(first));
+      if (claim) {
+        if (kCount) wk.c[4] += 1;
+        const u32 at = pos + __popc(cm & ((1u << lane) - 1u));
+        if (at < B.U) {
+          queue_w[at] = static_cast<u64>(dstv) | (static_cast<u64>(cdst) << 32);
+        } else {
+          atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
+        }
+      }
+    }
+  }
+}

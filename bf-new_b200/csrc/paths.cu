@@ -281,9 +281,171 @@ __global__ void payload_kernel(PathArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Edge-usage adjoint (no reference counterpart).  For L = sum_t g_t * d_t over
+// the targets' shortest paths, dL/dw_e = sum of g_t over the targets whose
+// path uses edge e.  Paths are recomputed from the final labels (predecessor
+// walk, or the backtracking search for flagged targets); nothing per round is
+// stored.  Contributions are summed exactly in per-edge fixed point (least
+// significant bit 2^-63, four 32-bit digits in 64-bit atomics) and rounded
+// once to float (nearest, ties to even), so the result does not depend on
+// the order in which threads add -- and equals an exact CPU tree walk.
+// Accepted upstream values: 0 or 2^-40 <= |g| < 2^40 (checked on the host).
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void exact_add(unsigned long long* acc, float g) {
+  const u32 bits = __float_as_uint(g);
+  const u32 ex = (bits >> 23) & 0xFFu;
+  if (ex == 0u) return;
+  const u64 m = static_cast<u64>((bits & 0x7FFFFFu) | 0x800000u);  // g = m * 2^(ex-150)
+  const u32 b = ex - 87u;                                         // bit of m's lsb at 2^-63
+  const u64 v = m << (b & 31u);
+  u64 lo = v & 0xFFFFFFFFull, hi = v >> 32;
+  if (bits >> 31) {
+    lo = 0ull - lo;
+    hi = 0ull - hi;
+  }
+  atomicAdd(acc + (b >> 5), lo);
+  if (hi != 0ull) atomicAdd(acc + (b >> 5) + 1u, hi);
+}
+
+__device__ float exact_round(const unsigned long long* acc) {
+  long long carry = 0;
+  u32 dig[4];
+  for (int d = 0; d < 4; ++d) {
+    const long long x = static_cast<long long>(acc[d]) + carry;
+    dig[d] = static_cast<u32>(x);
+    carry = x >> 32;
+  }
+  const bool neg = carry < 0;
+  u64 lo = (static_cast<u64>(dig[1]) << 32) | dig[0];
+  u64 hi = (static_cast<u64>(dig[3]) << 32) | dig[2];
+  if (neg) {
+    lo = ~lo + 1ull;
+    hi = ~hi + (lo == 0ull ? 1ull : 0ull);
+  }
+  if (hi == 0ull && lo == 0ull) return 0.0f;
+  const int p = hi ? 127 - __clzll(static_cast<long long>(hi)) : 63 - __clzll(static_cast<long long>(lo));
+  u64 mant;
+  int shift = 0;
+  if (p <= 23) {
+    mant = lo;
+  } else {
+    shift = p - 23;
+    // mant = bits [shift, shift + 24); guard = bit shift - 1; sticky = bits below.
+    auto bit_range = [&](int from, int count) -> u64 {  // count <= 64
+      u64 r;
+      if (from >= 64) {
+        r = hi >> (from - 64);
+      } else if (from == 0) {
+        r = lo;
+      } else {
+        r = (lo >> from) | (hi << (64 - from));
+      }
+      return count >= 64 ? r : (r & ((1ull << count) - 1ull));
+    };
+    mant = bit_range(shift, 24);
+    const u64 guard = bit_range(shift - 1, 1);
+    bool sticky = false;
+    if (shift - 1 > 0) {
+      const int n = shift - 1;
+      sticky = n >= 64 ? (lo != 0ull || (hi & ((1ull << (n - 64)) - 1ull)) != 0ull)
+                       : (lo & ((1ull << n) - 1ull)) != 0ull;
+    }
+    if (guard && (sticky || (mant & 1ull))) {
+      ++mant;
+      if (mant == (1ull << 24)) {
+        mant >>= 1;
+        ++shift;
+      }
+    }
+  }
+  const float r = ldexpf(static_cast<float>(mant), shift - 63);
+  return neg ? -r : r;
+}
+
+__global__ void adjoint_walk_kernel(PathArgs a, const float* grads, unsigned long long* acc) {
+  const u32 total = a.target_base[a.batch_count];
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    if ((a.lengths[i] & kFallback) != 0u || a.summaries[i].reconstruction != 0u) continue;
+    const float g = grads[i];
+    if (g == 0.0f) continue;
+    const u32 bi = find_b(a.target_base, a.batch_count, i);
+    const u32 b = a.first_batch + bi;
+    const DBatch& B = a.batches[b];
+    const u32 pos = i - a.target_base[bi];
+    const u32 lane = lane_of(B.tgt_off, B.W, pos);
+    const u64* d = B.dist[a.status[b].final_distance_slot];
+    u64 w = label(a.g, B, d, B.tgt[pos], lane);
+    while (static_cast<u32>(w) != 0u) {
+      const u32 e = static_cast<u32>(w) - 1u;
+      exact_add(acc + 4ull * e, g);
+      w = label(a.g, B, d, a.g.eid_src[e], lane);
+    }
+  }
+}
+
+__global__ void adjoint_search_kernel(PathArgs a, const float* grads, unsigned long long* acc) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const u32 total = a.target_base[a.batch_count];
+  for (u32 i = 0; i < total; ++i) {
+    if ((a.lengths[i] & kFallback) == 0u || a.summaries[i].reconstruction != 0u || grads[i] == 0.0f) continue;
+    const u32 bi = find_b(a.target_base, a.batch_count, i);
+    const u32 b = a.first_batch + bi;
+    const DBatch& B = a.batches[b];
+    const u32 pos = i - a.target_base[bi];
+    const u32 lane = lane_of(B.tgt_off, B.W, pos);
+    const u64* d = B.dist[a.status[b].final_distance_slot];
+    const u32 n = search_target(a, B, d, B.tgt[pos], lane);
+    for (u32 k = 1; k <= n && n != 0xFFFFFFFFu; ++k) exact_add(acc + 4ull * a.stack_e[k], grads[i]);
+  }
+}
+
+__global__ void adjoint_round_kernel(u32 E, const unsigned long long* acc, float* grad) {
+  for (u32 e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+    grad[e] = exact_round(acc + 4ull * e);
+  }
+}
+
 void check_ready(bfx_workspace* ws) {
   require(ws != nullptr, "null workspace");
   require(ws->executed, "no executed batches");
+}
+
+// PathArgs over the workspace's path buffer for the batches of the last
+// summaries pass (same layout the summaries pass wrote).
+PathArgs path_args(bfx_workspace* ws) {
+  const std::uint64_t T = ws->path_targets;
+  const std::uint32_t batch_count = ws->path_batch_count;
+  std::uint32_t max_union = 0;
+  for (std::uint32_t i = 0; i < batch_count; ++i) max_union = std::max(max_union, ws->batches[ws->path_first_batch + i].U);
+  char* base = static_cast<char*>(ws->paths.ptr);
+  const size_t o_tb = 0;
+  const size_t o_sum = align256(o_tb + (batch_count + 1) * 4);
+  const size_t o_len = align256(o_sum + T * sizeof(bfx_compact_target_summary));
+  const size_t o_vo = align256(o_len + T * 4);
+  const size_t o_eo = align256(o_vo + T * 8);
+  const size_t o_sv = align256(o_eo + T * 8);
+  const size_t o_sc = align256(o_sv + (size_t{max_union} + 1) * 4);
+  const size_t o_se = align256(o_sc + (size_t{max_union} + 1) * 4);
+  const size_t o_op = align256(o_se + (size_t{max_union} + 1) * 4);
+  PathArgs a{};
+  a.g = ws->graph->g;
+  a.batches = ws->params.batches;
+  a.status = ws->d_status;
+  a.first_batch = ws->path_first_batch;
+  a.batch_count = batch_count;
+  a.target_base = reinterpret_cast<const std::uint32_t*>(base + o_tb);
+  a.summaries = reinterpret_cast<bfx_compact_target_summary*>(base + o_sum);
+  a.lengths = reinterpret_cast<std::uint32_t*>(base + o_len);
+  a.vertex_offsets = reinterpret_cast<const std::uint64_t*>(base + o_vo);
+  a.edge_offsets = reinterpret_cast<const std::uint64_t*>(base + o_eo);
+  a.stack_v = reinterpret_cast<std::uint32_t*>(base + o_sv);
+  a.stack_c = reinterpret_cast<std::uint32_t*>(base + o_sc);
+  a.stack_e = reinterpret_cast<std::uint32_t*>(base + o_se);
+  a.on_path = reinterpret_cast<std::uint32_t*>(base + o_op);
+  a.max_union = max_union;
+  return a;
 }
 
 }  // namespace
@@ -442,3 +604,80 @@ int bfx_compact_path_payload(bfx_workspace* ws, uint32_t* vertices, float* dista
 }
 
 }  // extern "C"
+
+extern "C" int bfx_edge_usage_adjoint(bfx_workspace* ws, const float* target_grads, float* edge_grads) {
+  return bfx::guarded([&] {
+    bfx::check_ready(ws);
+    bfx::require(ws->paths_ready, "call bfx_compact_path_summaries first");
+    bfx::require(edge_grads != nullptr && (target_grads != nullptr || ws->path_targets == 0), "null argument");
+    const std::uint64_t T = ws->path_targets;
+    const std::uint32_t E = ws->graph->g.E;
+    for (std::uint64_t i = 0; i < T; ++i) {
+      const float g = target_grads[i];
+      const float a = g < 0 ? -g : g;
+      bfx::require(g == 0.0f || (a >= 0x1p-40f && a < 0x1p40f),
+                   "upstream gradients must be 0 or have magnitude in [2^-40, 2^40)");
+    }
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    const size_t o_acc = 0;
+    const size_t o_g = bfx::align256(o_acc + size_t{E} * 32);
+    const size_t o_out = bfx::align256(o_g + T * 4);
+    const size_t total = bfx::align256(o_out + size_t{E} * 4);
+    ws->adjoint.reserve(total, ws->graph->device);
+    char* base = static_cast<char*>(ws->adjoint.ptr);
+    auto* acc = reinterpret_cast<unsigned long long*>(base + o_acc);
+    auto* g = reinterpret_cast<float*>(base + o_g);
+    auto* out = reinterpret_cast<float*>(base + o_out);
+    BFX_CUDA(cudaMemsetAsync(acc, 0, size_t{E} * 32, ws->stream));
+    if (T) BFX_CUDA(cudaMemcpyAsync(g, target_grads, T * 4, cudaMemcpyHostToDevice, ws->stream));
+    const bfx::PathArgs a = bfx::path_args(ws);
+    if (T) {
+      const int blocks = static_cast<int>(std::min<std::uint64_t>((T + 255) / 256, 4096));
+      bfx::adjoint_walk_kernel<<<blocks, 256, 0, ws->stream>>>(a, g, acc);
+      BFX_CUDA(cudaGetLastError());
+      bfx::adjoint_search_kernel<<<1, 1, 0, ws->stream>>>(a, g, acc);
+      BFX_CUDA(cudaGetLastError());
+    }
+    bfx::adjoint_round_kernel<<<std::max(1, std::min<int>((E + 255) / 256, 8192)), 256, 0, ws->stream>>>(E, acc, out);
+    BFX_CUDA(cudaGetLastError());
+    BFX_CUDA(cudaMemcpyAsync(edge_grads, out, size_t{E} * 4, cudaMemcpyDeviceToHost, ws->stream));
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+  });
+}
+
+namespace bfx {
+namespace {
+
+__global__ void set_weights_kernel(uint4* csr, uint4* csc, u32 E, const float* w) {
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < E; i += gridDim.x * blockDim.x) {
+    csr[i].y = __float_as_uint(w[csr[i].z - 1u]);
+    csc[i].y = __float_as_uint(w[csc[i].z - 1u]);
+  }
+}
+
+}  // namespace
+}  // namespace bfx
+
+extern "C" int bfx_resident_graph_set_weights(bfx_resident_graph* graph, const float* weights_by_edge_id) {
+  return bfx::guarded([&] {
+    bfx::require(graph && weights_by_edge_id, "null argument");
+    const std::uint32_t E = graph->g.E;
+    std::vector<float> w(weights_by_edge_id, weights_by_edge_id + E);
+    for (float& x : w) {
+      if (!(x >= 0.0f) || x == __builtin_inff()) throw std::invalid_argument("edge weights must be finite and nonnegative");
+      if (x == 0.0f) x = 0.0f;  // canonical +0 (InputGraph canonicalisation)
+    }
+    BFX_CUDA(cudaSetDevice(graph->device));
+    float* d = nullptr;
+    BFX_CUDA(cudaMalloc(reinterpret_cast<void**>(&d), size_t{E} * 4 + 4));
+    cudaError_t err = cudaMemcpy(d, w.data(), size_t{E} * 4, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess && E) {
+      bfx::set_weights_kernel<<<std::min<int>((E + 255) / 256, 8192), 256>>>(const_cast<uint4*>(graph->g.csr),
+                                                                           const_cast<uint4*>(graph->g.csc), E, d);
+      err = cudaGetLastError();
+      if (err == cudaSuccess) err = cudaDeviceSynchronize();
+    }
+    cudaFree(d);
+    BFX_CUDA(err);
+  });
+}

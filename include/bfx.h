@@ -245,6 +245,21 @@ int bfx_compact_path_summaries(bfx_workspace *ws, uint32_t first_batch, uint32_t
  * path_length stable edge ids. */
 int bfx_compact_path_payload(bfx_workspace *ws, uint32_t *vertices, float *distance_labels, uint32_t *edge_ids);
 
+/* ---- edge-usage adjoint ------------------------------------------------------
+ * No counterpart in the reference (a new differentiable interface).  For
+ * L = sum_t g_t * dist_t over the targets of the last
+ * bfx_compact_path_summaries call (g in its summary order), writes
+ * edge_grads[e] = dL/dw_e = sum of g_t over the targets whose path uses the
+ * edge with stable id e (E entries).  Paths are recomputed from the final
+ * labels (no per-round state is kept); contributions are summed exactly and
+ * rounded once to float, so the result is independent of thread order.
+ * Accepted g: 0 or magnitude in [2^-40, 2^40); targets that are not
+ * complete (unreachable, failed lanes) contribute nothing. */
+int bfx_edge_usage_adjoint(bfx_workspace *ws, const float *target_grads, float *edge_grads);
+/* Replaces every edge weight of the resident graph; weights_by_edge_id[E] is
+ * indexed by stable edge id, finite and non-negative (-0 becomes +0). */
+int bfx_resident_graph_set_weights(bfx_resident_graph *graph, const float *weights_by_edge_id);
+
 /* Kernels launched by the most recent bfx_execute (its own kernels only). */
 int bfx_last_launch_count(bfx_workspace *ws, uint64_t *launches);
 

@@ -272,16 +272,70 @@ int oracle_compact_path(const oracle_graph *g, const oracle_query *q, const uint
   return status;
 }
 
-/* Edge usage: for each path p (in the given order) and each edge on it,
- * grad[edge] += g_p.  Sequential float adds in path order per edge. */
-int oracle_edge_usage_adjoint(uint32_t edge_count, uint32_t path_count, const uint32_t *path_offsets,
-                              const uint32_t *paths, const float *gvals, float *grad) {
-  for (uint32_t p = 0; p < path_count; ++p) {
-    for (uint32_t k = path_offsets[p]; k < path_offsets[p + 1]; ++k) {
-      const uint32_t e = paths[k];
-      if (e >= edge_count) return -1;
-      grad[e] = grad[e] + gvals[p];
+/* Correctly rounded (nearest, ties to even) float of the exact value
+ * n * 2^-63, n a signed 128-bit integer. */
+static float round_fixed63(__int128 n) {
+  if (n == 0) return 0.0f;
+  const int neg = n < 0;
+  unsigned __int128 m = neg ? (unsigned __int128)(-n) : (unsigned __int128)n;
+  int p = 127;
+  while (((m >> p) & 1) == 0) --p;
+  int shift = 0;
+  uint64_t mant;
+  if (p <= 23) {
+    mant = (uint64_t)m;
+  } else {
+    shift = p - 23;
+    mant = (uint64_t)((m >> shift) & 0xFFFFFF);
+    const int guard = (int)((m >> (shift - 1)) & 1);
+    const int sticky = shift > 1 && (m & (((unsigned __int128)1 << (shift - 1)) - 1)) != 0;
+    if (guard && (sticky || (mant & 1))) {
+      ++mant;
+      if (mant == (1u << 24)) {
+        mant >>= 1;
+        ++shift;
+      }
     }
   }
-  return 0;
+  const float r = ldexpf((float)mant, shift - 63);
+  return neg ? -r : r;
+}
+
+/* Edge usage over explicit paths: grad[e] = sum over paths p using e of g_p,
+ * summed exactly (fixed point with lsb 2^-63) and rounded once to float --
+ * the contract of the device adjoint, independent of summation order.
+ * g values must be 0 or have magnitude in [2^-40, 2^40).  grad[E] is
+ * overwritten. */
+int oracle_edge_usage_adjoint(uint32_t edge_count, uint32_t path_count, const uint32_t *path_offsets,
+                              const uint32_t *paths, const float *gvals, float *grad) {
+  __int128 *acc = (__int128 *)calloc(edge_count ? edge_count : 1, sizeof(__int128));
+  if (!acc) return -1;
+  int rc = 0;
+  for (uint32_t p = 0; p < path_count && rc == 0; ++p) {
+    const float g = gvals[p];
+    if (g == 0.0f) continue;
+    const float a = fabsf(g);
+    if (!(a >= 0x1p-40f && a < 0x1p40f)) {
+      rc = -2;
+      break;
+    }
+    const uint32_t bits = f_to_bits(g);
+    const int ex = (int)((bits >> 23) & 0xFF);
+    const __int128 m = (__int128)((bits & 0x7FFFFF) | 0x800000);
+    __int128 v = m << (ex - 87); /* g * 2^63 exactly */
+    if (bits >> 31) v = -v;
+    for (uint32_t k = path_offsets[p]; k < path_offsets[p + 1]; ++k) {
+      const uint32_t e = paths[k];
+      if (e >= edge_count) {
+        rc = -1;
+        break;
+      }
+      acc[e] += v;
+    }
+  }
+  if (rc == 0) {
+    for (uint32_t e = 0; e < edge_count; ++e) grad[e] = round_fixed63(acc[e]);
+  }
+  free(acc);
+  return rc;
 }

@@ -56,10 +56,11 @@ int oracle_region_sssp_many(const oracle_graph *g, uint32_t nq, const oracle_que
 int oracle_compact_path(const oracle_graph *g, const oracle_query *q, const uint32_t *dist_bits, uint32_t target,
                         uint32_t cap, uint32_t *vertices, uint32_t *edge_ids, uint32_t *length);
 
-/* Edge-usage adjoint over the predecessor forest: grad[e] += g_t for every
- * edge on the path of every target t, summed per edge in (query, target)
- * order with float adds.  paths: concatenated edge ids, path_offsets[n+1],
- * gvals[n].  grad[E] is accumulated into. */
+/* Edge-usage adjoint over explicit target paths: grad[e] = sum of g_t over
+ * the paths using edge e, summed exactly and rounded once to float (the
+ * device adjoint's contract; order independent).  paths: concatenated edge
+ * ids, path_offsets[n+1], gvals[n] (0 or |g| in [2^-40, 2^40)).  grad[E] is
+ * overwritten.  Returns 0, -1 on a bad edge id, -2 on an out-of-range g. */
 int oracle_edge_usage_adjoint(uint32_t edge_count, uint32_t path_count, const uint32_t *path_offsets,
                               const uint32_t *paths, const float *gvals, float *grad);
 

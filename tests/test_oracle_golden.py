@@ -107,8 +107,31 @@ def test_oracle_matches_reference_on_synthetic_c1():
                 eo += int(ln)
 
 
-def test_oracle_adjoint_sums_in_path_order():
-    orc_lib = Oracle.from_layout(load_case(fixture_paths()[0]).layout)
-    grad = orc_lib.edge_usage_adjoint(5, [np.array([0, 2], np.uint32), np.array([2, 4], np.uint32)],
-                                      np.array([0.25, 0.5], np.float32))
+def exact_round_f32(n: int) -> np.float32:
+    """Nearest-even float32 of n * 2^-63 (independent restatement for the test)."""
+    from fractions import Fraction
+    x = Fraction(n, 1 << 63)
+    f = np.float32(float(x))
+    # correct the double rounding step, if any, by checking neighbours
+    cands = [f, np.nextafter(f, np.float32(np.inf)), np.nextafter(f, np.float32(-np.inf))]
+    best = min(cands, key=lambda c: (abs(Fraction(float(c)) - x), int(np.float32(c).view(np.uint32)) & 1))
+    return np.float32(best)
+
+
+def test_oracle_adjoint_is_exact_and_order_free():
+    orc = Oracle.from_layout(load_case(fixture_paths()[0]).layout)
+    grad = orc.edge_usage_adjoint(5, [np.array([0, 2], np.uint32), np.array([2, 4], np.uint32)],
+                                  np.array([0.25, 0.5], np.float32))
     np.testing.assert_array_equal(grad, np.array([0.25, 0, 0.75, 0, 0.5], np.float32))
+    rng = np.random.default_rng(3)
+    g = (rng.random(400, dtype=np.float32) * np.float32(3)).astype(np.float32) + np.float32(1e-6)
+    g[::7] *= np.float32(-1)
+    paths = [rng.integers(0, 9, size=rng.integers(1, 6)).astype(np.uint32) for _ in range(400)]
+    paths = [np.unique(p) for p in paths]
+    grad = orc.edge_usage_adjoint(9, paths, g)
+    order = rng.permutation(400)
+    grad2 = orc.edge_usage_adjoint(9, [paths[i] for i in order], g[order])
+    np.testing.assert_array_equal(grad, grad2)
+    for e in range(9):
+        n = sum(int(np.float32(gv).astype(np.float64) * 2 ** 63) for gv, p in zip(g, paths) if e in p)
+        assert grad[e] == exact_round_f32(n)
