@@ -209,7 +209,7 @@ __global__ void seed_kernel(LaunchParams p, const u32* src_base) {
       if (old == 0u) {
         const u32 slot = atomicAdd(&p.ctl[b].count[0], 1u);
         if (slot < B.U) {
-          B.queue[0][slot] = v;
+          B.queue[0][slot] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
         } else {
           atomicOr(&p.ctl[b].error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
         }
@@ -218,90 +218,8 @@ __global__ void seed_kernel(LaunchParams p, const u32* src_base) {
   }
 }
 
-// ---------------------------------------------------------------------------
-// Frontier push: one warp per (batch, vertex) queue entry.
-// ---------------------------------------------------------------------------
-
-template <bool kCount>
-__device__ __forceinline__ void frontier_entry(const LaunchParams& p, const DBatch& B, DCtl& C, u32 v, u32 rd,
-                                               u32 widx, Work& wk) {
-  const u32 lane = lane_id();
-  const u32 st = __ldg(p.g.owner + v);
-  const uint2 sti = B.tiles[st];
-  const u32 cv = v - sti.y;
-  u32 m = 0;
-  if (lane == 0) m = atomicExch(&B.mask[rd][cv], 0u);
-  m = __shfl_sync(0xFFFFFFFFu, m, 0) & sti.x;
-  if (m == 0u) return;
-  const u32 k = __popc(m);
-  const u32 rb = __ldg(p.g.csr_off + v), re = __ldg(p.g.csr_off + v + 1);
-  if (kCount && lane == 0) {
-    wk.c[0] += 1;
-    wk.c[1] += re - rb;
-    wk.c[2] += k;
-  }
-  const u32 s = k <= 1u ? 0u : 32u - __clz(k - 1u);  // group = 2^s lanes per edge
-  const u32 kp = 1u << s;
-  const u32 slot = lane >> s;
-  const u32 j = lane & (kp - 1u);
-  const u32 G = 32u >> s;  // edges per warp iteration
-  const bool has_lane = j < k;
-  u32 ql = 0, src_bits = dev::kInfBits;
-  if (has_lane) {
-    u32 mm = m;
-    for (u32 t = 0; t < j; ++t) mm &= mm - 1u;  // drop the j lowest active lanes
-    ql = __ffs(mm) - 1u;
-    src_bits = dev::hi(dev::ld_cg(B.dist[0] + ((static_cast<u64>(cv) << B.shift) + ql)));
-  }
-  u32* const mask_w = B.mask[rd ^ 1u];
-  u32* const queue_w = B.queue[rd ^ 1u];
-  for (u32 base = rb; base < re; base += G) {
-    const u32 e = base + slot;
-    u32 bits = 0u, cdst = 0u, dstv = 0u;
-    if (e < re && has_lane) {
-      const uint4 rec = __ldg(p.g.csr + e);
-      const uint2 dt = B.tiles[rec.w];
-      cdst = rec.x - dt.y;
-      dstv = rec.x;
-      if (((dt.x >> ql) & 1u) && src_bits != dev::kInfBits) {
-        const u64 cand = dev::candidate(src_bits, rec.y, rec.z);
-        u64* const target = B.dist[0] + ((static_cast<u64>(cdst) << B.shift) + ql);
-        const u64 cur = dev::ld_cg(target);
-        if (kCount) wk.c[3] += 1;
-        if (cand < cur) {
-          dev::red_min(target, cand);
-          if (dev::hi(cand) < dev::hi(cur)) bits = 1u << ql;
-          if (kCount) {
-            wk.c[6] += 1;
-            wk.c[5] += bits != 0u;
-          }
-        }
-      }
-    }
-    for (u32 o = 1; o < kp; o <<= 1) bits |= __shfl_xor_sync(0xFFFFFFFFu, bits, o);
-    bool claim = false;
-    if (j == 0u && bits != 0u) {
-      const u32 old = atomicOr(mask_w + cdst, bits);
-      claim = old == 0u;
-    }
-    const u32 cm = __ballot_sync(0xFFFFFFFFu, claim);
-    if (cm != 0u) {
-      const u32 leader = __ffs(cm) - 1u;
-      u32 pos = 0;
-      if (lane == leader) pos = atomicAdd(&C.count[widx], static_cast<u32>(__popc(cm)));
-      pos = __shfl_sync(0xFFFFFFFFu, pos, static_cast<int>(leader));
-      if (claim) {
-        if (kCount) wk.c[4] += 1;
-        const u32 at = pos + __popc(cm & ((1u << lane) - 1u));
-        if (at < B.U) {
-          queue_w[at] = dstv;
-        } else {
-          atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
-        }
-      }
-    }
-  }
-}
+// Frontier push (see frontier.cuh).
+#include "frontier.cuh"
 
 // ---------------------------------------------------------------------------
 // Jacobi pull: lane = query lane, 32/W destination vertices per warp.
@@ -420,7 +338,10 @@ __device__ __forceinline__ u32 batch_exec(const LaunchParams& p, u32 b, u32 ridx
 __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
   const u32 ridx = r % 3u, widx = (r + 1u) % 3u;
   if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
-    block_prefix(prefix, p.nb, [&](u32 b) { return min(dev::ld_cg(&p.ctl[b].count[ridx]), p.batches[b].U); });
+    block_prefix(prefix, p.nb, [&](u32 b) {
+      const u32 n = min(dev::ld_cg(&p.ctl[b].count[ridx]), p.batches[b].U);
+      return p.batches[b].W <= 8u ? (n + 3u) >> 2 : n;  // warp items: 4 or 1 entries each
+    });
   } else {
     block_prefix(prefix, p.nb, [&](u32 b) {
       const DBatch& B = p.batches[b];
@@ -443,8 +364,12 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
     DCtl& C = p.ctl[b];
     const u32 item = w - prefix[b];
     if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
-      const u32 v = dev::ld_cg(B.queue[r & 1u] + item);
-      frontier_entry<kCount>(p, B, C, v, r & 1u, widx, wk);
+      const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
+      if (B.W <= 8u) {
+        frontier_group<kCount, 8>(p, B, C, item, n, r & 1u, widx, wk);
+      } else {
+        frontier_group<kCount, 32>(p, B, C, item, n, r & 1u, widx, wk);
+      }
     } else if (p.engine == BFX_ENGINE_JACOBI_PULL) {
       jacobi_item<kCount>(p, B, C, item, r, widx, wk);
     } else {
@@ -477,7 +402,7 @@ __device__ void flush_work(const LaunchParams& p, Work& wk) {
 }
 
 template <bool kCount>
-__global__ void __launch_bounds__(1024) persistent_kernel(LaunchParams p) {
+__global__ void __launch_bounds__(512, 3) persistent_kernel(LaunchParams p) {
   extern __shared__ u32 prefix[];
   const u32 nblocks = gridDim.x;
   Work wk;
@@ -503,7 +428,7 @@ __global__ void __launch_bounds__(1024) persistent_kernel(LaunchParams p) {
 
 // Host-poll modes: one round per launch over a fixed grid ...
 template <bool kCount>
-__global__ void __launch_bounds__(1024) round_kernel(LaunchParams p) {
+__global__ void __launch_bounds__(512, 3) round_kernel(LaunchParams p) {
   extern __shared__ u32 prefix[];
   if (dev::ld_cg(&p.run->done) != 0u) return;
   const u32 r = dev::ld_cg(&p.run->round);
@@ -977,7 +902,8 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
     for (std::uint32_t b = 0; b < count; ++b) {
       arena_off[b] = arena_total;
       const size_t U = sz[b].U;
-      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 5 + bfx::align256(size_t{g.T} * 8);
+      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 3 + bfx::align256(U * 8) * 2 +
+                     bfx::align256(size_t{g.T} * 8);
     }
     const bool grew = meta_total > ws->meta.bytes || arena_total > ws->arena.bytes;
     ws->meta.reserve(meta_total, ws->graph->device);
@@ -1033,10 +959,10 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
       a += bfx::align256(U * 4);
       B.mask[1] = reinterpret_cast<std::uint32_t*>(a);
       a += bfx::align256(U * 4);
-      B.queue[0] = reinterpret_cast<std::uint32_t*>(a);
-      a += bfx::align256(U * 4);
-      B.queue[1] = reinterpret_cast<std::uint32_t*>(a);
-      a += bfx::align256(U * 4);
+      B.queue[0] = reinterpret_cast<bfx::u64*>(a);
+      a += bfx::align256(U * 8);
+      B.queue[1] = reinterpret_cast<bfx::u64*>(a);
+      a += bfx::align256(U * 8);
       B.c2g = reinterpret_cast<std::uint32_t*>(a);
       a += bfx::align256(U * 4);
       B.tiles = reinterpret_cast<uint2*>(a);
@@ -1083,7 +1009,7 @@ void validate_options(const bfx_gpu_run_options& o) {
   if (o.engine > 2u) throw std::invalid_argument("invalid engine");
   if (o.control_mode > 2u) throw std::invalid_argument("invalid control mode");
   if (o.rounds_per_chunk == 0u) throw std::invalid_argument("invalid rounds per chunk");
-  if (o.block_size == 0u || o.block_size % 32u != 0u || o.block_size > 1024u)
+  if (o.block_size == 0u || o.block_size % 32u != 0u || o.block_size > 512u)
     throw std::invalid_argument("invalid block size");
   if (o.grid_policy > 1u) throw std::invalid_argument("invalid grid policy");
   if (o.grid_policy == 1u && o.blocks_per_wgp == 0u) throw std::invalid_argument("invalid blocks per SM");
@@ -1488,8 +1414,8 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
     const size_t o_mask0 = bfx::align256(o_dist1 + U * 8);
     const size_t o_mask1 = bfx::align256(o_mask0 + U * 4);
     const size_t o_q0 = bfx::align256(o_mask1 + U * 4);
-    const size_t o_q1 = bfx::align256(o_q0 + U * 4);
-    const size_t o_c2g = bfx::align256(o_q1 + U * 4);
+    const size_t o_q1 = bfx::align256(o_q0 + U * 8);
+    const size_t o_c2g = bfx::align256(o_q1 + U * 8);
     const size_t o_tiles = bfx::align256(o_c2g + U * 4);
     const size_t total = bfx::align256(o_tiles + size_t{T} * 8);
     if (total > bfx::kStaticScratchBytes) {
@@ -1513,8 +1439,8 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
     B.dist[1] = reinterpret_cast<u64*>(base + o_dist1);
     B.mask[0] = reinterpret_cast<u32*>(base + o_mask0);
     B.mask[1] = reinterpret_cast<u32*>(base + o_mask1);
-    B.queue[0] = reinterpret_cast<u32*>(base + o_q0);
-    B.queue[1] = reinterpret_cast<u32*>(base + o_q1);
+    B.queue[0] = reinterpret_cast<u64*>(base + o_q0);
+    B.queue[1] = reinterpret_cast<u64*>(base + o_q1);
     B.c2g = reinterpret_cast<u32*>(base + o_c2g);
     B.tiles = reinterpret_cast<uint2*>(base + o_tiles);
     B.src_off = reinterpret_cast<const u32*>(base + o_soff);

@@ -47,7 +47,7 @@ struct DBatch {
   u32 src_count, tgt_count, range_count, reserved;
   u64* dist[2];        // [U*W] labels (slot 1 only for Jacobi)
   u32* mask[2];        // [U] pending lane masks (frontier)
-  u32* queue[2];       // [U] frontier vertices (global ids)
+  u64* queue[2];       // [U] frontier entries {vertex, compact index << 32}
   u32* c2g;            // [U] compact -> global vertex
   uint2* tiles;        // [T] {lane mask, compact bias}
   const u32* src_off;  // [W+1]

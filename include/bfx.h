@@ -291,7 +291,7 @@ int bfx_run_query(bfx_workspace *ws, uint32_t source_count, const uint32_t *sour
  * (labels, pending masks, frontier queues, tile table, batch records, launch
  * state) lives in one fixed 32 MiB array in the library's device memory, so
  * the call allocates nothing.  Limits and rules:
- *  - the whole query image must fit in 32 MiB (about 36 bytes per selected
+ *  - the whole query image must fit in 32 MiB (about 44 bytes per selected
  *    vertex plus 8 bytes per graph tile); larger queries fail with
  *    BFX_ERR_OVERFLOW and a message -- use bfx_run_query for them;
  *  - every GPU that loads libbfx.so holds the 32 MiB array until exit;
