@@ -39,6 +39,7 @@ for _p in (REPO, REPO / "bf-new_b200"):
 import numpy as np  # noqa: E402
 
 METRIC = "batched SSSP queries/s (256 uneven regional queries, 2.1M V / 16.8M E, one persistent launch)"
+METRIC_C3 = "batched SSSP queries/s (64 full-graph sources, 16.8M V / 168M E, one persistent launch)"
 
 
 def log(*a):
@@ -171,9 +172,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="bfx", choices=["bfx", "reference"])
-    ap.add_argument("--engine", default="frontier", choices=["frontier", "jacobi", "dense"])
+    ap.add_argument("--engine", default="auto", choices=["auto", "frontier", "jacobi", "dense"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--queries", type=int, default=256)
+    ap.add_argument("--queries", type=int, default=None)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -195,12 +197,21 @@ def main():
     from bfx import workloads
 
     t0 = time.time()
-    g, order, gstats = bfx.synth_graph(**workloads.GRAPHS["c2"])
+    g, order, gstats = bfx.synth_graph(**workloads.GRAPHS[args.workload])
     layout = bfx.build_device_graph_layout(g, order)
-    grid = (128, 128)
-    queries = workloads.box_queries(layout, grid, args.queries, 4, 64, 202 + 1000 * rank)
+    if args.workload == "c2":
+        grid = (128, 128)
+        queries = workloads.box_queries(layout, grid, args.queries or 256, 4, 64, 202 + 1000 * rank)
+        policy = bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True)
+        workload_desc = ("c2: 256 uneven regional queries (box side U[4,64] tiles) on 128x128 tiles x 128 nodes, "
+                         "2,097,152 V / 16,777,216 E, f32 lognormal costs")
+    else:
+        grid = (256, 256)
+        queries = workloads.full_graph_queries(layout, grid, args.queries or 64, 303 + 1000 * rank)
+        policy = bfx.BatchPlannerPolicy(32, 0, 1, 64, 1)
+        workload_desc = ("c3: 64 full-graph sources in batches of 32 on 256x256 tiles x 256 nodes, "
+                         "16,777,216 V / 167,772,160 E, uint costs U[1,255]")
     t1 = time.time()
-    policy = bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True)
     plan = bfx.make_overlapping_batch_plan(layout, queries, policy)
     descs = plan.descriptions()
     t2 = time.time()
@@ -211,8 +222,14 @@ def main():
     device = local if world > 1 else 0
     resident = bfx.ResidentDeviceGraph.upload_once(layout, device)
     ws = bfx.Workspace(resident)
-    engine_id = {"frontier": bfx.ENGINE_FRONTIER_PUSH, "jacobi": bfx.ENGINE_JACOBI_PULL,
+    engine_id = {"auto": bfx.ENGINE_AUTO, "frontier": bfx.ENGINE_FRONTIER_PUSH, "jacobi": bfx.ENGINE_JACOBI_PULL,
                  "dense": bfx.ENGINE_DENSE_CHAOTIC_PUSH}[args.engine]
+    engines_chosen = None
+    if engine_id == bfx.ENGINE_AUTO:
+        t3 = time.time()
+        engines_chosen, measured = ws.autotune(descs)
+        log(f"[bench] autotune {time.time() - t3:.1f}s ({measured} batches timed): "
+            f"{ {e: engines_chosen.count(e) for e in set(engines_chosen)} } (0 jacobi, 1 dense, 2 frontier)")
     opts = bfx.GpuRunOptions(engine=engine_id)
     opts_instr = bfx.GpuRunOptions(engine=engine_id, instrumentation=1)
 
@@ -292,7 +309,7 @@ def main():
     e3 = torch.cuda.Event(enable_timing=True)
     s3.record(stream)
     for q in sample_q:
-        ws.run_query(q.sources, q.targets, q.selected_tiles, opts)
+        ws.run_query(q.sources, q.targets, q.selected_tiles, bfx.GpuRunOptions(engine=bfx.ENGINE_FRONTIER_PUSH))
     e3.record(stream)
     barrier()
     plain_ms = s3.elapsed_time(e3)
@@ -320,13 +337,14 @@ def main():
                 traffic = int(float(line.split(":")[1]))
 
     line = {
-        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "metric": METRIC if args.workload == "c2" else METRIC_C3, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "c2: 256 uneven regional queries (box side U[4,64] tiles) on 128x128 tiles x 128 "
-                               "nodes, 2,097,152 V / 16,777,216 E, f32 lognormal costs",
+        "config": {"workload": workload_desc,
                    "queries_per_gpu": len(queries), "batches": plan.batch_count,
                    "lane_widths": sorted({d.lane_width for d in descs}), "engine": args.engine,
+                   "engines_chosen": None if engines_chosen is None else
+                   {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
                    "control": "persistent_cooperative", "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (graph 0.54 GB + labels), no flush"},
         "gteps": lane_edges * world / (ms_per_step / 1000) / 1e9,
@@ -344,11 +362,12 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         try:
-            cb = cpu_reference_baseline(g, order, queries, 32, threads)
+            cb = cpu_reference_baseline(g, order, queries, 32, threads) if args.workload == "c2" else None
         except Exception as exc:  # reference build unusable here
             log(f"[bench] reference baseline failed: {exc}")
             cb = None
-        line["cpu_baseline"] = cb or cpu_port_baseline(layout, queries, 32, threads)
+        line["cpu_baseline"] = cb or cpu_port_baseline(layout, queries, 32 if args.workload == "c2" else threads,
+                                                       threads)
     if rank == 0:
         print(json.dumps(line))
     ws.close()

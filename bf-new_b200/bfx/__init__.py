@@ -32,6 +32,7 @@ u32, u64, i32, i64, f32 = C.c_uint32, C.c_uint64, C.c_int32, C.c_int64, C.c_floa
 P = C.POINTER
 
 ENGINE_JACOBI_PULL, ENGINE_DENSE_CHAOTIC_PUSH, ENGINE_FRONTIER_PUSH = 0, 1, 2
+ENGINE_AUTO = 0xFFFFFFFF
 CONTROL_PERSISTENT, CONTROL_CHUNKED, CONTROL_PER_ROUND = 0, 1, 2
 STOP_NONE, STOP_CONVERGED, STOP_MAXIMUM_ROUNDS, STOP_QUEUE_OVERFLOW, STOP_INVALID, STOP_FAILURE = range(6)
 INF_BITS = 0x7F800000
@@ -524,6 +525,24 @@ class Workspace:
 
     def execute(self, options: GpuRunOptions):
         _check(load().bfx_execute(self._h, C.byref(options)))
+
+    def autotune(self, batches: Sequence[BatchDescription], base: GpuRunOptions | None = None,
+                 trials: int = 2) -> tuple[list[int], int]:
+        """bfx_autotune: per-batch engine choice (timed, cached by batch shape);
+        leaves the batches prepared for ENGINE_AUTO launches.  Returns
+        (engines, batches measured)."""
+        arr = (BatchDescriptionC * len(batches))(*[b.c() for b in batches])
+        self._keep = batches
+        out = (u32 * len(batches))()
+        measured = u32()
+        _check(load().bfx_autotune(self._h, u32(len(batches)), arr, C.byref(base or GpuRunOptions()), u32(trials),
+                                   out, C.byref(measured)))
+        self.batch_count = len(batches)
+        return list(out), measured.value
+
+    def set_batch_engines(self, engines: Sequence[int]):
+        arr = (u32 * len(engines))(*engines)
+        _check(load().bfx_set_batch_engines(self._h, u32(len(engines)), arr))
 
     def fetch_statuses(self, controllers: bool = False):
         st = (DeviceRunStatus * self.batch_count)()

@@ -150,7 +150,7 @@ __global__ void init_kernel(LaunchParams p) {
     B.mask[1][cv] = 0u;
     for (u32 l = 0; l < B.W; ++l) {
       B.dist[0][(static_cast<u64>(cv) << B.shift) + l] = dev::kUnreached;
-      if (p.engine == BFX_ENGINE_JACOBI_PULL) B.dist[1][(static_cast<u64>(cv) << B.shift) + l] = dev::kUnreached;
+      if (engine_of(p, b) == BFX_ENGINE_JACOBI_PULL) B.dist[1][(static_cast<u64>(cv) << B.shift) + l] = dev::kUnreached;
     }
   }
   // Tile tables: clear every tile then write union tiles (a second pass in
@@ -203,8 +203,9 @@ __global__ void seed_kernel(LaunchParams p, const u32* src_base) {
     }
     const u32 cv = v - t.y;
     B.dist[0][(static_cast<u64>(cv) << B.shift) + lane] = dev::kSourceWord;
-    if (p.engine == BFX_ENGINE_JACOBI_PULL) B.dist[1][(static_cast<u64>(cv) << B.shift) + lane] = dev::kSourceWord;
-    if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
+    const u32 eng = engine_of(p, b);
+    if (eng == BFX_ENGINE_JACOBI_PULL) B.dist[1][(static_cast<u64>(cv) << B.shift) + lane] = dev::kSourceWord;
+    if (eng == BFX_ENGINE_FRONTIER_PUSH) {
       const u32 old = atomicOr(&B.mask[0][cv], 1u << lane);
       if (old == 0u) {
         const u32 slot = atomicAdd(&p.ctl[b].count[0], 1u);
@@ -331,23 +332,20 @@ __device__ __forceinline__ void dense_item(const LaunchParams& p, const DBatch& 
 
 __device__ __forceinline__ u32 batch_exec(const LaunchParams& p, u32 b, u32 ridx) {
   const u32 ch = dev::ld_cg(&p.ctl[b].changed[ridx]);
-  if (p.engine == BFX_ENGINE_JACOBI_PULL) return ch != 0u ? p.batches[b].valid : 0u;
+  if (engine_of(p, b) == BFX_ENGINE_JACOBI_PULL) return ch != 0u ? p.batches[b].valid : 0u;
   return p.per_lane ? ch : (ch != 0u ? p.batches[b].valid : 0u);
 }
 
 __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
   const u32 ridx = r % 3u, widx = (r + 1u) % 3u;
-  if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
-    block_prefix(prefix, p.nb, [&](u32 b) {
-      const u32 n = min(dev::ld_cg(&p.ctl[b].count[ridx]), p.batches[b].U);
-      return p.batches[b].W <= 8u ? (n + 3u) >> 2 : n;  // warp items: 4 or 1 entries each
-    });
-  } else {
-    block_prefix(prefix, p.nb, [&](u32 b) {
-      const DBatch& B = p.batches[b];
-      return batch_exec(p, b, ridx) != 0u ? (((B.U << B.shift) + 31u) >> 5) : 0u;
-    });
-  }
+  block_prefix(prefix, p.nb, [&](u32 b) {
+    const DBatch& B = p.batches[b];
+    if (engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH) {
+      const u32 n = min(dev::ld_cg(&p.ctl[b].count[ridx]), B.U);
+      return B.W <= 8u ? (n + 3u) >> 2 : n;  // warp items: 4 or 1 entries each
+    }
+    return batch_exec(p, b, ridx) != 0u ? (((B.U << B.shift) + 31u) >> 5) : 0u;
+  });
   return prefix[p.nb];
 }
 
@@ -363,14 +361,15 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
     const DBatch& B = p.batches[b];
     DCtl& C = p.ctl[b];
     const u32 item = w - prefix[b];
-    if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
+    const u32 eng = engine_of(p, b);
+    if (eng == BFX_ENGINE_FRONTIER_PUSH) {
       const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
       if (B.W <= 8u) {
         frontier_group<kCount, 8>(p, B, C, item, n, r & 1u, widx, wk);
       } else {
         frontier_group<kCount, 32>(p, B, C, item, n, r & 1u, widx, wk);
       }
-    } else if (p.engine == BFX_ENGINE_JACOBI_PULL) {
+    } else if (eng == BFX_ENGINE_JACOBI_PULL) {
       jacobi_item<kCount>(p, B, C, item, r, widx, wk);
     } else {
       dense_item<kCount>(p, B, C, item, batch_exec(p, b, ridx), widx, wk);
@@ -384,7 +383,7 @@ __device__ void round_bookkeeping(const LaunchParams& p, u32 r) {
   const u32 ridx = r % 3u, zidx = (r + 2u) % 3u;
   for (u32 b = threadIdx.x; b < p.nb; b += blockDim.x) {
     DCtl& C = p.ctl[b];
-    const bool work = p.engine == BFX_ENGINE_FRONTIER_PUSH ? dev::ld_cg(&C.count[ridx]) != 0u
+    const bool work = engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH ? dev::ld_cg(&C.count[ridx]) != 0u
                                                           : batch_exec(p, b, ridx) != 0u;
     if (work) C.rounds = r + 1u;
     C.count[zidx] = 0u;
@@ -475,6 +474,7 @@ __global__ void start_kernel(LaunchParams p) {
 
 __global__ void finalize_kernel(LaunchParams p, bfx_device_controller* controllers, bfx_device_run_status* statuses) {
   const u32 b = blockIdx.x;
+  const u32 eng = engine_of(p, b);
   const DBatch& B = p.batches[b];
   DCtl& C = p.ctl[b];
   __shared__ u32 s_missing, s_active;
@@ -487,12 +487,12 @@ __global__ void finalize_kernel(LaunchParams p, bfx_device_controller* controlle
   const u32 ridx = r_end % 3u;
   const bool aborted = p.run->abort != 0u;
   bool pending;
-  if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
+  if (eng == BFX_ENGINE_FRONTIER_PUSH) {
     pending = C.count[ridx] != 0u;
   } else {
     pending = batch_exec(p, b, ridx) != 0u;
   }
-  const u32 final_slot = p.engine == BFX_ENGINE_JACOBI_PULL ? (C.rounds & 1u) : 0u;
+  const u32 final_slot = eng == BFX_ENGINE_JACOBI_PULL ? (C.rounds & 1u) : 0u;
   const u64* const d = B.dist[final_slot];
   for (u32 i = threadIdx.x; i < B.tgt_count; i += blockDim.x) {
     const u32 lane = lane_of_position(B.tgt_off, B.W, i);
@@ -503,7 +503,7 @@ __global__ void finalize_kernel(LaunchParams p, bfx_device_controller* controlle
     if (!reached) atomicOr(&s_missing, 1u << lane);
   }
   if (pending && !aborted) {
-    if (p.engine == BFX_ENGINE_FRONTIER_PUSH) {
+    if (eng == BFX_ENGINE_FRONTIER_PUSH) {
       const u32* const mk = B.mask[r_end & 1u];
       u32 acc = 0u;
       for (u32 i = threadIdx.x; i < B.U; i += blockDim.x) acc |= mk[i];
@@ -556,15 +556,15 @@ __global__ void finalize_kernel(LaunchParams p, bfx_device_controller* controlle
   c.valid_lane_mask = valid;
   c.active_lane_mask = active;
   c.converged_lane_mask = conv_lanes;
-  c.engine_kind = p.engine;
+  c.engine_kind = eng;
   c.enable_per_lane_convergence = p.per_lane;
   c.rounds_completed = C.rounds;
   c.maximum_rounds = p.max_rounds;
   c.distance_read_slot = final_slot;
-  c.distance_write_slot = p.engine == BFX_ENGINE_JACOBI_PULL ? (final_slot ^ 1u) : 0u;
+  c.distance_write_slot = eng == BFX_ENGINE_JACOBI_PULL ? (final_slot ^ 1u) : 0u;
   c.frontier_read_slot = r_end & 1u;
   c.frontier_write_slot = (r_end & 1u) ^ 1u;
-  c.frontier_size[r_end & 1u] = p.engine == BFX_ENGINE_FRONTIER_PUSH ? C.count[ridx] : 0u;
+  c.frontier_size[r_end & 1u] = eng == BFX_ENGINE_FRONTIER_PUSH ? C.count[ridx] : 0u;
   c.done = 1u;
   c.stop_reason = stop;
   c.error_bits = error_bits;
@@ -1005,8 +1005,8 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
 namespace bfx {
 namespace {
 
-void validate_options(const bfx_gpu_run_options& o) {
-  if (o.engine > 2u) throw std::invalid_argument("invalid engine");
+void validate_options(const bfx_gpu_run_options& o, bool allow_auto = false) {
+  if (o.engine > 2u && !(allow_auto && o.engine == BFX_ENGINE_AUTO)) throw std::invalid_argument("invalid engine");
   if (o.control_mode > 2u) throw std::invalid_argument("invalid control mode");
   if (o.rounds_per_chunk == 0u) throw std::invalid_argument("invalid rounds per chunk");
   if (o.block_size == 0u || o.block_size % 32u != 0u || o.block_size > 512u)
@@ -1033,12 +1033,26 @@ int grid_blocks(bfx_workspace* ws, const void* kernel, int block, size_t smem, c
 
 void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   require(ws->nb > 0, "no prepared batches");
-  validate_options(o);
+  validate_options(o, true);
   BFX_CUDA(cudaSetDevice(ws->graph->device));
   LaunchParams p = ws->params;
   p.engine = o.engine;
   p.per_lane = o.enable_per_lane_convergence;
   p.max_rounds = o.maximum_rounds;
+  p.engines = nullptr;
+  if (o.engine == BFX_ENGINE_AUTO) {
+    // Per-batch engines chosen by bfx_autotune / bfx_set_batch_engines
+    // (frontier push where none was chosen).
+    std::vector<std::uint32_t> eng(ws->nb, BFX_ENGINE_FRONTIER_PUSH);
+    if (ws->batch_engines.size() == ws->nb) eng = ws->batch_engines;
+    ws->engines_dev.reserve(ws->nb * 4, ws->graph->device);
+    ws->status_host.reserve(ws->nb * 4 + 256);
+    std::memcpy(ws->status_host.ptr, eng.data(), ws->nb * 4);
+    BFX_CUDA(cudaMemcpyAsync(ws->engines_dev.ptr, ws->status_host.ptr, ws->nb * 4, cudaMemcpyHostToDevice,
+                             ws->stream));
+    p.engines = static_cast<const std::uint32_t*>(ws->engines_dev.ptr);
+    p.engine = BFX_ENGINE_FRONTIER_PUSH;
+  }
   const int block = static_cast<int>(o.block_size);
   const size_t smem = (size_t{ws->nb} + 1) * 4;
   std::uint64_t launches = 0;
@@ -1172,12 +1186,10 @@ int bfx_download_labels(bfx_workspace* ws, uint32_t batch, uint32_t* distance_bi
     BFX_CUDA(cudaSetDevice(ws->graph->device));
     const bfx::DBatch& B = ws->batches[batch];
     const size_t n = static_cast<size_t>(ws->graph->g.V) << B.shift;
-    std::uint32_t slot = 0;
-    if (ws->params.engine == BFX_ENGINE_JACOBI_PULL) {
-      bfx_device_run_status st;
-      BFX_CUDA(cudaMemcpy(&st, ws->d_status + batch, sizeof(st), cudaMemcpyDeviceToHost));
-      slot = st.final_distance_slot;
-    }
+    bfx_device_run_status st;
+    BFX_CUDA(cudaMemcpyAsync(&st, ws->d_status + batch, sizeof(st), cudaMemcpyDeviceToHost, ws->stream));
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    const std::uint32_t slot = st.final_distance_slot;
     std::uint32_t* d_out = nullptr;
     BFX_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_out), n * 8, ws->stream));
     bfx::expand_kernel<<<ws->sm_count * 8, 256, 0, ws->stream>>>(ws->graph->g, B, slot, d_out, d_out + n);
@@ -1235,6 +1247,15 @@ int bfx_workspace_transfer_bytes(bfx_workspace* ws, uint64_t out[2]) {
     bfx::require(ws && out, "null argument");
     out[0] = ws->last_h2d;
     out[1] = ws->last_d2h;
+  });
+}
+
+int bfx_set_batch_engines(bfx_workspace* ws, uint32_t count, const uint32_t* engines) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null workspace");
+    bfx::require(count == 0 || engines != nullptr, "null engines");
+    for (std::uint32_t i = 0; i < count; ++i) bfx::require(engines[i] <= 2u, "invalid engine");
+    ws->batch_engines.assign(engines, engines + count);
   });
 }
 
@@ -1521,5 +1542,63 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
     BFX_CUDA(cudaMemcpy(status, d_status, sizeof(*status), cudaMemcpyDeviceToHost));
     BFX_CUDA(cudaMemcpy(target_distance_bits, out, Tg * 4, cudaMemcpyDeviceToHost));
     BFX_CUDA(cudaMemcpy(target_predecessor_edges, out + Tg, Tg * 4, cudaMemcpyDeviceToHost));
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Barrier self-test (failure detection without a GPU fault).  A cooperative
+// grid runs `rounds` grid barriers; when absent_block < gridDim.x that block
+// never arrives, so the others' bounded waits run out after timeout_ns, raise
+// the abort flag and return -- the same path a stuck engine launch takes.
+// out = {aborted, barriers passed by block 0 (all blocks when none is
+// absent), blocks that observed the abort, 0}.
+// ---------------------------------------------------------------------------
+
+namespace bfx {
+namespace {
+
+__global__ void barrier_selftest_kernel(dev::GridSync* gs, u32 rounds, u32 absent_block, u64 timeout_ns, u32* out) {
+  if (blockIdx.x == absent_block) return;  // never arrives: nothing else sets the generation
+  u32 passed = 0;
+  for (u32 r = 0; r < rounds; ++r) {
+    if (!dev::grid_barrier(gs, gridDim.x, timeout_ns)) break;
+    ++passed;
+  }
+  if (threadIdx.x == 0) {
+    if (passed < rounds) atomicAdd(&out[2], 1u);
+    if (blockIdx.x == (absent_block == 0u ? 1u : 0u)) out[1] = passed;
+    if (gs->abort) out[0] = 1u;
+  }
+}
+
+}  // namespace
+}  // namespace bfx
+
+extern "C" int bfx_barrier_selftest(int device, uint32_t rounds, uint32_t absent_block, uint64_t timeout_ns,
+                                    uint32_t out[4]) {
+  return bfx::guarded([&] {
+    bfx::require(out != nullptr, "null output");
+    bfx::require(timeout_ns > 0 && timeout_ns <= 2000000000ull, "timeout must be in (0, 2 s]");
+    BFX_CUDA(cudaSetDevice(device));
+    int sms = 0, per_sm = 0;
+    BFX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    BFX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, reinterpret_cast<const void*>(bfx::barrier_selftest_kernel), 128, 0));
+    const int grid = std::max(2, std::min(per_sm, 2) * sms);
+    void* mem = nullptr;
+    BFX_CUDA(cudaMalloc(&mem, 256));
+    cudaError_t err = cudaMemset(mem, 0, 256);
+    auto* gs = static_cast<bfx::dev::GridSync*>(mem);
+    auto* dout = reinterpret_cast<std::uint32_t*>(static_cast<char*>(mem) + 64);
+    if (err == cudaSuccess) {
+      void* args[] = {&gs, &rounds, &absent_block, &timeout_ns, &dout};
+      err = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(bfx::barrier_selftest_kernel), grid, 128, args,
+                                        0, 0);
+    }
+    if (err == cudaSuccess) err = cudaDeviceSynchronize();
+    if (err == cudaSuccess) err = cudaMemcpy(out, dout, 16, cudaMemcpyDeviceToHost);
+    out[3] = static_cast<std::uint32_t>(grid);
+    cudaFree(mem);
+    BFX_CUDA(err);
   });
 }

@@ -99,11 +99,16 @@ struct LaunchParams {
   DRun* run;
   const u32* unit_base;  // [nb+1] prefix of U (init / finalize)
   u32 nb;
-  u32 engine;
+  u32 engine;            // engine of every batch when `engines` is null
   u32 per_lane;
   u32 reserved;
   u64 max_rounds;
+  const u32* engines;    // [nb] per-batch engine (autotuned launches) or null
 };
+
+__device__ __forceinline__ u32 engine_of(const LaunchParams& p, u32 b) {
+  return p.engines ? p.engines[b] : p.engine;
+}
 
 // Host side
 // ---------------------------------------------------------------------------
@@ -210,5 +215,7 @@ struct bfx_workspace {
   std::uint64_t path_edges{0};
   bool paths_ready{false};
   bfx::DeviceBuffer adjoint;     // per-edge exact accumulators, upstream values, result
+  std::vector<std::uint32_t> batch_engines;  // per-batch engine for BFX_ENGINE_AUTO launches
+  bfx::DeviceBuffer engines_dev;
 };
 

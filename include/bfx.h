@@ -260,6 +260,33 @@ int bfx_edge_usage_adjoint(bfx_workspace *ws, const float *target_grads, float *
  * indexed by stable edge id, finite and non-negative (-0 becomes +0). */
 int bfx_resident_graph_set_weights(bfx_resident_graph *graph, const float *weights_by_edge_id);
 
+/* ---- engine autotuner ----------------------------------------------------------
+ * No counterpart in the reference (its engine shootout, src/engine_shootout.cpp,
+ * only catalogues configurations).  Picks frontier push, Jacobi pull or dense
+ * chaotic push per batch by timing each engine on the batch alone (best of
+ * `trials` device timings), caching the choice per batch shape (lane width,
+ * valid lanes, magnitude of union vertices and tiles).  Leaves the workspace
+ * prepared with all `count` batches and their engines, so bfx_execute with
+ * options->engine == BFX_ENGINE_AUTO relaxes each batch with its own engine
+ * in one launch.  engines_out[count]; *measured (may be NULL) = batches that
+ * were timed rather than found in the cache. */
+int bfx_autotune(bfx_workspace *ws, uint32_t count, const bfx_batch_description *batches,
+                 const bfx_gpu_run_options *base, uint32_t trials, uint32_t *engines_out, uint32_t *measured);
+/* Forgets all cached autotuner choices. */
+int bfx_autotune_reset(void);
+/* Sets the per-batch engines used by BFX_ENGINE_AUTO launches of the prepared
+ * batches (count must equal the prepared batch count at execute time). */
+int bfx_set_batch_engines(bfx_workspace *ws, uint32_t count, const uint32_t *engines);
+
+/* Failure-detection self-test of the engines' grid barrier (no counterpart
+ * in the reference, whose cooperative barrier cannot time out).  Runs
+ * `rounds` barriers over a cooperative grid; if absent_block < grid size,
+ * that block never arrives and the others' bounded waits give up after
+ * timeout_ns (<= 2 s) and raise the abort flag -- the path a stuck engine
+ * launch takes to report BFX_STOP_DEVICE_FAILURE.  out = {aborted, barriers
+ * passed by a present block, blocks that gave up, grid size}. */
+int bfx_barrier_selftest(int device, uint32_t rounds, uint32_t absent_block, uint64_t timeout_ns, uint32_t out[4]);
+
 /* Kernels launched by the most recent bfx_execute (its own kernels only). */
 int bfx_last_launch_count(bfx_workspace *ws, uint64_t *launches);
 

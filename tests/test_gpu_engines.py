@@ -207,3 +207,32 @@ def test_invalid_options_and_descriptions_rejected(gpu, c1):
         eng.run_compact_status([bad], bfx.GpuRunOptions())
     ws.close()
     res.close()
+
+
+def test_autotuned_mixed_engines_one_launch(gpu):
+    """bfx_autotune picks an engine per batch; an ENGINE_AUTO launch relaxes
+    every batch with its own engine in one launch, bit-exact.  A forced mix
+    of all three engines checks the per-batch dispatch itself."""
+    layout, grid = workloads.build_graph("c2", scale_tiles=(32, 32))
+    qs = workloads.box_queries(layout, grid, 30, 2, 16, seed=19)
+    plan = bfx.make_overlapping_batch_plan(layout, qs, bfx.BatchPlannerPolicy(32, 0, 1, 8, 1, narrow_lanes=True))
+    descs = plan.descriptions()
+    lanes = [[qs[i] if i != bfx.NO_EDGE else None for i in d.query_index_by_lane] for d in descs]
+    res = bfx.ResidentDeviceGraph.upload_once(layout)
+    ws = bfx.Workspace(res)
+    lib = bfx.load()
+    lib.bfx_autotune_reset()
+    engines, measured = ws.autotune(descs)
+    assert len(engines) == len(descs) and set(engines) <= {0, 1, 2} and measured >= 1
+    engines2, measured2 = ws.autotune(descs)
+    assert engines2 == engines and measured2 == 0  # cached by shape
+    orc = Oracle.from_layout(layout)
+    for mix in (engines, [i % 3 for i in range(len(descs))]):
+        ws.prepare(descs)
+        ws.set_batch_engines(mix)
+        ws.execute(bfx.GpuRunOptions(engine=bfx.ENGINE_AUTO))
+        st = ws.fetch_statuses()
+        labels = [ws.download_labels(b, d.lane_width) for b, d in enumerate(descs)]
+        check_batches(layout, descs, lanes, st, labels, orc)
+    ws.close()
+    res.close()
