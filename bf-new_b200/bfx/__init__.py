@@ -534,11 +534,18 @@ class Workspace:
         arr = (BatchDescriptionC * len(batches))(*[b.c() for b in batches])
         self._keep = batches
         out = (u32 * len(batches))()
+        deltas = (f32 * len(batches))()
         measured = u32()
         _check(load().bfx_autotune(self._h, u32(len(batches)), arr, C.byref(base or GpuRunOptions()), u32(trials),
-                                   out, C.byref(measured)))
+                                   out, deltas, C.byref(measured)))
         self.batch_count = len(batches)
+        self.tuned_deltas = [float(x) for x in deltas]
         return list(out), measured.value
+
+    def set_batch_deltas(self, deltas: Sequence[float]):
+        """Near/far threshold steps per frontier batch (inf = plain frontier)."""
+        arr = (f32 * len(deltas))(*deltas)
+        _check(load().bfx_set_batch_deltas(self._h, u32(len(deltas)), arr))
 
     def set_batch_engines(self, engines: Sequence[int]):
         arr = (u32 * len(engines))(*engines)

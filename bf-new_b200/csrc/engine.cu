@@ -148,6 +148,7 @@ __global__ void init_kernel(LaunchParams p) {
     B.c2g[cv] = r.y + (cv - B.range_off[lo]);
     B.mask[0][cv] = 0u;
     B.mask[1][cv] = 0u;
+    B.fmask[cv] = 0u;
     for (u32 l = 0; l < B.W; ++l) {
       B.dist[0][(static_cast<u64>(cv) << B.shift) + l] = dev::kUnreached;
       if (engine_of(p, b) == BFX_ENGINE_JACOBI_PULL) B.dist[1][(static_cast<u64>(cv) << B.shift) + l] = dev::kUnreached;
@@ -166,6 +167,10 @@ __global__ void init_kernel(LaunchParams p) {
     DCtl& c = p.ctl[tid];
     c.count[0] = c.count[1] = c.count[2] = 0u;
     c.changed[0] = p.batches[tid].valid;
+    c.fcount[0] = c.fcount[1] = c.fcount[2] = 0u;
+    c.gen[0] = c.gen[1] = 0u;
+    c.delta = p.deltas ? p.deltas[tid] : dev::kInfBits;
+    c.tau[0] = c.tau[1] = c.delta;
     c.changed[1] = c.changed[2] = 0u;
     c.rounds = 0u;
     c.missing = 0u;
@@ -341,8 +346,11 @@ __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
   block_prefix(prefix, p.nb, [&](u32 b) {
     const DBatch& B = p.batches[b];
     if (engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH) {
-      const u32 n = min(dev::ld_cg(&p.ctl[b].count[ridx]), B.U);
-      return B.W <= 8u ? (n + 3u) >> 2 : n;  // warp items: 4 or 1 entries each
+      const DCtl& C = p.ctl[b];
+      const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
+      if (n != 0u) return B.W <= 8u ? (n + 3u) >> 2 : n;  // warp items: 4 or 1 entries each
+      const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
+      return (f + 31u) >> 5;  // split round: 32 far entries per warp item
     }
     return batch_exec(p, b, ridx) != 0u ? (((B.U << B.shift) + 31u) >> 5) : 0u;
   });
@@ -364,10 +372,18 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
     const u32 eng = engine_of(p, b);
     if (eng == BFX_ENGINE_FRONTIER_PUSH) {
       const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
-      if (B.W <= 8u) {
-        frontier_group<kCount, 8>(p, B, C, item, n, r & 1u, widx, wk);
+      const u32 g = dev::ld_cg(&C.gen[r & 1u]);
+      const u32 tau = dev::ld_cg(&C.tau[r & 1u]);
+      if (n != 0u) {
+        if (B.W <= 8u) {
+          frontier_group<kCount, 8>(p, B, C, item, n, r & 1u, widx, tau, g % 3u, wk);
+        } else {
+          frontier_group<kCount, 32>(p, B, C, item, n, r & 1u, widx, tau, g % 3u, wk);
+        }
       } else {
-        frontier_group<kCount, 32>(p, B, C, item, n, r & 1u, widx, wk);
+        const u32 f = min(dev::ld_cg(&C.fcount[g % 3u]), B.U);
+        const u32 tau_next = __float_as_uint(__fadd_rn(__uint_as_float(tau), __uint_as_float(C.delta)));
+        split_group<kCount>(p, B, C, item, f, r & 1u, widx, tau_next, g % 3u, (g + 1u) % 3u, wk);
       }
     } else if (eng == BFX_ENGINE_JACOBI_PULL) {
       jacobi_item<kCount>(p, B, C, item, r, widx, wk);
@@ -383,8 +399,26 @@ __device__ void round_bookkeeping(const LaunchParams& p, u32 r) {
   const u32 ridx = r % 3u, zidx = (r + 2u) % 3u;
   for (u32 b = threadIdx.x; b < p.nb; b += blockDim.x) {
     DCtl& C = p.ctl[b];
-    const bool work = engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH ? dev::ld_cg(&C.count[ridx]) != 0u
-                                                          : batch_exec(p, b, ridx) != 0u;
+    bool work;
+    if (engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH) {
+      // near round, split round (near frontier empty, far pile not), or idle;
+      // generation and threshold of round r+1 go to the other parity slot.
+      const u32 g = dev::ld_cg(&C.gen[r & 1u]);
+      const u32 tau = dev::ld_cg(&C.tau[r & 1u]);
+      const bool near = dev::ld_cg(&C.count[ridx]) != 0u;
+      const bool split = !near && dev::ld_cg(&C.fcount[g % 3u]) != 0u;
+      work = near || split;
+      if (split) {
+        C.fcount[(g + 2u) % 3u] = 0u;  // idle since two splits ago; the next split writes it
+        C.gen[(r + 1u) & 1u] = g + 1u;
+        C.tau[(r + 1u) & 1u] = __float_as_uint(__fadd_rn(__uint_as_float(tau), __uint_as_float(C.delta)));
+      } else {
+        C.gen[(r + 1u) & 1u] = g;
+        C.tau[(r + 1u) & 1u] = tau;
+      }
+    } else {
+      work = batch_exec(p, b, ridx) != 0u;
+    }
     if (work) C.rounds = r + 1u;
     C.count[zidx] = 0u;
     C.changed[zidx] = 0u;
@@ -488,7 +522,7 @@ __global__ void finalize_kernel(LaunchParams p, bfx_device_controller* controlle
   const bool aborted = p.run->abort != 0u;
   bool pending;
   if (eng == BFX_ENGINE_FRONTIER_PUSH) {
-    pending = C.count[ridx] != 0u;
+    pending = C.count[ridx] != 0u || C.fcount[C.gen[r_end & 1u] % 3u] != 0u;
   } else {
     pending = batch_exec(p, b, ridx) != 0u;
   }
@@ -506,7 +540,7 @@ __global__ void finalize_kernel(LaunchParams p, bfx_device_controller* controlle
     if (eng == BFX_ENGINE_FRONTIER_PUSH) {
       const u32* const mk = B.mask[r_end & 1u];
       u32 acc = 0u;
-      for (u32 i = threadIdx.x; i < B.U; i += blockDim.x) acc |= mk[i];
+      for (u32 i = threadIdx.x; i < B.U; i += blockDim.x) acc |= mk[i] | B.fmask[i];
       acc = __reduce_or_sync(0xFFFFFFFFu, acc);
       if (lane_id() == 0 && acc) atomicOr(&s_active, acc);
     } else if (threadIdx.x == 0) {
@@ -732,6 +766,9 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
     BFX_CUDA(cudaMemcpy(base + o_csr, csr.data(), size_t{E} * 16, cudaMemcpyHostToDevice));
     BFX_CUDA(cudaMemcpy(base + o_csc, csc.data(), size_t{E} * 16, cudaMemcpyHostToDevice));
     BFX_CUDA(cudaMemcpy(base + o_eid_src, eid_src.data(), size_t{E} * 4, cudaMemcpyHostToDevice));
+    double wsum = 0.0;
+    for (std::uint32_t e = 0; e < E; ++e) wsum += L.csr_weights[e];
+    G->mean_weight = E ? wsum / E : 0.0;
     G->g.V = V;
     G->g.E = E;
     G->g.T = T;
@@ -748,6 +785,14 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
 
 int bfx_resident_graph_destroy(bfx_resident_graph* graph) {
   return bfx::guarded([&] { delete graph; });
+}
+
+int bfx_workspace_graph_stats(bfx_workspace* ws, double out[2]) {
+  return bfx::guarded([&] {
+    bfx::require(ws && out, "null argument");
+    out[0] = ws->graph->mean_weight;
+    out[1] = static_cast<double>(ws->graph->g.E);
+  });
 }
 
 int bfx_resident_graph_info(const bfx_resident_graph* graph, uint64_t out[4]) {
@@ -902,7 +947,7 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
     for (std::uint32_t b = 0; b < count; ++b) {
       arena_off[b] = arena_total;
       const size_t U = sz[b].U;
-      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 3 + bfx::align256(U * 8) * 2 +
+      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 4 + bfx::align256(U * 8) * 5 +
                      bfx::align256(size_t{g.T} * 8);
     }
     const bool grew = meta_total > ws->meta.bytes || arena_total > ws->arena.bytes;
@@ -965,6 +1010,12 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
       a += bfx::align256(U * 8);
       B.c2g = reinterpret_cast<std::uint32_t*>(a);
       a += bfx::align256(U * 4);
+      B.fmask = reinterpret_cast<std::uint32_t*>(a);
+      a += bfx::align256(U * 4);
+      for (int k = 0; k < 3; ++k) {
+        B.fpile[k] = reinterpret_cast<bfx::u64*>(a);
+        a += bfx::align256(U * 8);
+      }
       B.tiles = reinterpret_cast<uint2*>(a);
       ubase[b] = static_cast<std::uint32_t>(usum);
       sbase[b] = static_cast<std::uint32_t>(ssum);
@@ -1040,6 +1091,16 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   p.per_lane = o.enable_per_lane_convergence;
   p.max_rounds = o.maximum_rounds;
   p.engines = nullptr;
+  p.deltas = nullptr;
+  if (!ws->batch_deltas.empty()) {
+    require(ws->batch_deltas.size() == ws->nb, "per-batch deltas do not match the prepared batches");
+    ws->deltas_dev.reserve(ws->nb * 4, ws->graph->device);
+    ws->deltas_host.reserve(ws->nb * 4 + 256);
+    std::memcpy(ws->deltas_host.ptr, ws->batch_deltas.data(), ws->nb * 4);
+    BFX_CUDA(cudaMemcpyAsync(ws->deltas_dev.ptr, ws->deltas_host.ptr, ws->nb * 4, cudaMemcpyHostToDevice,
+                             ws->stream));
+    p.deltas = static_cast<const std::uint32_t*>(ws->deltas_dev.ptr);
+  }
   if (o.engine == BFX_ENGINE_AUTO) {
     // Per-batch engines chosen by bfx_autotune / bfx_set_batch_engines
     // (frontier push where none was chosen).
@@ -1250,6 +1311,17 @@ int bfx_workspace_transfer_bytes(bfx_workspace* ws, uint64_t out[2]) {
   });
 }
 
+int bfx_set_batch_deltas(bfx_workspace* ws, uint32_t count, const float* deltas) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null workspace");
+    bfx::require(count == 0 || deltas != nullptr, "null deltas");
+    for (std::uint32_t i = 0; i < count; ++i) {
+      bfx::require(deltas[i] > 0.0f, "near/far steps must be positive (+inf: plain frontier)");
+    }
+    ws->batch_deltas.assign(deltas, deltas + count);
+  });
+}
+
 int bfx_set_batch_engines(bfx_workspace* ws, uint32_t count, const uint32_t* engines) {
   return bfx::guarded([&] {
     bfx::require(ws != nullptr, "null workspace");
@@ -1437,7 +1509,11 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
     const size_t o_q0 = bfx::align256(o_mask1 + U * 4);
     const size_t o_q1 = bfx::align256(o_q0 + U * 8);
     const size_t o_c2g = bfx::align256(o_q1 + U * 8);
-    const size_t o_tiles = bfx::align256(o_c2g + U * 4);
+    const size_t o_fmask = bfx::align256(o_c2g + U * 4);
+    const size_t o_fp0 = bfx::align256(o_fmask + U * 4);
+    const size_t o_fp1 = bfx::align256(o_fp0 + U * 8);
+    const size_t o_fp2 = bfx::align256(o_fp1 + U * 8);
+    const size_t o_tiles = bfx::align256(o_fp2 + U * 8);
     const size_t total = bfx::align256(o_tiles + size_t{T} * 8);
     if (total > bfx::kStaticScratchBytes) {
       throw std::overflow_error("query needs more than the 32 MiB static scratch (union of " + std::to_string(U) +
@@ -1463,6 +1539,10 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
     B.queue[0] = reinterpret_cast<u64*>(base + o_q0);
     B.queue[1] = reinterpret_cast<u64*>(base + o_q1);
     B.c2g = reinterpret_cast<u32*>(base + o_c2g);
+    B.fmask = reinterpret_cast<u32*>(base + o_fmask);
+    B.fpile[0] = reinterpret_cast<u64*>(base + o_fp0);
+    B.fpile[1] = reinterpret_cast<u64*>(base + o_fp1);
+    B.fpile[2] = reinterpret_cast<u64*>(base + o_fp2);
     B.tiles = reinterpret_cast<uint2*>(base + o_tiles);
     B.src_off = reinterpret_cast<const u32*>(base + o_soff);
     B.src = reinterpret_cast<const u32*>(base + o_src);

@@ -56,6 +56,8 @@ struct DBatch {
   const u32* tgt;
   const uint4* ranges;    // [R] {tile, begin, end, lane mask}
   const u32* range_off;   // [R+1] compact offsets
+  u32* fmask;             // [U] far lanes (near/far frontier)
+  u64* fpile[3];          // [U] far piles, rotating by far generation
 };
 
 struct DCtl {
@@ -65,6 +67,12 @@ struct DCtl {
   u32 missing;     // finalize: lanes with an unreached target
   u32 active;      // finalize: lanes still pending at the stop
   u32 error_bits;
+  // Near/far frontier: far pile sizes by generation % 3; generation and
+  // threshold (float bits) double-buffered by round parity.
+  u32 fcount[3];
+  u32 gen[2];
+  u32 tau[2];
+  u32 delta;       // threshold step (float bits); +inf = plain frontier
 };
 
 struct DRun {
@@ -104,6 +112,7 @@ struct LaunchParams {
   u32 reserved;
   u64 max_rounds;
   const u32* engines;    // [nb] per-batch engine (autotuned launches) or null
+  const u32* deltas;     // [nb] near/far threshold steps (float bits) or null (plain frontier)
 };
 
 __device__ __forceinline__ u32 engine_of(const LaunchParams& p, u32 b) {
@@ -171,6 +180,7 @@ struct bfx_resident_graph {
   bfx::DeviceBuffer mem;
   std::vector<std::uint32_t> tile_vertex_offsets;  // host copy, [T+1]
   std::uint64_t bytes{0};
+  double mean_weight{0.0};
 };
 
 struct bfx_workspace {
@@ -216,6 +226,9 @@ struct bfx_workspace {
   bool paths_ready{false};
   bfx::DeviceBuffer adjoint;     // per-edge exact accumulators, upstream values, result
   std::vector<std::uint32_t> batch_engines;  // per-batch engine for BFX_ENGINE_AUTO launches
+  std::vector<float> batch_deltas;           // per-batch near/far steps (empty: plain frontier)
+  bfx::DeviceBuffer deltas_dev;
+  bfx::PinnedBuffer deltas_host;
   bfx::DeviceBuffer engines_dev;
 };
 

@@ -20,7 +20,7 @@
 
 template <bool kCount, u32 S>
 __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBatch& B, DCtl& C, u32 item, u32 count,
-                                               u32 rd, u32 widx, Work& wk) {
+                                               u32 rd, u32 widx, u32 tau_bits, u32 pile, Work& wk) {
   constexpr u32 EPW = 32u / S;
   const u32 lane = lane_id();
   const u32 sl = lane & (S - 1u);
@@ -68,7 +68,7 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
   u64* const queue_w = B.queue[rd ^ 1u];
   for (u32 st = 0; st < steps; ++st) {
     const u32 e = rb + st * G + slot;
-    u32 bits = 0u, cdst = 0u, dstv = 0u;
+    u32 bits = 0u, fbits = 0u, cdst = 0u, dstv = 0u;
     if (has_lane && e < re) {
       const uint4 rec = __ldg(p.g.csr + e);
       const uint2 dt = B.tiles[rec.w];
@@ -81,15 +81,40 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
         if (kCount) wk.c[3] += 1;
         if (cand < cur) {
           dev::red_min(target, cand);
-          if (dev::hi(cand) < dev::hi(cur)) bits = 1u << ql;
+          if (dev::hi(cand) < dev::hi(cur)) {
+            // near: below this round's threshold; far: parked until a split
+            if (dev::hi(cand) < tau_bits) bits = 1u << ql; else fbits = 1u << ql;
+          }
           if (kCount) {
             wk.c[6] += 1;
-            wk.c[5] += bits != 0u;
+            wk.c[5] += (bits | fbits) != 0u;
           }
         }
       }
     }
-    for (u32 o = 1; o < kp; o <<= 1) bits |= __shfl_xor_sync(0xFFFFFFFFu, bits, o);
+    for (u32 o = 1; o < kp; o <<= 1) {
+      bits |= __shfl_xor_sync(0xFFFFFFFFu, bits, o);
+      fbits |= __shfl_xor_sync(0xFFFFFFFFu, fbits, o);
+    }
+    if (__any_sync(0xFFFFFFFFu, fbits != 0u)) {
+      bool fclaim = false;
+      if (j == 0u && fbits != 0u) fclaim = atomicOr(B.fmask + cdst, fbits) == 0u;
+      const u32 fm = __ballot_sync(0xFFFFFFFFu, fclaim);
+      if (fm != 0u) {
+        const u32 first = __ffs(fm) - 1u;
+        u32 pos = 0u;
+        if (lane == first) pos = atomicAdd(&C.fcount[pile], static_cast<u32>(__popc(fm)));
+        pos = __shfl_sync(0xFFFFFFFFu, pos, static_cast<int>(first));
+        if (fclaim) {
+          const u32 at = pos + __popc(fm & ((1u << lane) - 1u));
+          if (at < B.U) {
+            B.fpile[pile][at] = static_cast<u64>(dstv) | (static_cast<u64>(cdst) << 32);
+          } else {
+            atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
+          }
+        }
+      }
+    }
     bool claim = false;
     if (j == 0u && bits != 0u) claim = atomicOr(mask_w + cdst, bits) == 0u;
     const u32 cm = __ballot_sync(0xFFFFFFFFu, claim);
@@ -107,6 +132,63 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
           atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
         }
       }
+    }
+  }
+}
+
+// Split round of the near/far frontier: the batch's near frontier is empty,
+// so the threshold advances by delta and every parked (vertex, lane) of the
+// current far pile is re-examined: lanes whose label is now below the new
+// threshold join the next round's near frontier, the rest move to the next
+// pile.  One thread per far entry; claims are warp-aggregated.  The batch
+// runs no near round in the same round, so the far masks it reads are
+// stable and are cleared with plain stores.
+template <bool kCount>
+__device__ __forceinline__ void split_group(const LaunchParams& p, const DBatch& B, DCtl& C, u32 item, u32 count,
+                                            u32 rd, u32 widx, u32 tau_next, u32 pile_in, u32 pile_out, Work& wk) {
+  const u32 lane = lane_id();
+  const u32 entry = item * 32u + lane;
+  u32 near = 0u, far = 0u, v = 0u, cv = 0u;
+  if (entry < count) {
+    const u64 q = dev::ld_cg(B.fpile[pile_in] + entry);
+    v = static_cast<u32>(q);
+    cv = static_cast<u32>(q >> 32);
+    const u32 bits = dev::ld_cg(B.fmask + cv);
+    B.fmask[cv] = 0u;
+    for (u32 m = bits; m != 0u; m &= m - 1u) {
+      const u32 l = __ffs(m) - 1u;
+      const u32 d = dev::hi(dev::ld_cg(B.dist[0] + ((static_cast<u64>(cv) << B.shift) + l)));
+      if (d < tau_next) near |= 1u << l; else far |= 1u << l;
+    }
+    if (kCount) wk.c[0] += 1;
+  }
+  // far lanes stay parked (next pile); near lanes join the next round
+  bool fclaim = false, claim = false;
+  if (far != 0u) fclaim = atomicOr(B.fmask + cv, far) == 0u;
+  if (near != 0u) claim = atomicOr(B.mask[rd ^ 1u] + cv, near) == 0u;
+  const u32 fm = __ballot_sync(0xFFFFFFFFu, fclaim);
+  if (fm != 0u) {
+    const u32 first = __ffs(fm) - 1u;
+    u32 pos = 0u;
+    if (lane == first) pos = atomicAdd(&C.fcount[pile_out], static_cast<u32>(__popc(fm)));
+    pos = __shfl_sync(0xFFFFFFFFu, pos, static_cast<int>(first));
+    if (fclaim) {
+      const u32 at = pos + __popc(fm & ((1u << lane) - 1u));
+      if (at < B.U) B.fpile[pile_out][at] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
+      else atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
+    }
+  }
+  const u32 cm = __ballot_sync(0xFFFFFFFFu, claim);
+  if (cm != 0u) {
+    const u32 first = __ffs(cm) - 1u;
+    u32 pos = 0u;
+    if (lane == first) pos = atomicAdd(&C.count[widx], static_cast<u32>(__popc(cm)));
+    pos = __shfl_sync(0xFFFFFFFFu, pos, static_cast<int>(first));
+    if (claim) {
+      if (kCount) wk.c[4] += 1;
+      const u32 at = pos + __popc(cm & ((1u << lane) - 1u));
+      if (at < B.U) B.queue[rd ^ 1u][at] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
+      else atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
     }
   }
 }

@@ -271,12 +271,24 @@ int bfx_resident_graph_set_weights(bfx_resident_graph *graph, const float *weigh
  * in one launch.  engines_out[count]; *measured (may be NULL) = batches that
  * were timed rather than found in the cache. */
 int bfx_autotune(bfx_workspace *ws, uint32_t count, const bfx_batch_description *batches,
-                 const bfx_gpu_run_options *base, uint32_t trials, uint32_t *engines_out, uint32_t *measured);
+                 const bfx_gpu_run_options *base, uint32_t trials, uint32_t *engines_out, float *deltas_out,
+                 uint32_t *measured);
 /* Forgets all cached autotuner choices. */
 int bfx_autotune_reset(void);
 /* Sets the per-batch engines used by BFX_ENGINE_AUTO launches of the prepared
  * batches (count must equal the prepared batch count at execute time). */
 int bfx_set_batch_engines(bfx_workspace *ws, uint32_t count, const uint32_t *engines);
+/* Near/far frontier (a bfx scheduling option, results unchanged): per-batch
+ * threshold steps for frontier-push batches.  A frontier round relaxes only
+ * improvements below the batch's current threshold and parks the others;
+ * when nothing below it is left the threshold advances by the step and the
+ * parked (vertex, lane) pairs now below it rejoin -- fewer redundant
+ * relaxations than a plain frontier.  +inf (or an empty set) = plain
+ * frontier; steps must be positive.  count must equal the prepared batch
+ * count at execute time. */
+int bfx_set_batch_deltas(bfx_workspace *ws, uint32_t count, const float *deltas);
+/* {mean edge weight, edge count} of the workspace's resident graph. */
+int bfx_workspace_graph_stats(bfx_workspace *ws, double out[2]);
 
 /* Failure-detection self-test of the engines' grid barrier (no counterpart
  * in the reference, whose cooperative barrier cannot time out).  Runs
@@ -318,7 +330,7 @@ int bfx_run_query(bfx_workspace *ws, uint32_t source_count, const uint32_t *sour
  * (labels, pending masks, frontier queues, tile table, batch records, launch
  * state) lives in one fixed 32 MiB array in the library's device memory, so
  * the call allocates nothing.  Limits and rules:
- *  - the whole query image must fit in 32 MiB (about 44 bytes per selected
+ *  - the whole query image must fit in 32 MiB (about 72 bytes per selected
  *    vertex plus 8 bytes per graph tile); larger queries fail with
  *    BFX_ERR_OVERFLOW and a message -- use bfx_run_query for them;
  *  - every GPU that loads libbfx.so holds the 32 MiB array until exit;

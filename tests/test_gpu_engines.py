@@ -236,3 +236,47 @@ def test_autotuned_mixed_engines_one_launch(gpu):
         check_batches(layout, descs, lanes, st, labels, orc)
     ws.close()
     res.close()
+
+
+@pytest.mark.parametrize("step", [0.5, 3.0, 40.0])
+def test_near_far_frontier_bit_exact(gpu, c1, step):
+    """Near/far frontier with a threshold step (several splits on c1's uint
+    costs): same labels as the oracle, fewer or equal relaxations."""
+    layout = c1.layout
+    d = bfx.make_description(layout, c1.queries, 8)
+    layout2, grid = workloads.build_graph("c2", scale_tiles=(32, 32))
+    qs = workloads.box_queries(layout2, grid, 40, 2, 16, seed=23)
+    plan = bfx.make_overlapping_batch_plan(layout2, qs, bfx.BatchPlannerPolicy(32, 0, 1, 8, 1, narrow_lanes=True))
+    for lay, descs, lanes in ((layout, [d], [c1.queries]),
+                              (layout2, plan.descriptions(),
+                               [[qs[i] if i != bfx.NO_EDGE else None for i in x.query_index_by_lane]
+                                for x in plan.descriptions()])):
+        res = bfx.ResidentDeviceGraph.upload_once(lay)
+        ws = bfx.Workspace(res)
+        ws.prepare(descs)
+        ws.set_batch_deltas([step] * len(descs))
+        ws.execute(bfx.GpuRunOptions(instrumentation=1))
+        st = ws.fetch_statuses()
+        labels = [ws.download_labels(b, x.lane_width) for b, x in enumerate(descs)]
+        check_batches(lay, descs, lanes, st, labels, Oracle.from_layout(lay))
+        ws.close()
+        res.close()
+
+
+def test_autotuner_with_near_far_candidates(gpu):
+    layout, grid = workloads.build_graph("c2", scale_tiles=(32, 32))
+    qs = workloads.box_queries(layout, grid, 20, 4, 20, seed=29)
+    plan = bfx.make_overlapping_batch_plan(layout, qs, bfx.BatchPlannerPolicy(32, 0, 1, 8, 1, narrow_lanes=True))
+    descs = plan.descriptions()
+    res = bfx.ResidentDeviceGraph.upload_once(layout)
+    ws = bfx.Workspace(res)
+    bfx.load().bfx_autotune_reset()
+    engines, _ = ws.autotune(descs)
+    assert len(ws.tuned_deltas) == len(descs) and all(x > 0 for x in ws.tuned_deltas)
+    ws.execute(bfx.GpuRunOptions(engine=bfx.ENGINE_AUTO))
+    st = ws.fetch_statuses()
+    labels = [ws.download_labels(b, x.lane_width) for b, x in enumerate(descs)]
+    lanes = [[qs[i] if i != bfx.NO_EDGE else None for i in x.query_index_by_lane] for x in descs]
+    check_batches(layout, descs, lanes, st, labels, Oracle.from_layout(layout))
+    ws.close()
+    res.close()
