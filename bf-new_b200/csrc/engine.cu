@@ -33,6 +33,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -168,6 +169,7 @@ __global__ void init_kernel(LaunchParams p) {
     c.count[0] = c.count[1] = c.count[2] = 0u;
     c.changed[0] = p.batches[tid].valid;
     c.fcount[0] = c.fcount[1] = c.fcount[2] = 0u;
+    c.fmin[0] = c.fmin[1] = c.fmin[2] = 0xFFFFFFFFu;
     c.gen[0] = c.gen[1] = 0u;
     c.delta = p.deltas ? p.deltas[tid] : dev::kInfBits;
     c.tau[0] = c.tau[1] = c.delta;
@@ -382,7 +384,7 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
         }
       } else {
         const u32 f = min(dev::ld_cg(&C.fcount[g % 3u]), B.U);
-        const u32 tau_next = __float_as_uint(__fadd_rn(__uint_as_float(tau), __uint_as_float(C.delta)));
+        const u32 tau_next = split_threshold(C, tau, g % 3u);
         split_group<kCount>(p, B, C, item, f, r & 1u, widx, tau_next, g % 3u, (g + 1u) % 3u, wk);
       }
     } else if (eng == BFX_ENGINE_JACOBI_PULL) {
@@ -410,8 +412,9 @@ __device__ void round_bookkeeping(const LaunchParams& p, u32 r) {
       work = near || split;
       if (split) {
         C.fcount[(g + 2u) % 3u] = 0u;  // idle since two splits ago; the next split writes it
+        C.fmin[(g + 2u) % 3u] = 0xFFFFFFFFu;
         C.gen[(r + 1u) & 1u] = g + 1u;
-        C.tau[(r + 1u) & 1u] = __float_as_uint(__fadd_rn(__uint_as_float(tau), __uint_as_float(C.delta)));
+        C.tau[(r + 1u) & 1u] = split_threshold(C, tau, g % 3u);
       } else {
         C.gen[(r + 1u) & 1u] = g;
         C.tau[(r + 1u) & 1u] = tau;
@@ -440,12 +443,18 @@ __global__ void __launch_bounds__(512, 3) persistent_kernel(LaunchParams p) {
   const u32 nblocks = gridDim.x;
   Work wk;
   wk.zero();
+  const u64 t0 = dev::global_ns();
   u32 r = 0;
   for (;; ++r) {
     const u32 total = round_work(p, r, prefix);
     if (total == 0u || r >= p.max_rounds) break;
     if (blockIdx.x == 0) round_bookkeeping(p, r);
     round_body<kCount>(p, r, prefix, wk);
+    // Past the launch budget block 0 raises the barrier's abort before it
+    // arrives, so every block leaves after this round.
+    if (blockIdx.x == 0 && threadIdx.x == 0 && dev::global_ns() - t0 > p.budget_ns) {
+      atomicExch(&p.run->sync.abort, 1u);
+    }
     if (!dev::grid_barrier(&p.run->sync, nblocks, kBarrierTimeoutNs)) {
       if (threadIdx.x == 0) atomicExch(&p.run->abort, 1u);
       break;
@@ -1090,6 +1099,7 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   p.engine = o.engine;
   p.per_lane = o.enable_per_lane_convergence;
   p.max_rounds = o.maximum_rounds;
+  p.budget_ns = kLaunchBudgetNs;
   p.engines = nullptr;
   p.deltas = nullptr;
   if (!ws->batch_deltas.empty()) {
@@ -1178,11 +1188,17 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
     std::uint32_t* const done_host = static_cast<std::uint32_t*>(ws->status_host.ptr);
     const std::uint64_t max_chunks = (o.maximum_rounds + K - 1) / K + 1;
     ws->last_host_checks = 0;
+    const auto t0 = std::chrono::steady_clock::now();
     for (std::uint64_t c = 0; c < max_chunks; ++c) {
       BFX_CUDA(cudaMemcpyAsync(done_host, &p.run->done, 4, cudaMemcpyDeviceToHost, ws->stream));
       BFX_CUDA(cudaStreamSynchronize(ws->stream));
       ++ws->last_host_checks;
       if (*done_host) break;
+      if (std::chrono::steady_clock::now() - t0 > std::chrono::nanoseconds(kLaunchBudgetNs)) {
+        // same outcome as a persistent launch past its budget: device_failure
+        BFX_CUDA(cudaMemsetAsync(&p.run->abort, 1, 1, ws->stream));
+        break;
+      }
       BFX_CUDA(cudaGraphLaunch(ws->chunk_exec, ws->stream));
       launches += 2ull * K;
     }
@@ -1592,6 +1608,7 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
     p.engine = options->engine;
     p.per_lane = options->enable_per_lane_convergence;
     p.max_rounds = options->maximum_rounds;
+    p.budget_ns = bfx::kLaunchBudgetNs;
     int sms = 0;
     BFX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, graph->device));
     bfx::init_kernel<<<sms * 8, 256>>>(p);

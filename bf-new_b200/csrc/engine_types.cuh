@@ -70,10 +70,22 @@ struct DCtl {
   // Near/far frontier: far pile sizes by generation % 3; generation and
   // threshold (float bits) double-buffered by round parity.
   u32 fcount[3];
+  u32 fmin[3];     // smallest parked distance per far pile (float bits)
   u32 gen[2];
   u32 tau[2];
   u32 delta;       // threshold step (float bits); +inf = plain frontier
 };
+
+// Threshold of the split that consumes far pile `pile`: tau + delta, raised
+// above the pile's smallest parked distance so every split moves at least
+// one (vertex, lane) to the near frontier (progress even when tau + delta
+// rounds back to tau).
+__device__ __forceinline__ u32 split_threshold(const DCtl& C, u32 tau, u32 pile) {
+  const u32 stepped = __float_as_uint(__fadd_rn(__uint_as_float(tau), __uint_as_float(C.delta)));
+  const u32 fmin = C.fmin[pile];
+  const u32 above = fmin >= 0x7F800000u ? fmin : fmin + 1u;  // next float above fmin
+  return stepped > above ? stepped : above;
+}
 
 struct DRun {
   dev::GridSync sync;
@@ -99,6 +111,7 @@ struct Work {
 
 constexpr u32 kMaxBatchesPerLaunch = 4096;
 constexpr u64 kBarrierTimeoutNs = 2000000000ull;  // 2 s per barrier wait
+constexpr u64 kLaunchBudgetNs = 30000000000ull;   // 30 s per relaxation launch
 
 struct LaunchParams {
   DGraph g;
@@ -111,6 +124,7 @@ struct LaunchParams {
   u32 per_lane;
   u32 reserved;
   u64 max_rounds;
+  u64 budget_ns;         // wall-clock budget of one relaxation launch; past it the launch stops (device_failure)
   const u32* engines;    // [nb] per-batch engine (autotuned launches) or null
   const u32* deltas;     // [nb] near/far threshold steps (float bits) or null (plain frontier)
 };

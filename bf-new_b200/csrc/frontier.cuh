@@ -68,7 +68,7 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
   u64* const queue_w = B.queue[rd ^ 1u];
   for (u32 st = 0; st < steps; ++st) {
     const u32 e = rb + st * G + slot;
-    u32 bits = 0u, fbits = 0u, cdst = 0u, dstv = 0u;
+    u32 bits = 0u, fbits = 0u, cdst = 0u, dstv = 0u, fd = 0xFFFFFFFFu;
     if (has_lane && e < re) {
       const uint4 rec = __ldg(p.g.csr + e);
       const uint2 dt = B.tiles[rec.w];
@@ -83,7 +83,12 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
           dev::red_min(target, cand);
           if (dev::hi(cand) < dev::hi(cur)) {
             // near: below this round's threshold; far: parked until a split
-            if (dev::hi(cand) < tau_bits) bits = 1u << ql; else fbits = 1u << ql;
+            if (dev::hi(cand) < tau_bits) {
+              bits = 1u << ql;
+            } else {
+              fbits = 1u << ql;
+              fd = dev::hi(cand);
+            }
           }
           if (kCount) {
             wk.c[6] += 1;
@@ -97,6 +102,9 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
       fbits |= __shfl_xor_sync(0xFFFFFFFFu, fbits, o);
     }
     if (__any_sync(0xFFFFFFFFu, fbits != 0u)) {
+      // smallest parked distance of the pile (one atomic per warp step)
+      fd = __reduce_min_sync(0xFFFFFFFFu, fd);
+      if (lane == 0u) atomicMin(&C.fmin[pile], fd);
       bool fclaim = false;
       if (j == 0u && fbits != 0u) fclaim = atomicOr(B.fmask + cdst, fbits) == 0u;
       const u32 fm = __ballot_sync(0xFFFFFFFFu, fclaim);
@@ -137,7 +145,7 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
 }
 
 // Split round of the near/far frontier: the batch's near frontier is empty,
-// so the threshold advances by delta and every parked (vertex, lane) of the
+// so the threshold advances (split_threshold) and every parked (vertex, lane) of the
 // current far pile is re-examined: lanes whose label is now below the new
 // threshold join the next round's near frontier, the rest move to the next
 // pile.  One thread per far entry; claims are warp-aggregated.  The batch
@@ -148,7 +156,7 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const DBatch&
                                             u32 rd, u32 widx, u32 tau_next, u32 pile_in, u32 pile_out, Work& wk) {
   const u32 lane = lane_id();
   const u32 entry = item * 32u + lane;
-  u32 near = 0u, far = 0u, v = 0u, cv = 0u;
+  u32 near = 0u, far = 0u, v = 0u, cv = 0u, fd = 0xFFFFFFFFu;
   if (entry < count) {
     const u64 q = dev::ld_cg(B.fpile[pile_in] + entry);
     v = static_cast<u32>(q);
@@ -158,7 +166,12 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const DBatch&
     for (u32 m = bits; m != 0u; m &= m - 1u) {
       const u32 l = __ffs(m) - 1u;
       const u32 d = dev::hi(dev::ld_cg(B.dist[0] + ((static_cast<u64>(cv) << B.shift) + l)));
-      if (d < tau_next) near |= 1u << l; else far |= 1u << l;
+      if (d < tau_next) {
+        near |= 1u << l;
+      } else {
+        far |= 1u << l;
+        fd = min(fd, d);
+      }
     }
     if (kCount) wk.c[0] += 1;
   }
@@ -166,6 +179,8 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const DBatch&
   bool fclaim = false, claim = false;
   if (far != 0u) fclaim = atomicOr(B.fmask + cv, far) == 0u;
   if (near != 0u) claim = atomicOr(B.mask[rd ^ 1u] + cv, near) == 0u;
+  fd = __reduce_min_sync(0xFFFFFFFFu, fd);
+  if (lane == 0u && fd != 0xFFFFFFFFu) atomicMin(&C.fmin[pile_out], fd);
   const u32 fm = __ballot_sync(0xFFFFFFFFu, fclaim);
   if (fm != 0u) {
     const u32 first = __ffs(fm) - 1u;
