@@ -40,6 +40,8 @@ import numpy as np  # noqa: E402
 
 METRIC = "batched SSSP queries/s (256 uneven regional queries, 2.1M V / 16.8M E, one persistent launch)"
 METRIC_C3 = "batched SSSP queries/s (64 full-graph sources, 16.8M V / 168M E, one persistent launch)"
+METRIC_C5 = "batched SSSP queries/s (4,096 regional + 16 full-graph queries, 16.8M V / 168M E, autotuned)"
+METRICS = {"c2": METRIC, "c3": METRIC_C3, "c5": METRIC_C5}
 
 
 def log(*a):
@@ -173,7 +175,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="bfx", choices=["bfx", "reference"])
     ap.add_argument("--engine", default="auto", choices=["auto", "frontier", "jacobi", "dense"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=None)
     args = ap.parse_args()
@@ -199,18 +201,31 @@ def main():
     t0 = time.time()
     g, order, gstats = bfx.synth_graph(**workloads.GRAPHS[args.workload])
     layout = bfx.build_device_graph_layout(g, order)
+    # query classes: (queries, plain-engine sample size) -- the plain per-query
+    # rate is extrapolated class by class from its sample
     if args.workload == "c2":
         grid = (128, 128)
         queries = workloads.box_queries(layout, grid, args.queries or 256, 4, 64, 202 + 1000 * rank)
+        classes = [(queries, 64)]
         policy = bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True)
         workload_desc = ("c2: 256 uneven regional queries (box side U[4,64] tiles) on 128x128 tiles x 128 nodes, "
                          "2,097,152 V / 16,777,216 E, f32 lognormal costs")
-    else:
+    elif args.workload == "c3":
         grid = (256, 256)
         queries = workloads.full_graph_queries(layout, grid, args.queries or 64, 303 + 1000 * rank)
+        classes = [(queries, 4)]
         policy = bfx.BatchPlannerPolicy(32, 0, 1, 64, 1)
         workload_desc = ("c3: 64 full-graph sources in batches of 32 on 256x256 tiles x 256 nodes, "
                          "16,777,216 V / 167,772,160 E, uint costs U[1,255]")
+    else:
+        grid = (256, 256)
+        regional = workloads.box_queries(layout, grid, args.queries or 4096, 2, 16, 505 + 1000 * rank)
+        full = workloads.full_graph_queries(layout, grid, 16, 506 + 1000 * rank, first_id=len(regional))
+        queries = regional + full
+        classes = [(regional, 64), (full, 2)]
+        policy = bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True)
+        workload_desc = ("c5: 4,096 regional queries (box side U[2,16] tiles) + 16 full-graph sources on 256x256 "
+                         "tiles x 256 nodes, 16,777,216 V / 167,772,160 E, uint costs U[1,255]")
     t1 = time.time()
     plan = bfx.make_overlapping_batch_plan(layout, queries, policy)
     descs = plan.descriptions()
@@ -303,17 +318,21 @@ def main():
     h2d, d2h = ws.transfer_bytes()
 
     # ---- plain per-query engine (one query per launch sequence) on a sample
-    sample_q = queries[:64]
-    barrier()
-    s3 = torch.cuda.Event(enable_timing=True)
-    e3 = torch.cuda.Event(enable_timing=True)
-    s3.record(stream)
-    for q in sample_q:
-        ws.run_query(q.sources, q.targets, q.selected_tiles, bfx.GpuRunOptions(engine=bfx.ENGINE_FRONTIER_PUSH))
-    e3.record(stream)
-    barrier()
-    plain_ms = s3.elapsed_time(e3)
-    plain_qps = len(sample_q) / (plain_ms / 1000)
+    # of each query class; the whole set's time is extrapolated per class
+    plain_total_s, plain_sampled = 0.0, 0
+    for members, n in classes:
+        sample_q = members[:n]
+        barrier()
+        s3 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        s3.record(stream)
+        for q in sample_q:
+            ws.run_query(q.sources, q.targets, q.selected_tiles, bfx.GpuRunOptions(engine=bfx.ENGINE_FRONTIER_PUSH))
+        e3.record(stream)
+        barrier()
+        plain_total_s += s3.elapsed_time(e3) / 1000 / len(sample_q) * len(members)
+        plain_sampled += len(sample_q)
+    plain_qps = len(queries) / plain_total_s
 
     nq = len(queries) * world
     ms_per_step = dev_ms / args.steps
@@ -337,7 +356,7 @@ def main():
                 traffic = int(float(line.split(":")[1]))
 
     line = {
-        "metric": METRIC if args.workload == "c2" else METRIC_C3, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "metric": METRICS[args.workload], "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": workload_desc,
@@ -346,11 +365,12 @@ def main():
                    "engines_chosen": None if engines_chosen is None else
                    {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
                    "control": "persistent_cooperative", "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (graph 0.54 GB + labels), no flush"},
+                   "l2": "inputs larger than L2 (graph %s GB + labels), no flush" % (
+                       "0.54" if args.workload == "c2" else "5.4")},
         "gteps": lane_edges * world / (ms_per_step / 1000) / 1e9,
         "reached_lanes": reached,
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "plain_per_query": {"value": plain_qps, "unit": "queries/s", "sample": len(sample_q),
+        "plain_per_query": {"value": plain_qps, "unit": "queries/s", "sample": plain_sampled,
                             "batched_speedup": value / world / plain_qps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_src, "kernel": "persistent_kernel<false> (frontier)",

@@ -580,11 +580,12 @@ class Workspace:
         _check(load().bfx_workspace_transfer_bytes(self._h, out))
         return int(out[0]), int(out[1])
 
-    def compact_paths(self, first_batch: int = 0, batch_count: int | None = None) -> list:
+    def compact_paths(self, first_batch: int = 0, batch_count: int | None = None, raw: bool = False):
         """ReusableCompactPathWorkspace::reconstruct: per target (description
         order, batches [first_batch, first_batch+batch_count)) a dict with the
         summary fields and, for complete targets, vertices (source first),
-        distance labels and stable edge ids."""
+        distance labels and stable edge ids.  raw=True returns the summaries
+        as one structured array plus the flat payload arrays instead."""
         lib = load()
         n = (self.batch_count - first_batch) if batch_count is None else batch_count
         total = sum(self._keep[b].targets.shape[0] for b in range(first_batch, first_batch + n)) \
@@ -599,6 +600,9 @@ class Workspace:
         labels = np.zeros(max(nv, 1), np.float32)
         edges = np.zeros(max(ne, 1), np.uint32)
         _check(lib.bfx_compact_path_payload(self._h, _ptr(verts), _ptr(labels, f32), _ptr(edges)))
+        if raw:
+            return {"summaries": np.ctypeslib.as_array(summ)[:total].copy(), "vertices": verts[:nv],
+                    "labels": labels[:nv], "edges": edges[:ne]}
         out, vo, eo = [], 0, 0
         for i in range(total):
             s = summ[i]

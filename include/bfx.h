@@ -262,13 +262,15 @@ int bfx_resident_graph_set_weights(bfx_resident_graph *graph, const float *weigh
 
 /* ---- engine autotuner ----------------------------------------------------------
  * No counterpart in the reference (its engine shootout, src/engine_shootout.cpp,
- * only catalogues configurations).  Picks frontier push, Jacobi pull or dense
- * chaotic push per batch by timing each engine on the batch alone (best of
- * `trials` device timings), caching the choice per batch shape (lane width,
- * valid lanes, magnitude of union vertices and tiles).  Leaves the workspace
- * prepared with all `count` batches and their engines, so bfx_execute with
- * options->engine == BFX_ENGINE_AUTO relaxes each batch with its own engine
- * in one launch.  engines_out[count]; *measured (may be NULL) = batches that
+ * only catalogues configurations).  Picks, per batch, frontier push (plain or
+ * near/far with a threshold step of 2, 8 or 32 mean edge weights), Jacobi
+ * pull or dense chaotic push by timing each candidate on the batch alone
+ * (best of `trials` device timings), caching the choice per batch shape (lane
+ * width, valid lanes, magnitude of union vertices and tiles).  Leaves the
+ * workspace prepared with all `count` batches and their engines and steps, so
+ * bfx_execute with options->engine == BFX_ENGINE_AUTO relaxes each batch with
+ * its own engine in one launch.  engines_out[count]; deltas_out[count] (may be
+ * NULL) = chosen steps (+inf = plain); *measured (may be NULL) = batches that
  * were timed rather than found in the cache. */
 int bfx_autotune(bfx_workspace *ws, uint32_t count, const bfx_batch_description *batches,
                  const bfx_gpu_run_options *base, uint32_t trials, uint32_t *engines_out, float *deltas_out,
@@ -283,7 +285,9 @@ int bfx_set_batch_engines(bfx_workspace *ws, uint32_t count, const uint32_t *eng
  * improvements below the batch's current threshold and parks the others;
  * when nothing below it is left the threshold advances by the step and the
  * parked (vertex, lane) pairs now below it rejoin -- fewer redundant
- * relaxations than a plain frontier.  +inf (or an empty set) = plain
+ * relaxations than a plain frontier.  A split raises the threshold at least
+ * above the smallest parked distance, so every split makes progress.  +inf
+ * (or an empty set) = plain
  * frontier; steps must be positive.  count must equal the prepared batch
  * count at execute time. */
 int bfx_set_batch_deltas(bfx_workspace *ws, uint32_t count, const float *deltas);

@@ -135,3 +135,80 @@ def test_adjoint_uses_device_weights(gpu, nets):
     np.testing.assert_array_equal(grad, og)
     for p, (q, t) in zip(paths, order):
         assert np.float32(p["distance"]).view(np.uint32) == dists[q.query_id][int(t)]
+
+
+# ---- the 512-net configuration: c1 graph with lognormal float costs, 512 nets
+# of one source and U[1,32] targets in a box of side U[8,48] tiles clipped to
+# 32; target gradients U(0,1) f32 and all ones.
+
+@pytest.fixture(scope="module")
+def nets512():
+    layout, grid = workloads.build_graph("c1f")
+    qs = workloads.box_queries(layout, grid, 512, 8, 48, seed=0xC4, targets=(1, 32), clip=32)
+    return layout, qs
+
+
+@pytest.mark.parametrize("kind", ["uniform", "ones"])
+def test_512_nets_adjoint_equals_cpu_tree_walk_bitwise(gpu, nets512, kind):
+    layout, qs = nets512
+    rng = np.random.default_rng(0xC4)
+    gvals = {(q.query_id, int(t)): (np.float32(1) if kind == "ones" else rng.random(dtype=np.float32))
+             for q in qs for t in q.targets}
+    grad, paths, order, g = run_adjoint(layout, qs, gvals)
+    og, dists = oracle_grad(layout, order, g)
+    np.testing.assert_array_equal(grad.view(np.uint32), og.view(np.uint32))
+    for p, (q, t) in zip(paths, order):
+        assert np.float32(p["distance"]).view(np.uint32) == dists[q.query_id][int(t)]
+
+
+def test_512_nets_adjoint_finite_differences_1000_tie_free_edges(gpu, nets512):
+    """Central differences (delta = 1e-3) of L over 1,000 edges whose
+    perturbation changes no path, against the adjoint.  L(w +- delta e_k) is
+    evaluated by the engine itself with the perturbed weights uploaded through
+    bfx_resident_graph_set_weights; the unperturbed labels are pinned to the
+    oracle by the test above."""
+    layout, qs = nets512
+    rng = np.random.default_rng(0xC4F)
+    plan = bfx.make_overlapping_batch_plan(layout, qs, bfx.BatchPlannerPolicy(32, 0, 1, 16, 1, narrow_lanes=True))
+    descs = plan.descriptions()
+    order = [(qs[int(i)], t) for d in descs for i in d.query_index_by_lane if i != bfx.NO_EDGE
+             for t in qs[int(i)].targets]
+    g = rng.random(len(order), dtype=np.float32)
+    res = bfx.ResidentDeviceGraph.upload_once(layout)
+    ws = bfx.Workspace(res)
+    opts = bfx.GpuRunOptions()
+    try:
+        ws.prepare(descs)
+        ws.execute(opts)
+        base = ws.compact_paths(raw=True)
+        grad = ws.edge_usage_adjoint(g)
+        w0 = weights_by_eid(layout)
+        delta = np.float32(1e-3)
+        used = rng.permutation(np.nonzero(grad)[0])
+        checked = skipped = 0
+        for e in used:
+            L = {}
+            for sgn in (1, -1):
+                w = w0.copy()
+                w[e] = w[e] + sgn * delta
+                res.set_weights(w)
+                ws.execute(opts)
+                cur = ws.compact_paths(raw=True)
+                if not (np.array_equal(cur["edges"], base["edges"]) and
+                        np.array_equal(cur["summaries"]["reconstruction"], base["summaries"]["reconstruction"])):
+                    break
+                d = cur["summaries"]["distance"].astype(np.float64)
+                fin = np.isfinite(d)  # unreachable targets do not enter L
+                L[sgn] = float(np.sum(g[fin].astype(np.float64) * d[fin]))
+            if len(L) != 2:
+                skipped += 1
+                continue
+            fd = (L[1] - L[-1]) / (2 * float(delta))
+            assert abs(fd - float(grad[e])) <= 0.05 * max(1.0, abs(float(grad[e]))), (int(e), fd, float(grad[e]))
+            checked += 1
+            if checked == 1000:
+                break
+        assert checked == 1000, (checked, skipped)
+    finally:
+        ws.close()
+        res.close()
