@@ -33,10 +33,16 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
     const u64 q = dev::ld_cg(B.queue[rd] + entry);
     v = static_cast<u32>(q);
     cv = static_cast<u32>(q >> 32);
-    m = dev::ld_cg(mask_r + cv);
-    rb = __ldg(p.g.csr_off + v);
-    re = __ldg(p.g.csr_off + v + 1u);
-    mask_r[cv] = 0u;
+    if (v < p.g.V && cv < B.U) {
+      m = dev::ld_cg(mask_r + cv) & B.valid;
+      rb = __ldg(p.g.csr_off + v);
+      re = __ldg(p.g.csr_off + v + 1u);
+      mask_r[cv] = 0u;
+    } else {
+      // a queue word outside the batch: record it and skip the entry
+      atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
+      v = cv = 0u;
+    }
   }
   v = __shfl_sync(0xFFFFFFFFu, v, static_cast<int>(leader));
   cv = __shfl_sync(0xFFFFFFFFu, cv, static_cast<int>(leader));
@@ -161,8 +167,13 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const DBatch&
     const u64 q = dev::ld_cg(B.fpile[pile_in] + entry);
     v = static_cast<u32>(q);
     cv = static_cast<u32>(q >> 32);
-    const u32 bits = dev::ld_cg(B.fmask + cv);
-    B.fmask[cv] = 0u;
+    u32 bits = 0u;
+    if (cv < B.U) {
+      bits = dev::ld_cg(B.fmask + cv) & B.valid;
+      B.fmask[cv] = 0u;
+    } else {
+      atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
+    }
     for (u32 m = bits; m != 0u; m &= m - 1u) {
       const u32 l = __ffs(m) - 1u;
       const u32 d = dev::hi(dev::ld_cg(B.dist[0] + ((static_cast<u64>(cv) << B.shift) + l)));
