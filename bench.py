@@ -196,7 +196,7 @@ def main():
         dist = tdist
 
     import bfx
-    from bfx import workloads
+    from bfx import replicas, workloads
 
     t0 = time.time()
     g, order, gstats = bfx.synth_graph(**workloads.GRAPHS[args.workload])
@@ -259,11 +259,7 @@ def main():
         torch.cuda.synchronize(device)
 
     def max_over_ranks(x: float) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(dist, x) if dist else x
 
     # ---- instrumented pass (untimed): algorithmic work counts + parity spot check
     ws.prepare(descs)
@@ -298,6 +294,9 @@ def main():
     dev_ms = max_over_ranks(dev_ms)
     statuses = ws.fetch_statuses()
     assert all(s.stop_reason == bfx.STOP_CONVERGED for s in statuses)
+    if dist:  # the job's one exchange: every rank's status records to every rank
+        all_statuses = replicas.gather_statuses(dist, statuses)
+        assert all(s.stop_reason == bfx.STOP_CONVERGED for part in all_statuses for s in part)
 
     # ---- end-to-end timing through the C ABI from host buffers (e2e)
     for _ in range(args.warmup):

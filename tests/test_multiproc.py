@@ -12,7 +12,7 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 import bfx
-from bfx import workloads
+from bfx import replicas, workloads
 
 
 def _worker(rank, world, port, queue):
@@ -26,16 +26,19 @@ def _worker(rank, world, port, queue):
         est = [e[3] for e in plan.estimates]
         shards = workloads.shard_batches(est, world)
         mine = shards[rank]
-        # stand-in for the per-rank status records (48-byte DeviceRunStatus)
-        recs = torch.zeros((len(plan.descriptions()), 12), dtype=torch.int32)
+        # per-rank status records (48-byte DeviceRunStatus) as a rank's
+        # workspace returns them: rounds_completed carries the batch index
+        statuses = []
         for b in mine:
-            recs[b, 0] = b + 1
-            recs[b, 1] = rank
-        gathered = [torch.zeros_like(recs) for _ in range(world)]
-        dist.all_gather(gathered, recs)
-        t = torch.tensor([1.0 + rank], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        queue.put((rank, shards, [g.numpy() for g in gathered], float(t.item()), est))
+            s = bfx.DeviceRunStatus()
+            s.rounds_completed = b + 1
+            s.error_bits = rank
+            s.stop_reason = bfx.STOP_CONVERGED
+            statuses.append(s)
+        gathered = replicas.gather_statuses(dist, statuses)
+        recs = [[(int(s.rounds_completed), int(s.error_bits), int(s.stop_reason)) for s in g] for g in gathered]
+        t = replicas.max_over_ranks(dist, 1.0 + rank)
+        queue.put((rank, shards, recs, t, est))
     finally:
         dist.barrier()
         dist.destroy_process_group()
@@ -62,6 +65,9 @@ def test_replica_shards_gather_and_max_timing():
     loads = [sum(est[b] for b in s) for s in shards0]
     assert max(loads) - min(loads) <= max(est)  # greedy bound
     for rank in range(world):
-        g = sum(out[rank][2])
-        assert np.array_equal(np.sort(g[:, 0][g[:, 0] > 0] - 1), np.arange(len(flat)))
+        recs = out[rank][2]
+        assert len(recs) == world
+        for r in range(world):  # rank r's records, in its shard order, tagged with r
+            assert [x[0] - 1 for x in recs[r]] == shards0[r]
+            assert all(x[1] == r and x[2] == bfx.STOP_CONVERGED for x in recs[r])
         assert out[rank][3] == 2.0  # max over ranks
