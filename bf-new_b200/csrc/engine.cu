@@ -373,9 +373,23 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
     const u32 item = w - prefix[b];
     const u32 eng = engine_of(p, b);
     if (eng == BFX_ENGINE_FRONTIER_PUSH) {
-      const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
-      const u32 g = dev::ld_cg(&C.gen[r & 1u]);
-      const u32 tau = dev::ld_cg(&C.tau[r & 1u]);
+      // read once per warp and broadcast: the branch below and the sizes the
+      // frontier bodies see are warp-uniform by construction
+      u32 n = 0u, g = 0u, tau = 0u, f = 0u, tau_next = 0u;
+      if (lane_id() == 0u) {
+        n = min(dev::ld_cg(&C.count[ridx]), B.U);
+        g = dev::ld_cg(&C.gen[r & 1u]);
+        tau = dev::ld_cg(&C.tau[r & 1u]);
+        if (n == 0u) {
+          f = min(dev::ld_cg(&C.fcount[g % 3u]), B.U);
+          tau_next = split_threshold(C, tau, g % 3u);
+        }
+      }
+      n = __shfl_sync(0xFFFFFFFFu, n, 0);
+      g = __shfl_sync(0xFFFFFFFFu, g, 0);
+      tau = __shfl_sync(0xFFFFFFFFu, tau, 0);
+      f = __shfl_sync(0xFFFFFFFFu, f, 0);
+      tau_next = __shfl_sync(0xFFFFFFFFu, tau_next, 0);
       if (n != 0u) {
         if (B.W <= 8u) {
           frontier_group<kCount, 8>(p, B, C, item, n, r & 1u, widx, tau, g % 3u, wk);
@@ -383,8 +397,6 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
           frontier_group<kCount, 32>(p, B, C, item, n, r & 1u, widx, tau, g % 3u, wk);
         }
       } else {
-        const u32 f = min(dev::ld_cg(&C.fcount[g % 3u]), B.U);
-        const u32 tau_next = split_threshold(C, tau, g % 3u);
         split_group<kCount>(p, B, C, item, f, r & 1u, widx, tau_next, g % 3u, (g + 1u) % 3u, wk);
       }
     } else if (eng == BFX_ENGINE_JACOBI_PULL) {

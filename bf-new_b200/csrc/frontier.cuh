@@ -70,6 +70,11 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
   }
   const u32 steps_mine = live ? (re - rb + G - 1u) / G : 0u;
   const u32 steps = __reduce_max_sync(0xFFFFFFFFu, steps_mine);
+  // Sub-group sizes differ between the entries of one warp, so the OR
+  // combine runs the warp's largest trip count (every full-mask shuffle is
+  // executed by all 32 threads) and each thread keeps only the partners
+  // inside its own sub-group.
+  const u32 kp_warp = __reduce_max_sync(0xFFFFFFFFu, kp);
   u32* const mask_w = B.mask[rd ^ 1u];
   u64* const queue_w = B.queue[rd ^ 1u];
   for (u32 st = 0; st < steps; ++st) {
@@ -103,9 +108,13 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
         }
       }
     }
-    for (u32 o = 1; o < kp; o <<= 1) {
-      bits |= __shfl_xor_sync(0xFFFFFFFFu, bits, o);
-      fbits |= __shfl_xor_sync(0xFFFFFFFFu, fbits, o);
+    for (u32 o = 1; o < kp_warp; o <<= 1) {
+      const u32 xb = __shfl_xor_sync(0xFFFFFFFFu, bits, o);
+      const u32 xf = __shfl_xor_sync(0xFFFFFFFFu, fbits, o);
+      if (o < kp) {
+        bits |= xb;
+        fbits |= xf;
+      }
     }
     if (__any_sync(0xFFFFFFFFu, fbits != 0u)) {
       // smallest parked distance of the pile (one atomic per warp step)
