@@ -22,6 +22,7 @@
 // terminal slices, dense tile lane masks and one vertex range per union tile.
 #include "bfx_host.h"
 #include "bfx_internal.hpp"
+#include "host_region.hpp"
 
 #include <algorithm>
 #include <bit>
@@ -47,64 +48,6 @@ int compare(const Fraction& a, const Fraction& b) {
   const unsigned __int128 l = static_cast<unsigned __int128>(a.num) * b.den;
   const unsigned __int128 r = static_cast<unsigned __int128>(b.num) * a.den;
   return l < r ? -1 : (l > r ? 1 : 0);
-}
-
-struct RegionIndex {
-  u32 T{};
-  std::vector<u64> vertex_counts;
-  std::vector<u32> adj_offsets;
-  std::vector<u32> adj_tiles;
-  std::vector<u64> adj_edges;
-
-  u64 vertices(const std::vector<u32>& tiles) const {
-    u64 n = 0;
-    for (u32 t : tiles) n += vertex_counts[t];
-    return n;
-  }
-  // Edges whose endpoints both lie in the tile set marked in `member`.
-  u64 edges(const std::vector<u32>& tiles, const std::vector<std::uint8_t>& member) const {
-    u64 n = 0;
-    for (u32 t : tiles) {
-      for (u32 k = adj_offsets[t]; k < adj_offsets[t + 1]; ++k) {
-        if (member[adj_tiles[k]]) n += adj_edges[k];
-      }
-    }
-    return n;
-  }
-};
-
-RegionIndex make_region_index(const bfx_device_graph_layout32& g) {
-  RegionIndex r;
-  r.T = g.tile_count;
-  r.vertex_counts.assign(r.T, 0U);
-  for (u32 v = 0; v < g.vertex_count; ++v) ++r.vertex_counts[g.owner_tiles[v]];
-  std::vector<std::vector<std::pair<u32, u64>>> per(r.T);
-  for (u32 v = 0; v < g.vertex_count; ++v) {
-    const u32 st = g.owner_tiles[v];
-    for (u32 run = g.csr_row_run_offsets[v]; run < g.csr_row_run_offsets[v + 1]; ++run) {
-      per[st].emplace_back(g.csr_run_destination_tiles[run],
-                           g.csr_run_edge_offsets[run + 1] - g.csr_run_edge_offsets[run]);
-    }
-  }
-  r.adj_offsets.assign(r.T + 1, 0U);
-  for (u32 t = 0; t < r.T; ++t) {
-    auto& lst = per[t];
-    std::sort(lst.begin(), lst.end());
-    std::vector<std::pair<u32, u64>> merged;
-    for (const auto& p : lst) {
-      if (!merged.empty() && merged.back().first == p.first) {
-        merged.back().second += p.second;
-      } else {
-        merged.push_back(p);
-      }
-    }
-    r.adj_offsets[t + 1] = r.adj_offsets[t] + static_cast<u32>(merged.size());
-    for (const auto& p : merged) {
-      r.adj_tiles.push_back(p.first);
-      r.adj_edges.push_back(p.second);
-    }
-  }
-  return r;
 }
 
 struct Feature {

@@ -275,3 +275,21 @@ class Ref:
         wall = self.lib.ref_time_dijkstra(C.c_int(h), u32(len(q)), _p(q), u32(threads), C.byref(ind),
                                           C.byref(ss), C.byref(edges))
         return {"wall_s": wall, "induced_s": ind.value, "sssp_s": ss.value, "edges": int(edges.value)}
+
+    def expansion_run(self, h, nq: int, engine: int, policy: tuple, schedule_kind: int, fixed_ring: int,
+                      hybrid_count: int, maximum_expansions: int, terminal_policy: int, tile_cap: int,
+                      max_rounds: int = 1 << 40) -> dict:
+        """Reference run_host_batched_expansion over all queries of case h
+        (src/batched_expansion.cpp:1681): outcomes in query-id order."""
+        params = np.array([engine, *policy, schedule_kind, fixed_ring, hybrid_count, maximum_expansions,
+                           terminal_policy], np.uint64)
+        outc = np.zeros(12 * nq, np.uint64)
+        tiles = np.zeros(tile_cap, np.uint32)
+        metrics = np.zeros(24, np.uint64)
+        hist = np.zeros(64, np.uint64)
+        counts = np.zeros(2, np.uint64)
+        self._chk(self.lib.ref_expansion_run(C.c_int(h), _p(params, u64), u64(max_rounds), _p(outc, u64),
+                                             _p(tiles), u64(tile_cap), _p(metrics, u64), _p(hist, u64),
+                                             _p(counts, u64)))
+        return {"outcomes": outc.reshape(nq, 12), "tiles": tiles[:int(counts[0])], "metrics": metrics,
+                "histogram": hist[:int(counts[1])]}

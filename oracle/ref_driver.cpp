@@ -15,12 +15,14 @@
 //   reconstruct_compact_path_payload           src/compact_paths.cpp:540
 //   make_batch_query_features / make_overlapping_batch_plan  src/batch_plan.cpp:578 / :680
 //   prepare_batch_device_description           src/batch_layout.cpp:1056
+//   run_host_batched_expansion                 src/batched_expansion.cpp:1681
 //   run_host_batched_{frontier_push,jacobi_pull,dense_chaotic_push}
 //       src/batched_frontier_push.cpp:648, src/batched_jacobi_pull.cpp:572,
 //       src/batched_dense_chaotic_push.cpp:569
 // Fixture suites are included from the reference's tests/ directory.
 
 #include "bfnew/batch_layout.hpp"
+#include "bfnew/batched_expansion.hpp"
 #include "bfnew/batch_plan.hpp"
 #include "bfnew/batched_dense_chaotic_push.hpp"
 #include "bfnew/batched_frontier_push.hpp"
@@ -628,6 +630,79 @@ double ref_time_dijkstra(int h, std::uint32_t nq, const std::uint32_t* qidx,
   if (sssp_seconds) *sssp_seconds = sd;
   if (edges_out) *edges_out = se;
   return wall;
+}
+
+// Reference expansion loop (run_host_batched_expansion) over all queries of
+// the case.  params = {engine, lane_width, jn, jd, in, id, schedule_kind,
+// fixed_ring_size, hybrid_count, maximum_expansions, terminal_policy}.
+// Per outcome (query-id order) out_outcomes receives 12 u64 fields:
+// {query_id, disposition, attempts, scheduled, total, fallback, generation,
+// tile_count, vertex_count, edge_count, stop_reason, error_bits};
+// out_tiles the concatenated final tiles (capacity tile_cap); out_metrics
+// 24 u64 counters in bfx_expansion_metrics order; out_hist up to 64 entries
+// (count in out_counts[1]).  out_counts[0] = total tiles written.
+int ref_expansion_run(int h, const std::uint64_t* params, std::uint64_t max_rounds, std::uint64_t* out_outcomes,
+                      std::uint32_t* out_tiles, std::uint64_t tile_cap, std::uint64_t* out_metrics,
+                      std::uint64_t* out_hist, std::uint64_t* out_counts) {
+  return guarded([&]() -> int {
+    RefCase* c = get(h);
+    if (!c) throw std::invalid_argument{"bad handle"};
+    const WeightedGraph& g = c->partitioned->graph;
+    BatchedExpansionOptions o;
+    o.run_options.engine = static_cast<EngineKind>(params[0]);
+    o.run_options.maximum_rounds = max_rounds;
+    o.planner_policy.lane_width = static_cast<std::uint32_t>(params[1]);
+    o.planner_policy.minimum_jaccard_numerator = static_cast<std::uint32_t>(params[2]);
+    o.planner_policy.minimum_jaccard_denominator = static_cast<std::uint32_t>(params[3]);
+    o.planner_policy.maximum_union_inflation_numerator = static_cast<std::uint32_t>(params[4]);
+    o.planner_policy.maximum_union_inflation_denominator = static_cast<std::uint32_t>(params[5]);
+    o.execution_configuration_fingerprint = 1U;
+    o.schedule.kind = static_cast<ExpansionScheduleKind>(params[6]);
+    o.schedule.fixed_ring_size = static_cast<std::uint32_t>(params[7]);
+    o.schedule.hybrid_small_expansion_count = static_cast<std::uint32_t>(params[8]);
+    o.maximum_expansions = static_cast<std::uint32_t>(params[9]);
+    o.terminal_policy = static_cast<ExpansionTerminalPolicy>(params[10]);
+    const BatchedExpansionRunResult r =
+        run_host_batched_expansion(g, c->partitioned->tiles, c->runs, c->layout, c->queries, o);
+    std::uint64_t tiles_written = 0;
+    for (std::size_t i = 0; i < r.queries.size(); ++i) {
+      const ExpansionQueryOutcome& q = r.queries[i];
+      std::uint64_t* f = out_outcomes + 12 * i;
+      f[0] = q.final_query.query_id.value();
+      f[1] = static_cast<std::uint64_t>(q.disposition);
+      f[2] = q.attempts;
+      f[3] = q.scheduled_expansions;
+      f[4] = q.total_expansions;
+      f[5] = q.used_full_region_fallback ? 1U : 0U;
+      f[6] = q.final_query.expansion_generation;
+      f[7] = q.final_query.selected_tiles.size();
+      f[8] = q.selected_vertex_count;
+      f[9] = q.selected_edge_count;
+      f[10] = q.terminal_stop_reason;
+      f[11] = q.terminal_error_bits;
+      for (const TileId t : q.final_query.selected_tiles) {
+        if (tiles_written >= tile_cap) throw std::length_error{"tile buffer too small"};
+        out_tiles[tiles_written++] = t.value();
+      }
+    }
+    const BatchedExpansionMetrics& m = r.metrics;
+    const std::uint64_t mv[24] = {m.input_queries, m.initial_reached_queries, m.reached_queries,
+                                  m.unreachable_full_region_queries, m.expansion_limit_queries,
+                                  m.stalled_region_queries, m.identity_or_count_overflow_queries,
+                                  m.engine_failure_queries, m.planning_passes, m.batches_executed,
+                                  m.initial_batches_executed, m.retry_batches_executed, m.failed_lane_observations,
+                                  m.failed_origin_valid_lane_observations, m.retry_valid_lane_observations,
+                                  m.retry_lane_capacity, m.scheduled_expansions, m.full_region_fallbacks,
+                                  m.repeated_selected_edge_estimate, m.attempted_selected_vertex_count,
+                                  m.attempted_selected_edge_estimate, m.final_selected_tile_count,
+                                  m.final_selected_vertex_count, m.final_selected_edge_count};
+    std::memcpy(out_metrics, mv, sizeof(mv));
+    const std::size_t nh = std::min<std::size_t>(m.expansion_count_histogram.size(), 64U);
+    for (std::size_t i = 0; i < nh; ++i) out_hist[i] = m.expansion_count_histogram[i];
+    out_counts[0] = tiles_written;
+    out_counts[1] = m.expansion_count_histogram.size();
+    return static_cast<int>(r.queries.size());
+  });
 }
 
 }  // extern "C"
