@@ -176,6 +176,8 @@ def main():
     ap.add_argument("--impl", default="bfx", choices=["bfx", "reference"])
     ap.add_argument("--engine", default="auto", choices=["auto", "frontier", "jacobi", "dense"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"])
+    ap.add_argument("--frontier", default="groups", choices=["groups", "flat"],
+                    help="frontier-push work layout (sub-warp groups or flat work list)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=None)
     args = ap.parse_args()
@@ -237,6 +239,7 @@ def main():
     device = local if world > 1 else 0
     resident = bfx.ResidentDeviceGraph.upload_once(layout, device)
     ws = bfx.Workspace(resident)
+    ws.set_frontier_layout(bfx.FRONTIER_FLAT if args.frontier == "flat" else bfx.FRONTIER_GROUPS)
     engine_id = {"auto": bfx.ENGINE_AUTO, "frontier": bfx.ENGINE_FRONTIER_PUSH, "jacobi": bfx.ENGINE_JACOBI_PULL,
                  "dense": bfx.ENGINE_DENSE_CHAOTIC_PUSH}[args.engine]
     engines_chosen = None
@@ -361,6 +364,7 @@ def main():
         "config": {"workload": workload_desc,
                    "queries_per_gpu": len(queries), "batches": plan.batch_count,
                    "lane_widths": sorted({d.lane_width for d in descs}), "engine": args.engine,
+                   "frontier_layout": args.frontier,
                    "engines_chosen": None if engines_chosen is None else
                    {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
                    "control": "persistent_cooperative", "parallelism": f"replicas{world}",

@@ -34,6 +34,7 @@ P = C.POINTER
 ENGINE_JACOBI_PULL, ENGINE_DENSE_CHAOTIC_PUSH, ENGINE_FRONTIER_PUSH = 0, 1, 2
 ENGINE_AUTO = 0xFFFFFFFF
 CONTROL_PERSISTENT, CONTROL_CHUNKED, CONTROL_PER_ROUND = 0, 1, 2
+FRONTIER_GROUPS, FRONTIER_FLAT = 0, 1
 STOP_NONE, STOP_CONVERGED, STOP_MAXIMUM_ROUNDS, STOP_QUEUE_OVERFLOW, STOP_INVALID, STOP_FAILURE = range(6)
 INF_BITS = 0x7F800000
 NO_EDGE = 0xFFFFFFFF
@@ -546,6 +547,10 @@ class Workspace:
         """Near/far threshold steps per frontier batch (inf = plain frontier)."""
         arr = (f32 * len(deltas))(*deltas)
         _check(load().bfx_set_batch_deltas(self._h, u32(len(deltas)), arr))
+
+    def set_frontier_layout(self, layout: int):
+        """FRONTIER_GROUPS (sub-warp groups per entry) or FRONTIER_FLAT (flat work list)."""
+        _check(load().bfx_set_frontier_layout(self._h, u32(layout)))
 
     def set_batch_engines(self, engines: Sequence[int]):
         arr = (u32 * len(engines))(*engines)

@@ -350,7 +350,7 @@ __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
     if (engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH) {
       const DCtl& C = p.ctl[b];
       const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
-      if (n != 0u) return B.W <= 8u ? (n + 3u) >> 2 : n;  // warp items: 4 or 1 entries each
+      if (n != 0u) return p.flat ? (n + 31u) >> 5 : (B.W <= 8u ? (n + 3u) >> 2 : n);  // entries per warp item: 32, 4 or 1
       const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
       return (f + 31u) >> 5;  // split round: 32 far entries per warp item
     }
@@ -391,7 +391,9 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
       f = __shfl_sync(0xFFFFFFFFu, f, 0);
       tau_next = __shfl_sync(0xFFFFFFFFu, tau_next, 0);
       if (n != 0u) {
-        if (B.W <= 8u) {
+        if (p.flat) {
+          frontier_flat<kCount>(p, B, C, item, n, r & 1u, widx, tau, g % 3u, wk);
+        } else if (B.W <= 8u) {
           frontier_group<kCount, 8>(p, B, C, item, n, r & 1u, widx, tau, g % 3u, wk);
         } else {
           frontier_group<kCount, 32>(p, B, C, item, n, r & 1u, widx, tau, g % 3u, wk);
@@ -1114,6 +1116,7 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   p.budget_ns = kLaunchBudgetNs;
   p.engines = nullptr;
   p.deltas = nullptr;
+  p.flat = ws->frontier_layout == BFX_FRONTIER_FLAT ? 1u : 0u;
   if (!ws->batch_deltas.empty()) {
     require(ws->batch_deltas.size() == ws->nb, "per-batch deltas do not match the prepared batches");
     ws->deltas_dev.reserve(ws->nb * 4, ws->graph->device);
@@ -1232,6 +1235,14 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
 }  // namespace bfx
 
 extern "C" {
+
+int bfx_set_frontier_layout(bfx_workspace* ws, uint32_t layout) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null argument");
+    bfx::require(layout == BFX_FRONTIER_GROUPS || layout == BFX_FRONTIER_FLAT, "invalid frontier layout");
+    ws->frontier_layout = layout;
+  });
+}
 
 int bfx_execute(bfx_workspace* ws, const bfx_gpu_run_options* options) {
   return bfx::guarded([&] {

@@ -122,7 +122,7 @@ struct LaunchParams {
   u32 nb;
   u32 engine;            // engine of every batch when `engines` is null
   u32 per_lane;
-  u32 reserved;
+  u32 flat;              // frontier layout: 0 sub-warp groups, 1 flat work list
   u64 max_rounds;
   u64 budget_ns;         // wall-clock budget of one relaxation launch; past it the launch stops (device_failure)
   const u32* engines;    // [nb] per-batch engine (autotuned launches) or null
@@ -241,6 +241,7 @@ struct bfx_workspace {
   bfx::DeviceBuffer adjoint;     // per-edge exact accumulators, upstream values, result
   std::vector<std::uint32_t> batch_engines;  // per-batch engine for BFX_ENGINE_AUTO launches
   std::vector<float> batch_deltas;           // per-batch near/far steps (empty: plain frontier)
+  std::uint32_t frontier_layout = 0;         // BFX_FRONTIER_GROUPS / BFX_FRONTIER_FLAT
   bfx::DeviceBuffer deltas_dev;
   bfx::PinnedBuffer deltas_host;
   bfx::DeviceBuffer engines_dev;

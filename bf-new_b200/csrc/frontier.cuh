@@ -227,3 +227,132 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const DBatch&
     }
   }
 }
+
+// Warp-aggregated enqueue: the threads with `claim` set take consecutive
+// slots of `queue` from one atomicAdd on `*counter`; a slot beyond the batch
+// capacity raises queue_overflow.  Executed by all 32 threads.
+template <bool kCount>
+__device__ __forceinline__ void enqueue_claims(bool claim, u32 v, u32 cv, u32* counter, u64* queue, const DBatch& B,
+                                               DCtl& C, bool near, Work& wk) {
+  const u32 lane = lane_id();
+  const u32 cm = __ballot_sync(0xFFFFFFFFu, claim);
+  if (cm == 0u) return;  // warp-uniform
+  const u32 first = __ffs(cm) - 1u;
+  u32 pos = 0u;
+  if (lane == first) pos = atomicAdd(counter, static_cast<u32>(__popc(cm)));
+  pos = __shfl_sync(0xFFFFFFFFu, pos, static_cast<int>(first));
+  if (claim) {
+    if (kCount && near) wk.c[4] += 1;
+    const u32 at = pos + __popc(cm & ((1u << lane) - 1u));
+    if (at < B.U) {
+      queue[at] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
+    } else {
+      atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
+    }
+  }
+}
+
+// Flat frontier round body: one warp item covers up to 32 queue entries.
+// Every thread loads one entry's header (queue word, pending lanes, row
+// bounds) -- 32 independent header chains per warp -- and the entries'
+// (lane, out-edge) pairs are flattened into one work list, entry-major, then
+// lane, then edge, which the warp walks 32 items per step: thread t of step
+// s takes work item 32 s + t, finds its entry by a binary search over the
+// warp's inclusive work scan (five shuffles), and relaxes one lane over one
+// edge.  Every thread ORs its own success into the next round's pending
+// lanes; the OR that turns a word non-zero claims the queue slot, so no
+// per-edge combining is needed.  All loops are warp-uniform (trip counts
+// from shuffled warp totals).
+template <bool kCount>
+__device__ __forceinline__ void frontier_flat(const LaunchParams& p, const DBatch& B, DCtl& C, u32 item, u32 count,
+                                              u32 rd, u32 widx, u32 tau_bits, u32 pile, Work& wk) {
+  const u32 lane = lane_id();
+  const u32 entry = item * 32u + lane;
+  u32* const mask_r = B.mask[rd];
+  u32 v = 0u, cv = 0u, m = 0u, rb = 0u, deg = 0u;
+  if (entry < count) {
+    const u64 q = dev::ld_cg(B.queue[rd] + entry);
+    v = static_cast<u32>(q);
+    cv = static_cast<u32>(q >> 32);
+    if (v < p.g.V && cv < B.U) {
+      m = dev::ld_cg(mask_r + cv) & B.valid;
+      rb = __ldg(p.g.csr_off + v);
+      deg = __ldg(p.g.csr_off + v + 1u) - rb;
+      mask_r[cv] = 0u;
+    } else {
+      atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
+      v = cv = 0u;
+    }
+    if (kCount) {
+      wk.c[0] += 1;
+      wk.c[1] += deg;
+      wk.c[2] += __popc(m);
+    }
+  }
+  const u32 work = static_cast<u32>(__popc(m)) * deg;
+  u32 incl = work;
+  for (u32 o = 1; o < 32u; o <<= 1) {
+    const u32 y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const u32 excl = incl - work;
+  const u32 total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  u32* const mask_w = B.mask[rd ^ 1u];
+  u64* const queue_w = B.queue[rd ^ 1u];
+  for (u32 base = 0; base < total; base += 32u) {
+    const u32 w = base + lane;
+    // owner entry: the first lane whose inclusive work scan exceeds w
+    u32 e = 0u;
+    for (u32 s = 16u; s > 0u; s >>= 1) {
+      if (__shfl_sync(0xFFFFFFFFu, incl, static_cast<int>(e + s - 1u)) <= w) e += s;
+    }
+    const u32 ecv = __shfl_sync(0xFFFFFFFFu, cv, static_cast<int>(e));
+    const u32 em = __shfl_sync(0xFFFFFFFFu, m, static_cast<int>(e));
+    const u32 erb = __shfl_sync(0xFFFFFFFFu, rb, static_cast<int>(e));
+    const u32 edeg = __shfl_sync(0xFFFFFFFFu, deg, static_cast<int>(e));
+    const u32 eexcl = __shfl_sync(0xFFFFFFFFu, excl, static_cast<int>(e));
+    u32 bits = 0u, fbits = 0u, cdst = 0u, dstv = 0u, fd = 0xFFFFFFFFu;
+    if (w < total) {
+      const u32 r = w - eexcl;
+      const u32 j = r / edeg;  // lane ordinal within the entry
+      const u32 ed = erb + (r - j * edeg);
+      u32 mm = em;
+      for (u32 t = 0; t < j; ++t) mm &= mm - 1u;
+      const u32 ql = __ffs(mm) - 1u;
+      const u32 src_bits = dev::hi(dev::ld_cg(B.dist[0] + ((static_cast<u64>(ecv) << B.shift) + ql)));
+      const uint4 rec = __ldg(p.g.csr + ed);
+      const uint2 dt = B.tiles[rec.w];
+      cdst = rec.x - dt.y;
+      dstv = rec.x;
+      if (((dt.x >> ql) & 1u) && src_bits != dev::kInfBits) {
+        const u64 cand = dev::candidate(src_bits, rec.y, rec.z);
+        u64* const target = B.dist[0] + ((static_cast<u64>(cdst) << B.shift) + ql);
+        const u64 cur = dev::ld_cg(target);
+        if (kCount) wk.c[3] += 1;
+        if (cand < cur) {
+          dev::red_min(target, cand);
+          if (dev::hi(cand) < dev::hi(cur)) {
+            if (dev::hi(cand) < tau_bits) {
+              bits = 1u << ql;
+            } else {
+              fbits = 1u << ql;
+              fd = dev::hi(cand);
+            }
+          }
+          if (kCount) {
+            wk.c[6] += 1;
+            wk.c[5] += (bits | fbits) != 0u;
+          }
+        }
+      }
+    }
+    if (__any_sync(0xFFFFFFFFu, fbits != 0u)) {
+      fd = __reduce_min_sync(0xFFFFFFFFu, fd);
+      if (lane == 0u) atomicMin(&C.fmin[pile], fd);
+      const bool fclaim = fbits != 0u && atomicOr(B.fmask + cdst, fbits) == 0u;
+      enqueue_claims<kCount>(fclaim, dstv, cdst, &C.fcount[pile], B.fpile[pile], B, C, false, wk);
+    }
+    const bool claim = bits != 0u && atomicOr(mask_w + cdst, bits) == 0u;
+    enqueue_claims<kCount>(claim, dstv, cdst, &C.count[widx], queue_w, B, C, true, wk);
+  }
+}

@@ -280,3 +280,32 @@ def test_autotuner_with_near_far_candidates(gpu):
     check_batches(layout, descs, lanes, st, labels, Oracle.from_layout(layout))
     ws.close()
     res.close()
+
+
+@pytest.mark.parametrize("step", [None, 3.0])
+@pytest.mark.parametrize("control", [bfx.CONTROL_PERSISTENT, bfx.CONTROL_PER_ROUND], ids=["persistent", "per_round"])
+def test_flat_frontier_layout_bit_exact(gpu, c1, step, control):
+    """The flat work-list frontier (32 entries per warp, (lane, edge) pairs
+    walked 32 per step) gives the oracle's labels on full-graph W=8, regional
+    multi-batch W in {1, 8, 16, 32}, plain and near/far."""
+    layout = c1.layout
+    d = bfx.make_description(layout, c1.queries, 8)
+    layout2, grid = workloads.build_graph("c2", scale_tiles=(32, 32))
+    qs = workloads.box_queries(layout2, grid, 60, 2, 16, seed=31, targets=(1, 4))
+    plan = bfx.make_overlapping_batch_plan(layout2, qs, bfx.BatchPlannerPolicy(32, 0, 1, 8, 1, narrow_lanes=True))
+    for lay, descs, lanes in ((layout, [d], [c1.queries]),
+                              (layout2, plan.descriptions(),
+                               [[qs[i] if i != bfx.NO_EDGE else None for i in x.query_index_by_lane]
+                                for x in plan.descriptions()])):
+        res = bfx.ResidentDeviceGraph.upload_once(lay)
+        ws = bfx.Workspace(res)
+        ws.set_frontier_layout(bfx.FRONTIER_FLAT)
+        ws.prepare(descs)
+        if step is not None:
+            ws.set_batch_deltas([step] * len(descs))
+        ws.execute(bfx.GpuRunOptions(instrumentation=1, control_mode=control, maximum_rounds=1 << 20))
+        st = ws.fetch_statuses()
+        labels = [ws.download_labels(b, x.lane_width) for b, x in enumerate(descs)]
+        check_batches(lay, descs, lanes, st, labels, Oracle.from_layout(lay))
+        ws.close()
+        res.close()
