@@ -295,6 +295,7 @@ def main():
         execute_ms.append(x)
     launches_per_step = ws.last_launch_count()
     dev_ms = max_over_ranks(dev_ms)
+    log(f"[bench] device-resident: {dev_ms / args.steps:.3f} ms/step, relaxation kernel {np.mean(kernel_ms):.3f} ms")
     statuses = ws.fetch_statuses()
     assert all(s.stop_reason == bfx.STOP_CONVERGED for s in statuses)
     if dist:  # the job's one exchange: every rank's status records to every rank
@@ -317,6 +318,7 @@ def main():
     e2.record(stream)
     barrier()
     e2e_ms = max_over_ranks(s2.elapsed_time(e2))
+    log(f"[bench] end-to-end: {e2e_ms / args.steps:.3f} ms/step")
     h2d, d2h = ws.transfer_bytes()
 
     # ---- plain per-query engine (one query per launch sequence) on a sample

@@ -1411,6 +1411,22 @@ int bfx_run_query(bfx_workspace* ws, uint32_t source_count, const uint32_t* sour
     d.tile_lane_masks = masks.data();
     d.range_count = selected_tile_count;
     d.selected_vertex_ranges = ranges.data();
+    // The plain per-query engine runs the options' engine as given: per-batch
+    // engines and near/far steps of the workspace's batch set do not apply
+    // (they are kept for that set).
+    struct Keep {
+      bfx_workspace* ws;
+      std::vector<std::uint32_t> engines;
+      std::vector<float> deltas;
+      explicit Keep(bfx_workspace* w) : ws(w) {
+        engines.swap(w->batch_engines);
+        deltas.swap(w->batch_deltas);
+      }
+      ~Keep() {
+        ws->batch_engines.swap(engines);
+        ws->batch_deltas.swap(deltas);
+      }
+    } keep(ws);
     int rc = bfx_run_batches(ws, 1, &d, options, status);
     if (rc != BFX_OK) throw bfx::Error(rc, bfx_last_error());
   });

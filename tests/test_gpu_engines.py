@@ -309,3 +309,27 @@ def test_flat_frontier_layout_bit_exact(gpu, c1, step, control):
         check_batches(lay, descs, lanes, st, labels, Oracle.from_layout(lay))
         ws.close()
         res.close()
+
+
+def test_plain_query_after_autotune_ignores_batch_settings(gpu):
+    """run_query (one width-1 batch) runs the options' engine even when the
+    workspace holds autotuned per-batch engines and steps for a batch set."""
+    layout, grid = workloads.build_graph("c2", scale_tiles=(32, 32))
+    qs = workloads.box_queries(layout, grid, 12, 4, 12, seed=37)
+    plan = bfx.make_overlapping_batch_plan(layout, qs, bfx.BatchPlannerPolicy(32, 0, 1, 8, 1, narrow_lanes=True))
+    descs = plan.descriptions()
+    res = bfx.ResidentDeviceGraph.upload_once(layout)
+    ws = bfx.Workspace(res)
+    ws.autotune(descs)
+    orc = Oracle.from_layout(layout)
+    for q in qs[:3]:
+        st = ws.run_query(q.sources, q.targets, q.selected_tiles, bfx.GpuRunOptions(engine=bfx.ENGINE_FRONTIER_PUSH))
+        assert st.stop_reason == bfx.STOP_CONVERGED
+        d, _ = orc.region_sssp(q.sources, q.targets, q.selected_tiles)
+        assert bool(st.reached_target_mask & 1) == bool(np.all(d[q.targets] != bfx.INF_BITS))
+    # the tuned set is still usable after re-preparing it
+    ws.prepare(descs)
+    ws.execute(bfx.GpuRunOptions(engine=bfx.ENGINE_AUTO))
+    assert all(s.stop_reason == bfx.STOP_CONVERGED for s in ws.fetch_statuses())
+    ws.close()
+    res.close()
