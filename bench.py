@@ -178,6 +178,8 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"])
     ap.add_argument("--frontier", default="groups", choices=["groups", "flat"],
                     help="frontier-push work layout (sub-warp groups or flat work list)")
+    ap.add_argument("--regs", type=int, default=40, choices=[40, 64],
+                    help="register budget of the persistent kernel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=None)
     args = ap.parse_args()
@@ -240,6 +242,7 @@ def main():
     resident = bfx.ResidentDeviceGraph.upload_once(layout, device)
     ws = bfx.Workspace(resident)
     ws.set_frontier_layout(bfx.FRONTIER_FLAT if args.frontier == "flat" else bfx.FRONTIER_GROUPS)
+    ws.set_register_budget(args.regs)
     engine_id = {"auto": bfx.ENGINE_AUTO, "frontier": bfx.ENGINE_FRONTIER_PUSH, "jacobi": bfx.ENGINE_JACOBI_PULL,
                  "dense": bfx.ENGINE_DENSE_CHAOTIC_PUSH}[args.engine]
     engines_chosen = None
@@ -280,8 +283,12 @@ def main():
         start = torch.cuda.Event(enable_timing=True)
         end = torch.cuda.Event(enable_timing=True)
         start.record(stream)
+        # NVTX range: lets a profiler select the timed launches
+        # (ncu --nvtx --nvtx-include "bench_timed/")
+        torch.cuda.nvtx.range_push("bench_timed")
         for _ in range(args.steps):
             ws.execute(opts)
+        torch.cuda.nvtx.range_pop()
         end.record(stream)
         barrier()
     dev_ms = start.elapsed_time(end)
@@ -366,7 +373,7 @@ def main():
         "config": {"workload": workload_desc,
                    "queries_per_gpu": len(queries), "batches": plan.batch_count,
                    "lane_widths": sorted({d.lane_width for d in descs}), "engine": args.engine,
-                   "frontier_layout": args.frontier,
+                   "frontier_layout": args.frontier, "registers": args.regs,
                    "engines_chosen": None if engines_chosen is None else
                    {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
                    "control": "persistent_cooperative", "parallelism": f"replicas{world}",

@@ -548,6 +548,10 @@ class Workspace:
         arr = (f32 * len(deltas))(*deltas)
         _check(load().bfx_set_batch_deltas(self._h, u32(len(deltas)), arr))
 
+    def set_register_budget(self, registers: int):
+        """40 (three 512-thread blocks per SM) or 64 registers per thread for the persistent kernel."""
+        _check(load().bfx_set_register_budget(self._h, u32(registers)))
+
     def set_frontier_layout(self, layout: int):
         """FRONTIER_GROUPS (sub-warp groups per entry) or FRONTIER_FLAT (flat work list)."""
         _check(load().bfx_set_frontier_layout(self._h, u32(layout)))

@@ -390,16 +390,17 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
       tau = __shfl_sync(0xFFFFFFFFu, tau, 0);
       f = __shfl_sync(0xFFFFFFFFu, f, 0);
       tau_next = __shfl_sync(0xFFFFFFFFu, tau_next, 0);
+      const FrontierView V = frontier_view(B, r & 1u, g % 3u, (g + 1u) % 3u);
       if (n != 0u) {
         if (p.flat) {
-          frontier_flat<kCount>(p, B, C, item, n, r & 1u, widx, tau, g % 3u, wk);
+          frontier_flat<kCount>(p, V, C, item, n, r & 1u, widx, tau, g % 3u, wk);
         } else if (B.W <= 8u) {
-          frontier_group<kCount, 8>(p, B, C, item, n, r & 1u, widx, tau, g % 3u, wk);
+          frontier_group<kCount, 8>(p, V, C, item, n, r & 1u, widx, tau, g % 3u, wk);
         } else {
-          frontier_group<kCount, 32>(p, B, C, item, n, r & 1u, widx, tau, g % 3u, wk);
+          frontier_group<kCount, 32>(p, V, C, item, n, r & 1u, widx, tau, g % 3u, wk);
         }
       } else {
-        split_group<kCount>(p, B, C, item, f, r & 1u, widx, tau_next, g % 3u, (g + 1u) % 3u, wk);
+        split_group<kCount>(p, V, C, item, f, r & 1u, widx, tau_next, g % 3u, (g + 1u) % 3u, wk);
       }
     } else if (eng == BFX_ENGINE_JACOBI_PULL) {
       jacobi_item<kCount>(p, B, C, item, r, widx, wk);
@@ -451,8 +452,11 @@ __device__ void flush_work(const LaunchParams& p, Work& wk) {
   }
 }
 
-template <bool kCount>
-__global__ void __launch_bounds__(512, 3) persistent_kernel(LaunchParams p) {
+// kMinBlocks = resident 512-thread blocks per SM the register budget is set
+// for: 3 -> 40 registers per thread (48 warps per SM), 2 -> 64 registers
+// (32 warps per SM, no spills).
+template <bool kCount, int kMinBlocks>
+__global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParams p) {
   extern __shared__ u32 prefix[];
   const u32 nblocks = gridDim.x;
   Work wk;
@@ -1156,8 +1160,12 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   BFX_CUDA(cudaGetLastError());
   BFX_CUDA(cudaEventRecord(ws->ev[1], ws->stream));
   if (o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
-    const void* kfn = o.instrumentation ? reinterpret_cast<const void*>(persistent_kernel<true>)
-                                        : reinterpret_cast<const void*>(persistent_kernel<false>);
+    const bool wide = ws->register_budget == 64u;
+    const void* kfn = o.instrumentation
+                          ? (wide ? reinterpret_cast<const void*>(persistent_kernel<true, 2>)
+                                  : reinterpret_cast<const void*>(persistent_kernel<true, 3>))
+                          : (wide ? reinterpret_cast<const void*>(persistent_kernel<false, 2>)
+                                  : reinterpret_cast<const void*>(persistent_kernel<false, 3>));
     const int grid = grid_blocks(ws, kfn, block, smem, o);
     void* args[] = {&p};
     BFX_CUDA(cudaLaunchCooperativeKernel(kfn, grid, block, args, smem, ws->stream));
@@ -1235,6 +1243,14 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
 }  // namespace bfx
 
 extern "C" {
+
+int bfx_set_register_budget(bfx_workspace* ws, uint32_t registers) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null argument");
+    bfx::require(registers == 40u || registers == 64u, "register budget must be 40 or 64");
+    ws->register_budget = registers;
+  });
+}
 
 int bfx_set_frontier_layout(bfx_workspace* ws, uint32_t layout) {
   return bfx::guarded([&] {
@@ -1658,7 +1674,7 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
     const size_t smem = 8;
     int per_sm = 0;
     BFX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, reinterpret_cast<const void*>(bfx::persistent_kernel<false>), block, smem));
+        &per_sm, reinterpret_cast<const void*>(bfx::persistent_kernel<false, 3>), block, smem));
     if (per_sm <= 0) throw bfx::Error(BFX_ERR_CUDA, "kernel cannot be resident with this block size");
     if (options->grid_policy == 1u) {
       if (static_cast<int>(options->blocks_per_wgp) > per_sm)
@@ -1666,7 +1682,7 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
       per_sm = static_cast<int>(options->blocks_per_wgp);
     }
     void* args[] = {&p};
-    BFX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(bfx::persistent_kernel<false>),
+    BFX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(bfx::persistent_kernel<false, 3>),
                                          per_sm * sms, block, args, smem, 0));
     auto* d_status = reinterpret_cast<bfx_device_run_status*>(base + o_status);
     bfx::finalize_kernel<<<1, 256>>>(p, reinterpret_cast<bfx_device_controller*>(base + o_ctrl), d_status);

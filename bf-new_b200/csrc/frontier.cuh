@@ -18,8 +18,42 @@
 // queue slots with one atomicAdd.
 #pragma once
 
+// Registers-only view of one batch for one round of the frontier engine:
+// the per-round slots (read / write pending masks and queues, the far pile
+// of this generation) are selected once per warp item, so the round body
+// never re-reads the batch record from global memory after its atomics.
+struct FrontierView {
+  u64* dist;
+  u32* mask_r;
+  u32* mask_w;
+  u64* queue_r;
+  u64* queue_w;
+  const uint2* tiles;
+  u32* fmask;
+  u64* pile;      // near round: far pile being filled; split round: pile read
+  u64* pile_out;  // split round: pile written
+  u32 shift, valid, U;
+};
+
+__device__ __forceinline__ FrontierView frontier_view(const DBatch& b, u32 rd, u32 pile, u32 pile_out) {
+  FrontierView v;
+  v.dist = b.dist[0];
+  v.mask_r = b.mask[rd];
+  v.mask_w = b.mask[rd ^ 1u];
+  v.queue_r = b.queue[rd];
+  v.queue_w = b.queue[rd ^ 1u];
+  v.tiles = b.tiles;
+  v.fmask = b.fmask;
+  v.pile = b.fpile[pile];
+  v.pile_out = b.fpile[pile_out];
+  v.shift = b.shift;
+  v.valid = b.valid;
+  v.U = b.U;
+  return v;
+}
+
 template <bool kCount, u32 S>
-__device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBatch& B, DCtl& C, u32 item, u32 count,
+__device__ __forceinline__ void frontier_group(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
                                                u32 rd, u32 widx, u32 tau_bits, u32 pile, Work& wk) {
   constexpr u32 EPW = 32u / S;
   const u32 lane = lane_id();
@@ -27,10 +61,10 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
   const u32 leader = lane & ~(S - 1u);
   const u32 entry = item * EPW + (lane / S);
   const bool live = entry < count;
-  u32* const mask_r = B.mask[rd];
+  u32* const mask_r = B.mask_r;
   u32 v = 0u, cv = 0u, m = 0u, rb = 0u, re = 0u;
   if (live && sl == 0u) {
-    const u64 q = dev::ld_cg(B.queue[rd] + entry);
+    const u64 q = dev::ld_cg(B.queue_r + entry);
     v = static_cast<u32>(q);
     cv = static_cast<u32>(q >> 32);
     if (v < p.g.V && cv < B.U) {
@@ -66,7 +100,7 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
     u32 mm = m;
     for (u32 t = 0; t < j; ++t) mm &= mm - 1u;  // drop the j lowest active lanes
     ql = __ffs(mm) - 1u;
-    src_bits = dev::hi(dev::ld_cg(B.dist[0] + ((static_cast<u64>(cv) << B.shift) + ql)));
+    src_bits = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(cv) << B.shift) + ql)));
   }
   const u32 steps_mine = live ? (re - rb + G - 1u) / G : 0u;
   const u32 steps = __reduce_max_sync(0xFFFFFFFFu, steps_mine);
@@ -75,8 +109,8 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
   // executed by all 32 threads) and each thread keeps only the partners
   // inside its own sub-group.
   const u32 kp_warp = __reduce_max_sync(0xFFFFFFFFu, kp);
-  u32* const mask_w = B.mask[rd ^ 1u];
-  u64* const queue_w = B.queue[rd ^ 1u];
+  u32* const mask_w = B.mask_w;
+  u64* const queue_w = B.queue_w;
   for (u32 st = 0; st < steps; ++st) {
     const u32 e = rb + st * G + slot;
     u32 bits = 0u, fbits = 0u, cdst = 0u, dstv = 0u, fd = 0xFFFFFFFFu;
@@ -87,7 +121,7 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
       dstv = rec.x;
       if (((dt.x >> ql) & 1u) && src_bits != dev::kInfBits) {
         const u64 cand = dev::candidate(src_bits, rec.y, rec.z);
-        u64* const target = B.dist[0] + ((static_cast<u64>(cdst) << B.shift) + ql);
+        u64* const target = B.dist + ((static_cast<u64>(cdst) << B.shift) + ql);
         const u64 cur = dev::ld_cg(target);
         if (kCount) wk.c[3] += 1;
         if (cand < cur) {
@@ -131,7 +165,7 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
         if (fclaim) {
           const u32 at = pos + __popc(fm & ((1u << lane) - 1u));
           if (at < B.U) {
-            B.fpile[pile][at] = static_cast<u64>(dstv) | (static_cast<u64>(cdst) << 32);
+            B.pile[at] = static_cast<u64>(dstv) | (static_cast<u64>(cdst) << 32);
           } else {
             atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
           }
@@ -167,13 +201,13 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const DBat
 // runs no near round in the same round, so the far masks it reads are
 // stable and are cleared with plain stores.
 template <bool kCount>
-__device__ __forceinline__ void split_group(const LaunchParams& p, const DBatch& B, DCtl& C, u32 item, u32 count,
+__device__ __forceinline__ void split_group(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
                                             u32 rd, u32 widx, u32 tau_next, u32 pile_in, u32 pile_out, Work& wk) {
   const u32 lane = lane_id();
   const u32 entry = item * 32u + lane;
   u32 near = 0u, far = 0u, v = 0u, cv = 0u, fd = 0xFFFFFFFFu;
   if (entry < count) {
-    const u64 q = dev::ld_cg(B.fpile[pile_in] + entry);
+    const u64 q = dev::ld_cg(B.pile + entry);
     v = static_cast<u32>(q);
     cv = static_cast<u32>(q >> 32);
     u32 bits = 0u;
@@ -185,7 +219,7 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const DBatch&
     }
     for (u32 m = bits; m != 0u; m &= m - 1u) {
       const u32 l = __ffs(m) - 1u;
-      const u32 d = dev::hi(dev::ld_cg(B.dist[0] + ((static_cast<u64>(cv) << B.shift) + l)));
+      const u32 d = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(cv) << B.shift) + l)));
       if (d < tau_next) {
         near |= 1u << l;
       } else {
@@ -198,7 +232,7 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const DBatch&
   // far lanes stay parked (next pile); near lanes join the next round
   bool fclaim = false, claim = false;
   if (far != 0u) fclaim = atomicOr(B.fmask + cv, far) == 0u;
-  if (near != 0u) claim = atomicOr(B.mask[rd ^ 1u] + cv, near) == 0u;
+  if (near != 0u) claim = atomicOr(B.mask_w + cv, near) == 0u;
   fd = __reduce_min_sync(0xFFFFFFFFu, fd);
   if (lane == 0u && fd != 0xFFFFFFFFu) atomicMin(&C.fmin[pile_out], fd);
   const u32 fm = __ballot_sync(0xFFFFFFFFu, fclaim);
@@ -209,7 +243,7 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const DBatch&
     pos = __shfl_sync(0xFFFFFFFFu, pos, static_cast<int>(first));
     if (fclaim) {
       const u32 at = pos + __popc(fm & ((1u << lane) - 1u));
-      if (at < B.U) B.fpile[pile_out][at] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
+      if (at < B.U) B.pile_out[at] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
       else atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
     }
   }
@@ -222,7 +256,7 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const DBatch&
     if (claim) {
       if (kCount) wk.c[4] += 1;
       const u32 at = pos + __popc(cm & ((1u << lane) - 1u));
-      if (at < B.U) B.queue[rd ^ 1u][at] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
+      if (at < B.U) B.queue_w[at] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
       else atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
     }
   }
@@ -232,7 +266,7 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const DBatch&
 // slots of `queue` from one atomicAdd on `*counter`; a slot beyond the batch
 // capacity raises queue_overflow.  Executed by all 32 threads.
 template <bool kCount>
-__device__ __forceinline__ void enqueue_claims(bool claim, u32 v, u32 cv, u32* counter, u64* queue, const DBatch& B,
+__device__ __forceinline__ void enqueue_claims(bool claim, u32 v, u32 cv, u32* counter, u64* queue, const FrontierView& B,
                                                DCtl& C, bool near, Work& wk) {
   const u32 lane = lane_id();
   const u32 cm = __ballot_sync(0xFFFFFFFFu, claim);
@@ -264,14 +298,14 @@ __device__ __forceinline__ void enqueue_claims(bool claim, u32 v, u32 cv, u32* c
 // per-edge combining is needed.  All loops are warp-uniform (trip counts
 // from shuffled warp totals).
 template <bool kCount>
-__device__ __forceinline__ void frontier_flat(const LaunchParams& p, const DBatch& B, DCtl& C, u32 item, u32 count,
+__device__ __forceinline__ void frontier_flat(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
                                               u32 rd, u32 widx, u32 tau_bits, u32 pile, Work& wk) {
   const u32 lane = lane_id();
   const u32 entry = item * 32u + lane;
-  u32* const mask_r = B.mask[rd];
+  u32* const mask_r = B.mask_r;
   u32 v = 0u, cv = 0u, m = 0u, rb = 0u, deg = 0u;
   if (entry < count) {
-    const u64 q = dev::ld_cg(B.queue[rd] + entry);
+    const u64 q = dev::ld_cg(B.queue_r + entry);
     v = static_cast<u32>(q);
     cv = static_cast<u32>(q >> 32);
     if (v < p.g.V && cv < B.U) {
@@ -297,8 +331,8 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const DBatc
   }
   const u32 excl = incl - work;
   const u32 total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-  u32* const mask_w = B.mask[rd ^ 1u];
-  u64* const queue_w = B.queue[rd ^ 1u];
+  u32* const mask_w = B.mask_w;
+  u64* const queue_w = B.queue_w;
   for (u32 base = 0; base < total; base += 32u) {
     const u32 w = base + lane;
     // owner entry: the first lane whose inclusive work scan exceeds w
@@ -319,14 +353,14 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const DBatc
       u32 mm = em;
       for (u32 t = 0; t < j; ++t) mm &= mm - 1u;
       const u32 ql = __ffs(mm) - 1u;
-      const u32 src_bits = dev::hi(dev::ld_cg(B.dist[0] + ((static_cast<u64>(ecv) << B.shift) + ql)));
+      const u32 src_bits = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(ecv) << B.shift) + ql)));
       const uint4 rec = __ldg(p.g.csr + ed);
       const uint2 dt = B.tiles[rec.w];
       cdst = rec.x - dt.y;
       dstv = rec.x;
       if (((dt.x >> ql) & 1u) && src_bits != dev::kInfBits) {
         const u64 cand = dev::candidate(src_bits, rec.y, rec.z);
-        u64* const target = B.dist[0] + ((static_cast<u64>(cdst) << B.shift) + ql);
+        u64* const target = B.dist + ((static_cast<u64>(cdst) << B.shift) + ql);
         const u64 cur = dev::ld_cg(target);
         if (kCount) wk.c[3] += 1;
         if (cand < cur) {
@@ -350,7 +384,7 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const DBatc
       fd = __reduce_min_sync(0xFFFFFFFFu, fd);
       if (lane == 0u) atomicMin(&C.fmin[pile], fd);
       const bool fclaim = fbits != 0u && atomicOr(B.fmask + cdst, fbits) == 0u;
-      enqueue_claims<kCount>(fclaim, dstv, cdst, &C.fcount[pile], B.fpile[pile], B, C, false, wk);
+      enqueue_claims<kCount>(fclaim, dstv, cdst, &C.fcount[pile], B.pile, B, C, false, wk);
     }
     const bool claim = bits != 0u && atomicOr(mask_w + cdst, bits) == 0u;
     enqueue_claims<kCount>(claim, dstv, cdst, &C.count[widx], queue_w, B, C, true, wk);

@@ -298,6 +298,10 @@ int bfx_set_batch_deltas(bfx_workspace *ws, uint32_t count, const float *deltas)
  * list, 32 per step. */
 enum { BFX_FRONTIER_GROUPS = 0, BFX_FRONTIER_FLAT = 1 };
 int bfx_set_frontier_layout(bfx_workspace *ws, uint32_t layout);
+/* Register budget of the persistent relaxation kernel (a bfx tuning option,
+ * results unchanged): 40 registers per thread (three 512-thread blocks per
+ * SM, the default) or 64 (two blocks per SM, fewer spills). */
+int bfx_set_register_budget(bfx_workspace *ws, uint32_t registers);
 /* {mean edge weight, edge count} of the workspace's resident graph. */
 int bfx_workspace_graph_stats(bfx_workspace *ws, double out[2]);
 
