@@ -290,29 +290,93 @@ __device__ __forceinline__ void enqueue_claims(bool claim, u32 v, u32 cv, u32* c
 // Every thread loads one entry's header (queue word, pending lanes, row
 // bounds) -- 32 independent header chains per warp -- and the entries'
 // (lane, out-edge) pairs are flattened into one work list, entry-major, then
-// lane, then edge, which the warp walks 32 items per step: thread t of step
-// s takes work item 32 s + t, finds its entry by a binary search over the
-// warp's inclusive work scan (five shuffles), and relaxes one lane over one
-// edge.  Every thread ORs its own success into the next round's pending
-// lanes; the OR that turns a word non-zero claims the queue slot, so no
-// per-edge combining is needed.  All loops are warp-uniform (trip counts
-// from shuffled warp totals).
+// lane, then edge.  The warp walks the list 64 items per iteration, two per
+// thread, with the memory accesses of the two items interleaved phase by
+// phase (record and source label, tile entry, target label, pending-word OR)
+// so each thread keeps two dependent chains in flight.  A thread finds the
+// entry of a work item by a binary search over the warp's inclusive work scan
+// (five shuffles).  Every thread ORs its own success into the next round's
+// pending word; the OR that turns the word non-zero claims the vertex, and
+// claimed vertices are staged in the warp's shared-memory buffer and written
+// to the next queue with one counter atomic per 32 or more claims, off the
+// per-step chain.  All loops are warp-uniform.
+constexpr u32 kStage = 64;  // staged claims per warp: < 32 before a call adds <= 32
+
+struct FlatItem {
+  bool live;
+  u32 ql, ed, cv;
+};
+
+__device__ __forceinline__ FlatItem flat_decode(u32 w, u32 total, u32 incl, u32 excl, u32 cv, u32 m, u32 rb,
+                                                u32 deg) {
+  u32 e = 0u;
+  for (u32 s = 16u; s > 0u; s >>= 1) {
+    if (__shfl_sync(0xFFFFFFFFu, incl, static_cast<int>(e + s - 1u)) <= w) e += s;
+  }
+  const u32 ecv = __shfl_sync(0xFFFFFFFFu, cv, static_cast<int>(e));
+  const u32 em = __shfl_sync(0xFFFFFFFFu, m, static_cast<int>(e));
+  const u32 erb = __shfl_sync(0xFFFFFFFFu, rb, static_cast<int>(e));
+  const u32 edeg = __shfl_sync(0xFFFFFFFFu, deg, static_cast<int>(e));
+  const u32 eexcl = __shfl_sync(0xFFFFFFFFu, excl, static_cast<int>(e));
+  FlatItem it{w < total, 0u, 0u, ecv};
+  if (it.live) {
+    const u32 r = w - eexcl;
+    const u32 j = r / edeg;  // lane ordinal within the entry
+    it.ed = erb + (r - j * edeg);
+    u32 mm = em;
+    for (u32 t = 0; t < j; ++t) mm &= mm - 1u;
+    it.ql = __ffs(mm) - 1u;
+  }
+  return it;
+}
+
+// Appends the claiming threads' vertices to the warp's stage; flushes the
+// stage to `queue` (one atomicAdd on `counter`) once it holds >= 32 entries,
+// or whenever `final` is set.  Executed by all 32 threads.
+template <bool kCount>
+__device__ __forceinline__ void stage_claims(bool claim, u32 v, u32 cv, u64* stage, u32& n, bool final, u32* counter,
+                                             u64* queue, const FrontierView& B, DCtl& C, Work& wk) {
+  const u32 lane = lane_id();
+  const u32 cm = __ballot_sync(0xFFFFFFFFu, claim);
+  if (claim) {
+    stage[n + __popc(cm & ((1u << lane) - 1u))] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
+    if (kCount) wk.c[4] += 1;
+  }
+  n += static_cast<u32>(__popc(cm));
+  if (n == 0u || (n < 32u && !final)) return;  // warp-uniform
+  __syncwarp();
+  u32 pos = 0u;
+  if (lane == 0u) pos = atomicAdd(counter, n);
+  pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
+  for (u32 i = lane; i < n; i += 32u) {
+    if (pos + i < B.U) {
+      queue[pos + i] = stage[i];
+    } else {
+      atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
+    }
+  }
+  __syncwarp();
+  n = 0u;
+}
+
 template <bool kCount>
 __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
                                               u32 rd, u32 widx, u32 tau_bits, u32 pile, Work& wk) {
+  __shared__ u64 s_stage[16][kStage];  // blocks of up to 512 threads
+  u64* const stage = s_stage[threadIdx.x >> 5];
+  u32 staged = 0u;
   const u32 lane = lane_id();
   const u32 entry = item * 32u + lane;
-  u32* const mask_r = B.mask_r;
   u32 v = 0u, cv = 0u, m = 0u, rb = 0u, deg = 0u;
   if (entry < count) {
     const u64 q = dev::ld_cg(B.queue_r + entry);
     v = static_cast<u32>(q);
     cv = static_cast<u32>(q >> 32);
     if (v < p.g.V && cv < B.U) {
-      m = dev::ld_cg(mask_r + cv) & B.valid;
+      m = dev::ld_cg(B.mask_r + cv) & B.valid;
       rb = __ldg(p.g.csr_off + v);
       deg = __ldg(p.g.csr_off + v + 1u) - rb;
-      mask_r[cv] = 0u;
+      B.mask_r[cv] = 0u;
     } else {
       atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
       v = cv = 0u;
@@ -331,62 +395,82 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
   }
   const u32 excl = incl - work;
   const u32 total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-  u32* const mask_w = B.mask_w;
-  u64* const queue_w = B.queue_w;
-  for (u32 base = 0; base < total; base += 32u) {
-    const u32 w = base + lane;
-    // owner entry: the first lane whose inclusive work scan exceeds w
-    u32 e = 0u;
-    for (u32 s = 16u; s > 0u; s >>= 1) {
-      if (__shfl_sync(0xFFFFFFFFu, incl, static_cast<int>(e + s - 1u)) <= w) e += s;
+  for (u32 base = 0; base < total; base += 64u) {
+    FlatItem it[2];
+    u32 src[2], bits[2], fbits[2], cdst[2], dstv[2];
+    uint4 rec[2];
+    uint2 dt[2];
+    u32 fd = 0xFFFFFFFFu;
+#pragma unroll
+    for (u32 u = 0; u < 2u; ++u) {
+      it[u] = flat_decode(base + 32u * u + lane, total, incl, excl, cv, m, rb, deg);
+      bits[u] = fbits[u] = cdst[u] = dstv[u] = 0u;
+      src[u] = dev::kInfBits;
     }
-    const u32 ecv = __shfl_sync(0xFFFFFFFFu, cv, static_cast<int>(e));
-    const u32 em = __shfl_sync(0xFFFFFFFFu, m, static_cast<int>(e));
-    const u32 erb = __shfl_sync(0xFFFFFFFFu, rb, static_cast<int>(e));
-    const u32 edeg = __shfl_sync(0xFFFFFFFFu, deg, static_cast<int>(e));
-    const u32 eexcl = __shfl_sync(0xFFFFFFFFu, excl, static_cast<int>(e));
-    u32 bits = 0u, fbits = 0u, cdst = 0u, dstv = 0u, fd = 0xFFFFFFFFu;
-    if (w < total) {
-      const u32 r = w - eexcl;
-      const u32 j = r / edeg;  // lane ordinal within the entry
-      const u32 ed = erb + (r - j * edeg);
-      u32 mm = em;
-      for (u32 t = 0; t < j; ++t) mm &= mm - 1u;
-      const u32 ql = __ffs(mm) - 1u;
-      const u32 src_bits = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(ecv) << B.shift) + ql)));
-      const uint4 rec = __ldg(p.g.csr + ed);
-      const uint2 dt = B.tiles[rec.w];
-      cdst = rec.x - dt.y;
-      dstv = rec.x;
-      if (((dt.x >> ql) & 1u) && src_bits != dev::kInfBits) {
-        const u64 cand = dev::candidate(src_bits, rec.y, rec.z);
-        u64* const target = B.dist + ((static_cast<u64>(cdst) << B.shift) + ql);
-        const u64 cur = dev::ld_cg(target);
+#pragma unroll
+    for (u32 u = 0; u < 2u; ++u) {
+      if (it[u].live) {
+        src[u] = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(it[u].cv) << B.shift) + it[u].ql)));
+        rec[u] = __ldg(p.g.csr + it[u].ed);
+      }
+    }
+#pragma unroll
+    for (u32 u = 0; u < 2u; ++u) {
+      if (it[u].live) {
+        dt[u] = B.tiles[rec[u].w];
+        cdst[u] = rec[u].x - dt[u].y;
+        dstv[u] = rec[u].x;
+      }
+    }
+    u64 cur[2], cand[2];
+    bool relax[2];
+#pragma unroll
+    for (u32 u = 0; u < 2u; ++u) {
+      relax[u] = it[u].live && ((dt[u].x >> it[u].ql) & 1u) && src[u] != dev::kInfBits;
+      if (relax[u]) {
+        cand[u] = dev::candidate(src[u], rec[u].y, rec[u].z);
+        cur[u] = dev::ld_cg(B.dist + ((static_cast<u64>(cdst[u]) << B.shift) + it[u].ql));
+      }
+    }
+#pragma unroll
+    for (u32 u = 0; u < 2u; ++u) {
+      if (relax[u]) {
         if (kCount) wk.c[3] += 1;
-        if (cand < cur) {
-          dev::red_min(target, cand);
-          if (dev::hi(cand) < dev::hi(cur)) {
-            if (dev::hi(cand) < tau_bits) {
-              bits = 1u << ql;
+        if (cand[u] < cur[u]) {
+          dev::red_min(B.dist + ((static_cast<u64>(cdst[u]) << B.shift) + it[u].ql), cand[u]);
+          if (dev::hi(cand[u]) < dev::hi(cur[u])) {
+            if (dev::hi(cand[u]) < tau_bits) {
+              bits[u] = 1u << it[u].ql;
             } else {
-              fbits = 1u << ql;
-              fd = dev::hi(cand);
+              fbits[u] = 1u << it[u].ql;
+              fd = min(fd, dev::hi(cand[u]));
             }
           }
           if (kCount) {
             wk.c[6] += 1;
-            wk.c[5] += (bits | fbits) != 0u;
+            wk.c[5] += (bits[u] | fbits[u]) != 0u;
           }
         }
       }
     }
-    if (__any_sync(0xFFFFFFFFu, fbits != 0u)) {
+    if (__any_sync(0xFFFFFFFFu, (fbits[0] | fbits[1]) != 0u)) {
       fd = __reduce_min_sync(0xFFFFFFFFu, fd);
       if (lane == 0u) atomicMin(&C.fmin[pile], fd);
-      const bool fclaim = fbits != 0u && atomicOr(B.fmask + cdst, fbits) == 0u;
-      enqueue_claims<kCount>(fclaim, dstv, cdst, &C.fcount[pile], B.pile, B, C, false, wk);
+#pragma unroll
+      for (u32 u = 0; u < 2u; ++u) {
+        const bool fclaim = fbits[u] != 0u && atomicOr(B.fmask + cdst[u], fbits[u]) == 0u;
+        enqueue_claims<kCount>(fclaim, dstv[u], cdst[u], &C.fcount[pile], B.pile, B, C, false, wk);
+      }
     }
-    const bool claim = bits != 0u && atomicOr(mask_w + cdst, bits) == 0u;
-    enqueue_claims<kCount>(claim, dstv, cdst, &C.count[widx], queue_w, B, C, true, wk);
+    // both pending-word ORs are issued before either result is used
+    u32 old[2];
+#pragma unroll
+    for (u32 u = 0; u < 2u; ++u) old[u] = bits[u] != 0u ? atomicOr(B.mask_w + cdst[u], bits[u]) : 1u;
+#pragma unroll
+    for (u32 u = 0; u < 2u; ++u) {
+      stage_claims<kCount>(old[u] == 0u, dstv[u], cdst[u], stage, staged, false, &C.count[widx], B.queue_w, B, C,
+                           wk);
+    }
   }
+  stage_claims<kCount>(false, 0u, 0u, stage, staged, true, &C.count[widx], B.queue_w, B, C, wk);
 }
