@@ -241,8 +241,8 @@ struct bfx_workspace {
   bfx::DeviceBuffer adjoint;     // per-edge exact accumulators, upstream values, result
   std::vector<std::uint32_t> batch_engines;  // per-batch engine for BFX_ENGINE_AUTO launches
   std::vector<float> batch_deltas;           // per-batch near/far steps (empty: plain frontier)
-  std::uint32_t frontier_layout = 0;         // BFX_FRONTIER_GROUPS / BFX_FRONTIER_FLAT
-  std::uint32_t register_budget = 40;        // persistent kernel: 40 or 64 registers per thread
+  std::uint32_t frontier_layout = 1;         // BFX_FRONTIER_FLAT (default) / BFX_FRONTIER_GROUPS
+  std::uint32_t register_budget = 64;        // persistent kernel: 64 (default) or 40 registers per thread
   bfx::DeviceBuffer deltas_dev;
   bfx::PinnedBuffer deltas_host;
   bfx::DeviceBuffer engines_dev;

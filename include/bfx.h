@@ -292,15 +292,16 @@ int bfx_set_batch_engines(bfx_workspace *ws, uint32_t count, const uint32_t *eng
  * count at execute time. */
 int bfx_set_batch_deltas(bfx_workspace *ws, uint32_t count, const float *deltas);
 /* Frontier-push work layout (a bfx scheduling option, results unchanged):
- * BFX_FRONTIER_GROUPS (default) gives each queue entry a sub-warp group of 8
- * threads (batches of <= 8 lanes) or a whole warp; BFX_FRONTIER_FLAT gives a
- * warp 32 entries and walks their (lane, out-edge) pairs as one flat work
- * list, 32 per step. */
+ * BFX_FRONTIER_FLAT (default) gives a warp 32 entries and walks their
+ * (lane, out-edge) pairs as one flat work list, two items per thread per
+ * step; BFX_FRONTIER_GROUPS gives each queue entry a sub-warp group of 8
+ * threads (batches of <= 8 lanes) or a whole warp. */
 enum { BFX_FRONTIER_GROUPS = 0, BFX_FRONTIER_FLAT = 1 };
 int bfx_set_frontier_layout(bfx_workspace *ws, uint32_t layout);
 /* Register budget of the persistent relaxation kernel (a bfx tuning option,
  * results unchanged): 40 registers per thread (three 512-thread blocks per
- * SM, the default) or 64 (two blocks per SM, fewer spills). */
+ * SM) or 64 (two blocks per SM, the default: no spills in the group layout,
+ * few in the flat one). */
 int bfx_set_register_budget(bfx_workspace *ws, uint32_t registers);
 /* {mean edge weight, edge count} of the workspace's resident graph. */
 int bfx_workspace_graph_stats(bfx_workspace *ws, double out[2]);
