@@ -272,6 +272,7 @@ def main():
     ws.execute(opts_instr)
     statuses = ws.fetch_statuses()
     work = ws.work_counters()
+    engine_work = ws.engine_work()
     assert all(s.stop_reason == bfx.STOP_CONVERGED for s in statuses), "benchmark run did not converge"
     reached = sum(bin(s.reached_target_mask).count("1") for s in statuses)
 
@@ -350,8 +351,13 @@ def main():
     value = nq / (ms_per_step / 1000)
     e2e_value = nq / (e2e_ms / args.steps / 1000)
     kernel_avg = float(np.mean(kernel_ms))
-    F, S, Pp, L, N = (work[k] for k in ("entries", "records", "active_pairs", "relaxations", "claims"))
-    alg_bytes = 16 * F + 12 * S + 8 * Pp + 16 * L + 8 * N
+    # algorithmic bytes per launch, per engine class:
+    #   push (frontier, dense): 16 F + 12 S + 8 P + 16 L + 8 N (dense has N = 0)
+    #   Jacobi pull:            16 (vertex-lane items) + 12 (in-edge records) + 8 (relaxations)
+    pw, jw = engine_work["push"], engine_work["jacobi"]
+    F, S, Pp, L, N = (pw[k] for k in ("entries", "records", "active_pairs", "relaxations", "claims"))
+    alg_bytes = (16 * F + 12 * S + 8 * Pp + 16 * L + 8 * N +
+                 16 * jw["items"] + 12 * jw["records"] + 8 * jw["relaxations"])
     peaks_path = REPO / "MEASURED_PEAKS.json"
     if peaks_path.exists():
         peak = json.loads(peaks_path.read_text())["hbm_gbs"]
@@ -387,7 +393,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_src, "kernel": "persistent_kernel<false> (frontier)",
                      "kernel_ms": kernel_avg, "execute_ms": float(np.mean(execute_ms)),
-                     "algorithmic_bytes_per_launch": alg_bytes, "work": work},
+                     "algorithmic_bytes_per_launch": alg_bytes, "work": work, "engine_work": engine_work},
         "clocks": clocks.summary(),
         "gpu_launches": launches_per_step * args.steps,
     }

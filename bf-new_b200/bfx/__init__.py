@@ -644,6 +644,14 @@ class Workspace:
         _check(load().bfx_fetch_work_statistics(self._h, None, out))
         return dict(zip(self.WORK_KEYS, (int(x) for x in out)))
 
+    def engine_work(self) -> dict:
+        """Work counters split by engine class: push (frontier / dense) and Jacobi pull."""
+        out = (u64 * 16)()
+        _check(load().bfx_fetch_engine_work(self._h, out))
+        w = [int(x) for x in out]
+        return {"push": dict(zip(self.WORK_KEYS[:7], w[:7])), "rounds": w[7],
+                "jacobi": {"items": w[8], "records": w[9], "relaxations": w[10], "changes": w[11]}}
+
     def run_query(self, sources, targets, selected_tiles, options: GpuRunOptions) -> DeviceRunStatus:
         s = np.ascontiguousarray(np.unique(np.asarray(sources, np.uint32)))
         t = np.ascontiguousarray(np.unique(np.asarray(targets, np.uint32)))

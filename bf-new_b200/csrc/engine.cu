@@ -187,7 +187,7 @@ __global__ void init_kernel(LaunchParams p) {
     p.run->done = 0u;
     p.run->stop = 0u;
     p.run->abort = 0u;
-    for (int i = 0; i < 8; ++i) p.run->work[i] = 0u;
+    for (int i = 0; i < 16; ++i) p.run->work[i] = 0u;
   }
 }
 
@@ -251,13 +251,10 @@ __device__ __forceinline__ void jacobi_item(const LaunchParams& p, const DBatch&
     const u64 idx = (static_cast<u64>(cv) << B.shift) + ql;
     const u64 old = dev::ld_cg(dr + idx);
     u64 best = old;
+    if (kCount) wk.c[7] += 1;  // every vertex-lane item reads its label and writes the other slot
     if ((vt.x >> ql) & 1u) {
       const u32 cb = __ldg(p.g.csc_off + v), ce = __ldg(p.g.csc_off + v + 1);
-      if (kCount) {
-        wk.c[0] += 1;
-        wk.c[1] += ce - cb;
-        wk.c[2] += 1;
-      }
+      if (kCount) wk.c[8] += ce - cb;
       for (u32 e = cb; e < ce; ++e) {
         const uint4 rec = __ldg(p.g.csc + e);
         const uint2 su = B.tiles[rec.w];
@@ -266,12 +263,12 @@ __device__ __forceinline__ void jacobi_item(const LaunchParams& p, const DBatch&
           if (sb != dev::kInfBits) {
             const u64 cand = dev::candidate(sb, rec.y, rec.z);
             best = cand < best ? cand : best;
-            if (kCount) wk.c[3] += 1;
+            if (kCount) wk.c[9] += 1;
           }
         }
       }
       if (dev::hi(best) != dev::hi(old)) changed = 1u << ql;
-      if (kCount) wk.c[5] += changed != 0u;
+      if (kCount) wk.c[10] += changed != 0u;
     }
     dw[idx] = best;
   }
@@ -445,10 +442,11 @@ __device__ void round_bookkeeping(const LaunchParams& p, u32 r) {
 
 // Adds each thread's counters into the launch-wide totals.
 __device__ void flush_work(const LaunchParams& p, Work& wk) {
-  for (int i = 0; i < 7; ++i) {
+  for (int i = 0; i < 11; ++i) {
     u64 x = wk.c[i];
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xFFFFFFFFu, x, o);
-    if (lane_id() == 0 && x) atomicAdd(reinterpret_cast<unsigned long long*>(&p.run->work[i]), x);
+    const int slot = i < 7 ? i : i + 1;  // work[7] holds the round count
+    if (lane_id() == 0 && x) atomicAdd(reinterpret_cast<unsigned long long*>(&p.run->work[slot]), x);
   }
 }
 
@@ -1325,9 +1323,12 @@ int bfx_fetch_work_statistics(bfx_workspace* ws, bfx_device_work_statistics* sta
     bfx::require(ws != nullptr, "null workspace");
     bfx::require(ws->executed, "no executed batches");
     BFX_CUDA(cudaSetDevice(ws->graph->device));
-    std::uint64_t w[8];
-    BFX_CUDA(cudaMemcpyAsync(w, ws->params.run->work, sizeof(w), cudaMemcpyDeviceToHost, ws->stream));
+    std::uint64_t raw[16];
+    BFX_CUDA(cudaMemcpyAsync(raw, ws->params.run->work, sizeof(raw), cudaMemcpyDeviceToHost, ws->stream));
     BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    // totals over the engines: Jacobi items count as entries and source reads
+    const std::uint64_t w[8] = {raw[0] + raw[8], raw[1] + raw[9], raw[2] + raw[8], raw[3] + raw[10],
+                                raw[4],          raw[5] + raw[11], raw[6],         raw[7]};
     if (counters) std::memcpy(counters, w, sizeof(w));
     if (stats) {
       std::memset(stats, 0, sizeof(*stats));
@@ -1344,6 +1345,17 @@ int bfx_fetch_work_statistics(bfx_workspace* ws, bfx_device_work_statistics* sta
       stats->host_synchronizations = ws->last_host_checks;
       stats->controller_copies = ws->last_host_checks;
     }
+  });
+}
+
+int bfx_fetch_engine_work(bfx_workspace* ws, uint64_t counters[16]) {
+  return bfx::guarded([&] {
+    bfx::require(ws && counters, "null argument");
+    bfx::require(ws->executed, "no executed batches");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    BFX_CUDA(cudaMemcpyAsync(counters, ws->params.run->work, 16 * sizeof(std::uint64_t), cudaMemcpyDeviceToHost,
+                             ws->stream));
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
   });
 }
 

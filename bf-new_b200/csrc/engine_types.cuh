@@ -95,17 +95,21 @@ struct DRun {
   u32 abort;       // device failure seen
   u64 max_rounds;
   u64 launches;
-  u64 work[8];     // launch-wide work counters (instrumented runs)
+  u64 work[16];    // launch-wide work counters: [0..6] push engines, [7] rounds, [8..11] Jacobi
 };
 
 // Work counters of an instrumented run (instrumentation >= 1):
 // 0 queue entries processed, 1 edge records read, 2 active (vertex, lane)
 // source reads, 3 lane-edge relaxations, 4 queue claims, 5 distance
 // decreases, 6 min-reductions issued, 7 rounds executed.
+// Per-thread work counters of an instrumented run: c[0..6] frontier and
+// dense push (entries / vertex items, edge records, source reads, lane-edge
+// relaxations, queue claims, decreases, min-reductions), c[7..10] Jacobi
+// pull (vertex-lane items, in-edge records, relaxations, changes).
 struct Work {
-  u64 c[7];
+  u64 c[11];
   __device__ void zero() {
-    for (int i = 0; i < 7; ++i) c[i] = 0;
+    for (int i = 0; i < 11; ++i) c[i] = 0;
   }
 };
 

@@ -325,6 +325,11 @@ int bfx_last_launch_count(bfx_workspace *ws, uint64_t *launches);
  * relaxations, queue claims, distance decreases, min-reductions issued,
  * rounds}.  Without instrumentation the counters read zero. */
 int bfx_fetch_work_statistics(bfx_workspace *ws, bfx_device_work_statistics *stats, uint64_t counters[8]);
+/* The same counters split by engine (bfx extension, for per-engine
+ * algorithmic byte counts): [0..6] frontier and dense push in the order
+ * above, [7] rounds, [8..11] Jacobi pull {vertex-lane items, in-edge records,
+ * relaxations, changes}, [12..15] zero. */
+int bfx_fetch_engine_work(bfx_workspace *ws, uint64_t counters[16]);
 
 /* ---- plain per-query engine ----------------------------------------------
  * Replaces GpuSsspEngine::run(RouteQuery, GpuRunOptions) (gpu_api.hpp:203-211)
