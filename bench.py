@@ -382,6 +382,10 @@ def main():
                    "frontier_layout": args.frontier, "registers": args.regs,
                    "engines_chosen": None if engines_chosen is None else
                    {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
+                   "frontier_steps_chosen": None if engines_chosen is None else
+                   {("plain" if not np.isfinite(d) else f"{d:.4g}"): sum(
+                       1 for e, x in zip(engines_chosen, ws.tuned_deltas) if e == 2 and x == d)
+                    for d in sorted({x for e, x in zip(engines_chosen, ws.tuned_deltas) if e == 2})},
                    "control": "persistent_cooperative", "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (graph %s GB + labels), no flush" % (
                        "0.54" if args.workload == "c2" else "5.4")},

@@ -2,8 +2,8 @@
 // shootout, src/engine_shootout.cpp, only catalogues configurations).
 //
 // For every batch of a set, the tuner runs the candidate configurations --
-// frontier push (plain, and near/far with threshold steps of 2, 8 and 32
-// mean edge weights), Jacobi pull, dense chaotic push -- on that batch alone
+// frontier push (plain, and near/far with threshold steps of 1/2, 1, 2, 4, 8
+// and 32 mean edge weights), Jacobi pull, dense chaotic push -- on that batch alone
 // and keeps the fastest by device time (the library's own CUDA events around
 // the relaxation launch, best of `trials`).  Choices are cached per batch
 // signature -- lane width, valid lanes, and the binary magnitudes of the
@@ -64,10 +64,12 @@ extern "C" int bfx_autotune(bfx_workspace* ws, uint32_t count, const bfx_batch_d
     bfx::check(bfx_workspace_graph_stats(ws, stats));
     const float w = stats[0] > 0.0 ? static_cast<float>(stats[0]) : 1.0f;
     // Candidates: the three engines; frontier push also with near/far
-    // threshold steps of 2, 8 and 32 mean edge weights.
-    const Choice candidates[] = {{BFX_ENGINE_FRONTIER_PUSH, kPlain},       {BFX_ENGINE_FRONTIER_PUSH, 2.0f * w},
-                                 {BFX_ENGINE_FRONTIER_PUSH, 8.0f * w},     {BFX_ENGINE_FRONTIER_PUSH, 32.0f * w},
-                                 {BFX_ENGINE_JACOBI_PULL, kPlain},         {BFX_ENGINE_DENSE_CHAOTIC_PUSH, kPlain}};
+    // threshold steps of 1/2, 1, 2, 4, 8 and 32 mean edge weights.
+    const Choice candidates[] = {{BFX_ENGINE_FRONTIER_PUSH, kPlain},       {BFX_ENGINE_FRONTIER_PUSH, 0.5f * w},
+                                 {BFX_ENGINE_FRONTIER_PUSH, 1.0f * w},     {BFX_ENGINE_FRONTIER_PUSH, 2.0f * w},
+                                 {BFX_ENGINE_FRONTIER_PUSH, 4.0f * w},     {BFX_ENGINE_FRONTIER_PUSH, 8.0f * w},
+                                 {BFX_ENGINE_FRONTIER_PUSH, 32.0f * w},    {BFX_ENGINE_JACOBI_PULL, kPlain},
+                                 {BFX_ENGINE_DENSE_CHAOTIC_PUSH, kPlain}};
     std::vector<Choice> chosen(count, Choice{BFX_ENGINE_FRONTIER_PUSH, kPlain});
     std::uint32_t n_measured = 0;
     for (std::uint32_t b = 0; b < count; ++b) {

@@ -263,7 +263,7 @@ int bfx_resident_graph_set_weights(bfx_resident_graph *graph, const float *weigh
 /* ---- engine autotuner ----------------------------------------------------------
  * No counterpart in the reference (its engine shootout, src/engine_shootout.cpp,
  * only catalogues configurations).  Picks, per batch, frontier push (plain or
- * near/far with a threshold step of 2, 8 or 32 mean edge weights), Jacobi
+ * near/far with a threshold step of 1/2, 1, 2, 4, 8 or 32 mean edge weights), Jacobi
  * pull or dense chaotic push by timing each candidate on the batch alone
  * (best of `trials` device timings), caching the choice per batch shape (lane
  * width, valid lanes, magnitude of union vertices and tiles).  Leaves the
