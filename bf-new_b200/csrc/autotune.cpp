@@ -1,15 +1,19 @@
 // Per-batch engine autotuner (a bfx component; the reference's engine
 // shootout, src/engine_shootout.cpp, only catalogues configurations).
 //
-// For every batch of a set, the tuner runs the candidate configurations --
-// frontier push (plain, and near/far with threshold steps of 1/2, 1, 2, 4, 8
-// and 32 mean edge weights), Jacobi pull, dense chaotic push -- on that batch alone
-// and keeps the fastest by device time (the library's own CUDA events around
-// the relaxation launch, best of `trials`).  Choices are cached per batch
-// signature -- lane width, valid lanes, and the binary magnitudes of the
-// union vertex count and union tile count -- so later sets with batches of
-// the same shape are tuned without measuring.  The set is prepared again at
-// the end and its per-batch engines and steps are stored in the workspace, so an
+// Three phases, all timed on the device with the library's own CUDA events
+// around the relaxation launch (best of `trials`):
+//  1. In context: the whole set on frontier push with one near/far step for
+//     every batch -- plain, and 1/2, 1, 2, 4, 8, 32 mean edge weights -- as it
+//     will run, in one launch; the fastest step wins.  (A batch timed alone
+//     favours few rounds; in one launch with others the work matters.)
+//  2. Per batch shape: Jacobi pull or dense chaotic push replaces frontier
+//     push only where it is at least 1.5x faster on the batch alone.  Cached
+//     by batch signature -- lane width, valid lanes, and the binary
+//     magnitudes of the union vertex and tile counts.
+//  3. In context again: the per-batch engines are kept only if the whole set
+//     runs faster with them than all-frontier with the phase-1 step.
+// The set is left prepared with its per-batch engines and steps, so an
 // execute with engine == BFX_ENGINE_AUTO runs each batch on its own engine
 // inside one launch.
 #include "bfx.h"
@@ -52,6 +56,24 @@ void check(int rc) {
 }  // namespace
 }  // namespace bfx
 
+namespace bfx {
+namespace {
+
+// Best-of-`trials` relaxation time of the prepared set with `o`.
+float time_set(bfx_workspace* ws, const bfx_gpu_run_options& o, std::uint32_t trials) {
+  float best = 0.0f;
+  for (std::uint32_t t = 0; t < trials; ++t) {
+    check(bfx_execute(ws, &o));
+    float ms[2];
+    check(bfx_last_execute_timing(ws, ms));
+    if (t == 0 || ms[0] < best) best = ms[0];
+  }
+  return best;
+}
+
+}  // namespace
+}  // namespace bfx
+
 extern "C" int bfx_autotune(bfx_workspace* ws, uint32_t count, const bfx_batch_description* batches,
                             const bfx_gpu_run_options* base, uint32_t trials, uint32_t* engines_out,
                             float* deltas_out, uint32_t* measured) {
@@ -63,14 +85,32 @@ extern "C" int bfx_autotune(bfx_workspace* ws, uint32_t count, const bfx_batch_d
     double stats[2];
     bfx::check(bfx_workspace_graph_stats(ws, stats));
     const float w = stats[0] > 0.0 ? static_cast<float>(stats[0]) : 1.0f;
-    // Candidates: the three engines; frontier push also with near/far
-    // threshold steps of 1/2, 1, 2, 4, 8 and 32 mean edge weights.
-    const Choice candidates[] = {{BFX_ENGINE_FRONTIER_PUSH, kPlain},       {BFX_ENGINE_FRONTIER_PUSH, 0.5f * w},
-                                 {BFX_ENGINE_FRONTIER_PUSH, 1.0f * w},     {BFX_ENGINE_FRONTIER_PUSH, 2.0f * w},
-                                 {BFX_ENGINE_FRONTIER_PUSH, 4.0f * w},     {BFX_ENGINE_FRONTIER_PUSH, 8.0f * w},
-                                 {BFX_ENGINE_FRONTIER_PUSH, 32.0f * w},    {BFX_ENGINE_JACOBI_PULL, kPlain},
-                                 {BFX_ENGINE_DENSE_CHAOTIC_PUSH, kPlain}};
-    std::vector<Choice> chosen(count, Choice{BFX_ENGINE_FRONTIER_PUSH, kPlain});
+    bfx_gpu_run_options o;
+    std::memcpy(&o, base, sizeof(o));
+    o.instrumentation = 0;
+
+    // Phase 1, in context: every batch on frontier push with one step, the
+    // whole set relaxed together as it will run; keep the fastest step.
+    const float steps[] = {kPlain, 0.5f * w, 1.0f * w, 2.0f * w, 4.0f * w, 8.0f * w, 32.0f * w};
+    bfx::check(bfx_prepare_batches(ws, count, batches));
+    o.engine = BFX_ENGINE_FRONTIER_PUSH;
+    float best_step = kPlain, best_set = 0.0f;
+    for (std::size_t i = 0; i < sizeof(steps) / sizeof(steps[0]); ++i) {
+      const std::vector<float> d(count, steps[i]);
+      bfx::check(bfx_set_batch_deltas(ws, count, d.data()));
+      const float t = bfx::time_set(ws, o, trials);
+      if (i == 0 || t < best_set) {
+        best_set = t;
+        best_step = steps[i];
+      }
+    }
+
+    // Phase 2, per batch shape: Jacobi pull or dense push replaces frontier
+    // push (with the chosen step) only where it is at least 1.5x faster on
+    // the batch alone; choices are cached by batch signature.
+    const Choice frontier{BFX_ENGINE_FRONTIER_PUSH, best_step};
+    const Choice candidates[] = {frontier, {BFX_ENGINE_JACOBI_PULL, kPlain}, {BFX_ENGINE_DENSE_CHAOTIC_PUSH, kPlain}};
+    std::vector<Choice> chosen(count, frontier);
     std::uint32_t n_measured = 0;
     for (std::uint32_t b = 0; b < count; ++b) {
       const bfx::Signature sig = bfx::signature(batches[b]);
@@ -78,46 +118,55 @@ extern "C" int bfx_autotune(bfx_workspace* ws, uint32_t count, const bfx_batch_d
         std::lock_guard<std::mutex> lock(bfx::g_tune_mutex);
         const auto it = bfx::g_tune_cache.find(sig);
         if (it != bfx::g_tune_cache.end()) {
-          chosen[b] = it->second;
+          chosen[b] = it->second.engine == BFX_ENGINE_FRONTIER_PUSH ? frontier : it->second;
           continue;
         }
       }
       bfx::check(bfx_prepare_batches(ws, 1, &batches[b]));
-      float best = 0.0f;
-      Choice best_choice{BFX_ENGINE_FRONTIER_PUSH, kPlain};
-      bool have = false;
+      float t_frontier = 0.0f, best = 0.0f;
+      Choice pick = frontier;
       for (const Choice& c : candidates) {
-        bfx_gpu_run_options o;
-        std::memcpy(&o, base, sizeof(o));
-        o.engine = c.engine;
-        o.instrumentation = 0;
         bfx::check(bfx_set_batch_deltas(ws, 1, &c.delta));
-        float t_best = 0.0f;
-        for (std::uint32_t t = 0; t < trials; ++t) {
-          bfx::check(bfx_execute(ws, &o));
-          float ms[2];
-          bfx::check(bfx_last_execute_timing(ws, ms));
-          if (t == 0 || ms[0] < t_best) t_best = ms[0];
-        }
-        if (!have || t_best < best) {
-          best = t_best;
-          best_choice = c;
-          have = true;
+        bfx_gpu_run_options oc = o;
+        oc.engine = c.engine;
+        const float t = bfx::time_set(ws, oc, trials);
+        if (c.engine == BFX_ENGINE_FRONTIER_PUSH) {
+          t_frontier = best = t;
+        } else if (t * 1.5f <= t_frontier && t < best) {
+          best = t;
+          pick = c;
         }
       }
-      chosen[b] = best_choice;
+      chosen[b] = pick;
       ++n_measured;
       std::lock_guard<std::mutex> lock(bfx::g_tune_mutex);
-      bfx::g_tune_cache[sig] = best_choice;
+      bfx::g_tune_cache[sig] = pick;
     }
-    bfx::check(bfx_prepare_batches(ws, count, batches));
+
+    // Phase 3, in context: keep the per-batch engines only if the whole set
+    // runs faster with them than all-frontier with the chosen step.
     std::vector<std::uint32_t> engines(count);
     std::vector<float> deltas(count);
     for (std::uint32_t b = 0; b < count; ++b) {
       engines[b] = chosen[b].engine;
       deltas[b] = chosen[b].delta;
-      engines_out[b] = chosen[b].engine;
-      if (deltas_out) deltas_out[b] = chosen[b].delta;
+    }
+    bfx::check(bfx_prepare_batches(ws, count, batches));
+    bool mixed = false;
+    for (std::uint32_t e : engines) mixed = mixed || e != BFX_ENGINE_FRONTIER_PUSH;
+    if (mixed) {
+      bfx::check(bfx_set_batch_engines(ws, count, engines.data()));
+      bfx::check(bfx_set_batch_deltas(ws, count, deltas.data()));
+      bfx_gpu_run_options oa = o;
+      oa.engine = BFX_ENGINE_AUTO;
+      if (bfx::time_set(ws, oa, trials) >= best_set) {
+        std::fill(engines.begin(), engines.end(), static_cast<std::uint32_t>(BFX_ENGINE_FRONTIER_PUSH));
+        std::fill(deltas.begin(), deltas.end(), best_step);
+      }
+    }
+    for (std::uint32_t b = 0; b < count; ++b) {
+      engines_out[b] = engines[b];
+      if (deltas_out) deltas_out[b] = deltas[b];
     }
     bfx::check(bfx_set_batch_engines(ws, count, engines.data()));
     bfx::check(bfx_set_batch_deltas(ws, count, deltas.data()));

@@ -262,11 +262,13 @@ int bfx_resident_graph_set_weights(bfx_resident_graph *graph, const float *weigh
 
 /* ---- engine autotuner ----------------------------------------------------------
  * No counterpart in the reference (its engine shootout, src/engine_shootout.cpp,
- * only catalogues configurations).  Picks, per batch, frontier push (plain or
- * near/far with a threshold step of 1/2, 1, 2, 4, 8 or 32 mean edge weights), Jacobi
- * pull or dense chaotic push by timing each candidate on the batch alone
- * (best of `trials` device timings), caching the choice per batch shape (lane
- * width, valid lanes, magnitude of union vertices and tiles).  Leaves the
+ * only catalogues configurations).  Picks the near/far step of frontier push
+ * (plain, or 1/2, 1, 2, 4, 8 or 32 mean edge weights) by timing the whole set
+ * in one launch, then per batch shape Jacobi pull or dense chaotic push where
+ * it is at least 1.5x faster on the batch alone (cached per lane width, valid
+ * lanes, magnitude of union vertices and tiles), and keeps those engines only
+ * if the whole set runs faster with them (best of `trials` device timings
+ * each).  Leaves the
  * workspace prepared with all `count` batches and their engines and steps, so
  * bfx_execute with options->engine == BFX_ENGINE_AUTO relaxes each batch with
  * its own engine in one launch.  engines_out[count]; deltas_out[count] (may be
