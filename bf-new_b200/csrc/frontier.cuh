@@ -296,10 +296,11 @@ __device__ __forceinline__ void enqueue_claims(bool claim, u32 v, u32 cv, u32* c
 // so each thread keeps two dependent chains in flight.  A thread finds the
 // entry of a work item by a binary search over the warp's inclusive work scan
 // (five shuffles).  Every thread ORs its own success into the next round's
-// pending word; the OR that turns the word non-zero claims the vertex, and
-// claimed vertices are staged in the warp's shared-memory buffer and written
-// to the next queue with one counter atomic per 32 or more claims, off the
-// per-step chain.  All loops are warp-uniform.
+// pending word; the OR that turns the word non-zero claims the vertex.  The
+// ORs' results are read one iteration later (after the next items' first
+// loads are issued), and claimed vertices are staged in the warp's
+// shared-memory buffer and written to the next queue with one counter atomic
+// per 32 or more claims, off the per-step chain.  All loops are warp-uniform.
 constexpr u32 kStage = 64;  // staged claims per warp: < 32 before a call adds <= 32
 
 struct FlatItem {
@@ -395,6 +396,9 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
   }
   const u32 excl = incl - work;
   const u32 total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  // Claims of the previous iteration: their pending-word ORs stay in flight
+  // while this iteration decodes its items and issues its first loads.
+  u32 p_old[2] = {1u, 1u}, p_v[2] = {0u, 0u}, p_cv[2] = {0u, 0u};
   for (u32 base = 0; base < total; base += 64u) {
     FlatItem it[2];
     u32 src[2], bits[2], fbits[2], cdst[2], dstv[2];
@@ -413,6 +417,11 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
         src[u] = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(it[u].cv) << B.shift) + it[u].ql)));
         rec[u] = __ldg(p.g.csr + it[u].ed);
       }
+    }
+#pragma unroll
+    for (u32 u = 0; u < 2u; ++u) {
+      stage_claims<kCount>(p_old[u] == 0u, p_v[u], p_cv[u], stage, staged, false, &C.count[widx], B.queue_w, B, C,
+                           wk);
     }
 #pragma unroll
     for (u32 u = 0; u < 2u; ++u) {
@@ -462,15 +471,18 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
         enqueue_claims<kCount>(fclaim, dstv[u], cdst[u], &C.fcount[pile], B.pile, B, C, false, wk);
       }
     }
-    // both pending-word ORs are issued before either result is used
-    u32 old[2];
-#pragma unroll
-    for (u32 u = 0; u < 2u; ++u) old[u] = bits[u] != 0u ? atomicOr(B.mask_w + cdst[u], bits[u]) : 1u;
+    // both pending-word ORs are issued here; their results are read by the
+    // next iteration (or after the loop)
 #pragma unroll
     for (u32 u = 0; u < 2u; ++u) {
-      stage_claims<kCount>(old[u] == 0u, dstv[u], cdst[u], stage, staged, false, &C.count[widx], B.queue_w, B, C,
-                           wk);
+      p_old[u] = bits[u] != 0u ? atomicOr(B.mask_w + cdst[u], bits[u]) : 1u;
+      p_v[u] = dstv[u];
+      p_cv[u] = cdst[u];
     }
   }
-  stage_claims<kCount>(false, 0u, 0u, stage, staged, true, &C.count[widx], B.queue_w, B, C, wk);
+#pragma unroll
+  for (u32 u = 0; u < 2u; ++u) {
+    stage_claims<kCount>(p_old[u] == 0u, p_v[u], p_cv[u], stage, staged, u == 1u, &C.count[widx], B.queue_w, B, C,
+                         wk);
+  }
 }
