@@ -180,6 +180,8 @@ def main():
                     help="frontier-push work layout (sub-warp groups or flat work list)")
     ap.add_argument("--regs", type=int, default=64, choices=[40, 64],
                     help="register budget of the persistent kernel")
+    ap.add_argument("--items", type=int, default=2, choices=[2, 3, 4],
+                    help="flat layout: work items per thread per iteration")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=None)
     args = ap.parse_args()
@@ -203,7 +205,7 @@ def main():
     from bfx import replicas, workloads
 
     t0 = time.time()
-    g, order, gstats = bfx.synth_graph(**workloads.GRAPHS[args.workload])
+    g, order, gstats = bfx.synth_graph(**workloads.GRAPHS["c3" if args.workload == "c5" else args.workload])
     layout = bfx.build_device_graph_layout(g, order)
     # query classes: (queries, plain-engine sample size) -- the plain per-query
     # rate is extrapolated class by class from its sample
@@ -243,6 +245,7 @@ def main():
     ws = bfx.Workspace(resident)
     ws.set_frontier_layout(bfx.FRONTIER_FLAT if args.frontier == "flat" else bfx.FRONTIER_GROUPS)
     ws.set_register_budget(args.regs)
+    ws.set_flat_items(args.items)
     engine_id = {"auto": bfx.ENGINE_AUTO, "frontier": bfx.ENGINE_FRONTIER_PUSH, "jacobi": bfx.ENGINE_JACOBI_PULL,
                  "dense": bfx.ENGINE_DENSE_CHAOTIC_PUSH}[args.engine]
     engines_chosen = None
@@ -379,7 +382,7 @@ def main():
         "config": {"workload": workload_desc,
                    "queries_per_gpu": len(queries), "batches": plan.batch_count,
                    "lane_widths": sorted({d.lane_width for d in descs}), "engine": args.engine,
-                   "frontier_layout": args.frontier, "registers": args.regs,
+                   "frontier_layout": args.frontier, "registers": args.regs, "flat_items": args.items,
                    "engines_chosen": None if engines_chosen is None else
                    {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
                    "frontier_steps_chosen": None if engines_chosen is None else

@@ -552,6 +552,10 @@ class Workspace:
         """40 (three 512-thread blocks per SM) or 64 registers per thread for the persistent kernel."""
         _check(load().bfx_set_register_budget(self._h, u32(registers)))
 
+    def set_flat_items(self, items: int):
+        """Flat layout: work items per thread per iteration (2, 3 or 4)."""
+        _check(load().bfx_set_flat_items(self._h, u32(items)))
+
     def set_frontier_layout(self, layout: int):
         """FRONTIER_GROUPS (sub-warp groups per entry) or FRONTIER_FLAT (flat work list)."""
         _check(load().bfx_set_frontier_layout(self._h, u32(layout)))

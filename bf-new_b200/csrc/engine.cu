@@ -356,7 +356,7 @@ __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
   return prefix[p.nb];
 }
 
-template <bool kCount>
+template <bool kCount, u32 kItems>
 __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work& wk) {
   const u32 ridx = r % 3u, widx = (r + 1u) % 3u;
   const u32 total = prefix[p.nb];
@@ -390,7 +390,7 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
       const FrontierView V = frontier_view(B, r & 1u, g % 3u, (g + 1u) % 3u);
       if (n != 0u) {
         if (p.flat) {
-          frontier_flat<kCount>(p, V, C, item, n, r & 1u, widx, tau, g % 3u, wk);
+          frontier_flat<kCount, kItems>(p, V, C, item, n, r & 1u, widx, tau, g % 3u, wk);
         } else if (B.W <= 8u) {
           frontier_group<kCount, 8>(p, V, C, item, n, r & 1u, widx, tau, g % 3u, wk);
         } else {
@@ -453,7 +453,8 @@ __device__ void flush_work(const LaunchParams& p, Work& wk) {
 // kMinBlocks = resident 512-thread blocks per SM the register budget is set
 // for: 3 -> 40 registers per thread (48 warps per SM), 2 -> 64 registers
 // (32 warps per SM, no spills).
-template <bool kCount, int kMinBlocks>
+// kItems = flat-layout work items per thread per iteration.
+template <bool kCount, int kMinBlocks, u32 kItems>
 __global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParams p) {
   extern __shared__ u32 prefix[];
   const u32 nblocks = gridDim.x;
@@ -465,7 +466,7 @@ __global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParam
     const u32 total = round_work(p, r, prefix);
     if (total == 0u || r >= p.max_rounds) break;
     if (blockIdx.x == 0) round_bookkeeping(p, r);
-    round_body<kCount>(p, r, prefix, wk);
+    round_body<kCount, kItems>(p, r, prefix, wk);
     // Past the launch budget block 0 raises the barrier's abort before it
     // arrives, so every block leaves after this round.
     if (blockIdx.x == 0 && threadIdx.x == 0 && dev::global_ns() - t0 > p.budget_ns) {
@@ -494,7 +495,7 @@ __global__ void __launch_bounds__(512, 3) round_kernel(LaunchParams p) {
   if (total == 0u) return;
   Work wk;
   wk.zero();
-  round_body<kCount>(p, r, prefix, wk);
+  round_body<kCount, 2>(p, r, prefix, wk);
   if (kCount) flush_work(p, wk);
 }
 
@@ -1107,6 +1108,25 @@ int grid_blocks(bfx_workspace* ws, const void* kernel, int block, size_t smem, c
   return per_sm * ws->sm_count;
 }
 
+// Persistent kernel instantiation: 64 registers (two 512-thread blocks per
+// SM) with 2, 3 or 4 flat work items per thread, or 40 registers with 2.
+const void* persistent_entry(bool count, bool wide, std::uint32_t items) {
+  if (!wide) {
+    return count ? reinterpret_cast<const void*>(persistent_kernel<true, 3, 2>)
+                 : reinterpret_cast<const void*>(persistent_kernel<false, 3, 2>);
+  }
+  if (items == 3u) {
+    return count ? reinterpret_cast<const void*>(persistent_kernel<true, 2, 3>)
+                 : reinterpret_cast<const void*>(persistent_kernel<false, 2, 3>);
+  }
+  if (items == 4u) {
+    return count ? reinterpret_cast<const void*>(persistent_kernel<true, 2, 4>)
+                 : reinterpret_cast<const void*>(persistent_kernel<false, 2, 4>);
+  }
+  return count ? reinterpret_cast<const void*>(persistent_kernel<true, 2, 2>)
+               : reinterpret_cast<const void*>(persistent_kernel<false, 2, 2>);
+}
+
 void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   require(ws->nb > 0, "no prepared batches");
   validate_options(o, true);
@@ -1158,12 +1178,7 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   BFX_CUDA(cudaGetLastError());
   BFX_CUDA(cudaEventRecord(ws->ev[1], ws->stream));
   if (o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
-    const bool wide = ws->register_budget == 64u;
-    const void* kfn = o.instrumentation
-                          ? (wide ? reinterpret_cast<const void*>(persistent_kernel<true, 2>)
-                                  : reinterpret_cast<const void*>(persistent_kernel<true, 3>))
-                          : (wide ? reinterpret_cast<const void*>(persistent_kernel<false, 2>)
-                                  : reinterpret_cast<const void*>(persistent_kernel<false, 3>));
+    const void* kfn = persistent_entry(o.instrumentation != 0u, ws->register_budget == 64u, ws->flat_items);
     const int grid = grid_blocks(ws, kfn, block, smem, o);
     void* args[] = {&p};
     BFX_CUDA(cudaLaunchCooperativeKernel(kfn, grid, block, args, smem, ws->stream));
@@ -1247,6 +1262,14 @@ int bfx_set_register_budget(bfx_workspace* ws, uint32_t registers) {
     bfx::require(ws != nullptr, "null argument");
     bfx::require(registers == 40u || registers == 64u, "register budget must be 40 or 64");
     ws->register_budget = registers;
+  });
+}
+
+int bfx_set_flat_items(bfx_workspace* ws, uint32_t items) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null argument");
+    bfx::require(items >= 2u && items <= 4u, "flat work items per thread must be 2, 3 or 4");
+    ws->flat_items = items;
   });
 }
 
@@ -1686,7 +1709,7 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
     const size_t smem = 8;
     int per_sm = 0;
     BFX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, reinterpret_cast<const void*>(bfx::persistent_kernel<false, 3>), block, smem));
+        &per_sm, reinterpret_cast<const void*>(bfx::persistent_kernel<false, 3, 2>), block, smem));
     if (per_sm <= 0) throw bfx::Error(BFX_ERR_CUDA, "kernel cannot be resident with this block size");
     if (options->grid_policy == 1u) {
       if (static_cast<int>(options->blocks_per_wgp) > per_sm)
@@ -1694,7 +1717,7 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
       per_sm = static_cast<int>(options->blocks_per_wgp);
     }
     void* args[] = {&p};
-    BFX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(bfx::persistent_kernel<false, 3>),
+    BFX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(bfx::persistent_kernel<false, 3, 2>),
                                          per_sm * sms, block, args, smem, 0));
     auto* d_status = reinterpret_cast<bfx_device_run_status*>(base + o_status);
     bfx::finalize_kernel<<<1, 256>>>(p, reinterpret_cast<bfx_device_controller*>(base + o_ctrl), d_status);

@@ -303,6 +303,14 @@ __device__ __forceinline__ void enqueue_claims(bool claim, u32 v, u32 cv, u32* c
 // per 32 or more claims, off the per-step chain.  All loops are warp-uniform.
 constexpr u32 kStage = 64;  // staged claims per warp: < 32 before a call adds <= 32
 
+template <u32 N>
+__device__ __forceinline__ bool any_far(const u32 (&f)[N]) {
+  u32 x = 0u;
+#pragma unroll
+  for (u32 u = 0; u < N; ++u) x |= f[u];
+  return x != 0u;
+}
+
 struct FlatItem {
   bool live;
   u32 ql, ed, cv;
@@ -360,7 +368,7 @@ __device__ __forceinline__ void stage_claims(bool claim, u32 v, u32 cv, u64* sta
   n = 0u;
 }
 
-template <bool kCount>
+template <bool kCount, u32 kItems>
 __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
                                               u32 rd, u32 widx, u32 tau_bits, u32 pile, Work& wk) {
   __shared__ u64 s_stage[16][kStage];  // blocks of up to 512 threads
@@ -398,43 +406,48 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
   const u32 total = __shfl_sync(0xFFFFFFFFu, incl, 31);
   // Claims of the previous iteration: their pending-word ORs stay in flight
   // while this iteration decodes its items and issues its first loads.
-  u32 p_old[2] = {1u, 1u}, p_v[2] = {0u, 0u}, p_cv[2] = {0u, 0u};
-  for (u32 base = 0; base < total; base += 64u) {
-    FlatItem it[2];
-    u32 src[2], bits[2], fbits[2], cdst[2], dstv[2];
-    uint4 rec[2];
-    uint2 dt[2];
+  u32 p_old[kItems], p_v[kItems], p_cv[kItems];
+#pragma unroll
+  for (u32 u = 0; u < kItems; ++u) {
+    p_old[u] = 1u;
+    p_v[u] = p_cv[u] = 0u;
+  }
+  for (u32 base = 0; base < total; base += 32u * kItems) {
+    FlatItem it[kItems];
+    u32 src[kItems], bits[kItems], fbits[kItems], cdst[kItems], dstv[kItems];
+    uint4 rec[kItems];
+    uint2 dt[kItems];
     u32 fd = 0xFFFFFFFFu;
 #pragma unroll
-    for (u32 u = 0; u < 2u; ++u) {
+    for (u32 u = 0; u < kItems; ++u) {
       it[u] = flat_decode(base + 32u * u + lane, total, incl, excl, cv, m, rb, deg);
       bits[u] = fbits[u] = cdst[u] = dstv[u] = 0u;
       src[u] = dev::kInfBits;
     }
 #pragma unroll
-    for (u32 u = 0; u < 2u; ++u) {
+    for (u32 u = 0; u < kItems; ++u) {
       if (it[u].live) {
         src[u] = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(it[u].cv) << B.shift) + it[u].ql)));
         rec[u] = __ldg(p.g.csr + it[u].ed);
       }
     }
 #pragma unroll
-    for (u32 u = 0; u < 2u; ++u) {
+    for (u32 u = 0; u < kItems; ++u) {
       stage_claims<kCount>(p_old[u] == 0u, p_v[u], p_cv[u], stage, staged, false, &C.count[widx], B.queue_w, B, C,
                            wk);
     }
 #pragma unroll
-    for (u32 u = 0; u < 2u; ++u) {
+    for (u32 u = 0; u < kItems; ++u) {
       if (it[u].live) {
         dt[u] = B.tiles[rec[u].w];
         cdst[u] = rec[u].x - dt[u].y;
         dstv[u] = rec[u].x;
       }
     }
-    u64 cur[2], cand[2];
-    bool relax[2];
+    u64 cur[kItems], cand[kItems];
+    bool relax[kItems];
 #pragma unroll
-    for (u32 u = 0; u < 2u; ++u) {
+    for (u32 u = 0; u < kItems; ++u) {
       relax[u] = it[u].live && ((dt[u].x >> it[u].ql) & 1u) && src[u] != dev::kInfBits;
       if (relax[u]) {
         cand[u] = dev::candidate(src[u], rec[u].y, rec[u].z);
@@ -442,7 +455,7 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
       }
     }
 #pragma unroll
-    for (u32 u = 0; u < 2u; ++u) {
+    for (u32 u = 0; u < kItems; ++u) {
       if (relax[u]) {
         if (kCount) wk.c[3] += 1;
         if (cand[u] < cur[u]) {
@@ -462,11 +475,11 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
         }
       }
     }
-    if (__any_sync(0xFFFFFFFFu, (fbits[0] | fbits[1]) != 0u)) {
+    if (__any_sync(0xFFFFFFFFu, any_far(fbits))) {
       fd = __reduce_min_sync(0xFFFFFFFFu, fd);
       if (lane == 0u) atomicMin(&C.fmin[pile], fd);
 #pragma unroll
-      for (u32 u = 0; u < 2u; ++u) {
+      for (u32 u = 0; u < kItems; ++u) {
         const bool fclaim = fbits[u] != 0u && atomicOr(B.fmask + cdst[u], fbits[u]) == 0u;
         enqueue_claims<kCount>(fclaim, dstv[u], cdst[u], &C.fcount[pile], B.pile, B, C, false, wk);
       }
@@ -474,15 +487,15 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
     // both pending-word ORs are issued here; their results are read by the
     // next iteration (or after the loop)
 #pragma unroll
-    for (u32 u = 0; u < 2u; ++u) {
+    for (u32 u = 0; u < kItems; ++u) {
       p_old[u] = bits[u] != 0u ? atomicOr(B.mask_w + cdst[u], bits[u]) : 1u;
       p_v[u] = dstv[u];
       p_cv[u] = cdst[u];
     }
   }
 #pragma unroll
-  for (u32 u = 0; u < 2u; ++u) {
-    stage_claims<kCount>(p_old[u] == 0u, p_v[u], p_cv[u], stage, staged, u == 1u, &C.count[widx], B.queue_w, B, C,
+  for (u32 u = 0; u < kItems; ++u) {
+    stage_claims<kCount>(p_old[u] == 0u, p_v[u], p_cv[u], stage, staged, u == kItems - 1u, &C.count[widx], B.queue_w, B, C,
                          wk);
   }
 }

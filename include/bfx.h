@@ -305,6 +305,11 @@ int bfx_set_frontier_layout(bfx_workspace *ws, uint32_t layout);
  * SM) or 64 (two blocks per SM, the default: no spills in the group layout,
  * few in the flat one). */
 int bfx_set_register_budget(bfx_workspace *ws, uint32_t registers);
+/* Flat layout, persistent control with the 64-register budget: work items
+ * each thread keeps in flight per iteration, 2 (default), 3 or 4 -- more
+ * independent memory chains against more register spills.  Other
+ * configurations use 2. */
+int bfx_set_flat_items(bfx_workspace *ws, uint32_t items);
 /* {mean edge weight, edge count} of the workspace's resident graph. */
 int bfx_workspace_graph_stats(bfx_workspace *ws, double out[2]);
 
