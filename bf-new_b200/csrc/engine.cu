@@ -452,7 +452,7 @@ __device__ void flush_work(const LaunchParams& p, Work& wk) {
 
 // kMinBlocks = resident 512-thread blocks per SM the register budget is set
 // for: 3 -> 40 registers per thread (48 warps per SM), 2 -> 64 registers
-// (32 warps per SM, no spills).
+// (32 warps per SM; no spills in the group layout, a few in the flat one).
 // kItems = flat-layout work items per thread per iteration.
 template <bool kCount, int kMinBlocks, u32 kItems>
 __global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParams p) {
