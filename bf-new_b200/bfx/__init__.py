@@ -648,6 +648,14 @@ class Workspace:
         _check(load().bfx_fetch_work_statistics(self._h, None, out))
         return dict(zip(self.WORK_KEYS, (int(x) for x in out)))
 
+    def round_trace(self) -> np.ndarray:
+        """(rounds, 2) array of {start ns, warp items} from the last instrumentation-2 persistent run."""
+        n = u32()
+        _check(load().bfx_fetch_round_trace(self._h, u32(0), None, C.byref(n)))
+        out = np.zeros((max(n.value, 1), 2), np.uint64)
+        _check(load().bfx_fetch_round_trace(self._h, u32(n.value), _ptr(out, u64), C.byref(n)))
+        return out[:n.value]
+
     def engine_work(self) -> dict:
         """Work counters split by engine class: push (frontier / dense) and Jacobi pull."""
         out = (u64 * 16)()

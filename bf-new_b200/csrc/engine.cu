@@ -466,6 +466,10 @@ __global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParam
     const u32 total = round_work(p, r, prefix);
     if (total == 0u || r >= p.max_rounds) break;
     if (blockIdx.x == 0) round_bookkeeping(p, r);
+    if (p.round_trace != nullptr && blockIdx.x == 0 && threadIdx.x == 0 && r < p.trace_cap) {
+      p.round_trace[2u * r] = dev::global_ns();
+      p.round_trace[2u * r + 1u] = total;
+    }
     round_body<kCount, kItems>(p, r, prefix, wk);
     // Past the launch budget block 0 raises the barrier's abort before it
     // arrives, so every block leaves after this round.
@@ -1139,6 +1143,13 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   p.engines = nullptr;
   p.deltas = nullptr;
   p.flat = ws->frontier_layout == BFX_FRONTIER_FLAT ? 1u : 0u;
+  p.round_trace = nullptr;
+  p.trace_cap = 0u;
+  if (o.instrumentation == 2u && o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
+    ws->round_trace.reserve(size_t{kRoundTraceCap} * 16u, ws->graph->device);
+    p.round_trace = static_cast<u64*>(ws->round_trace.ptr);
+    p.trace_cap = kRoundTraceCap;
+  }
   if (!ws->batch_deltas.empty()) {
     require(ws->batch_deltas.size() == ws->nb, "per-batch deltas do not match the prepared batches");
     ws->deltas_dev.reserve(ws->nb * 4, ws->graph->device);
@@ -1367,6 +1378,24 @@ int bfx_fetch_work_statistics(bfx_workspace* ws, bfx_device_work_statistics* sta
       stats->host_checks = ws->last_host_checks;
       stats->host_synchronizations = ws->last_host_checks;
       stats->controller_copies = ws->last_host_checks;
+    }
+  });
+}
+
+int bfx_fetch_round_trace(bfx_workspace* ws, uint32_t capacity, uint64_t* trace, uint32_t* rounds) {
+  return bfx::guarded([&] {
+    bfx::require(ws && rounds, "null argument");
+    bfx::require(ws->executed, "no executed batches");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    std::uint64_t w[8];
+    BFX_CUDA(cudaMemcpyAsync(w, ws->params.run->work, sizeof(w), cudaMemcpyDeviceToHost, ws->stream));
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    bfx::require(ws->round_trace.ptr != nullptr, "no traced run (instrumentation 2, persistent control)");
+    const std::uint32_t n = static_cast<std::uint32_t>(std::min<std::uint64_t>(w[7], bfx::kRoundTraceCap));
+    *rounds = n;
+    if (trace && capacity) {
+      const std::uint32_t m = std::min(n, capacity);
+      BFX_CUDA(cudaMemcpy(trace, ws->round_trace.ptr, size_t{m} * 16u, cudaMemcpyDeviceToHost));
     }
   });
 }

@@ -131,7 +131,12 @@ struct LaunchParams {
   u64 budget_ns;         // wall-clock budget of one relaxation launch; past it the launch stops (device_failure)
   const u32* engines;    // [nb] per-batch engine (autotuned launches) or null
   const u32* deltas;     // [nb] near/far threshold steps (float bits) or null (plain frontier)
+  u64* round_trace;      // instrumentation 2: per round {start %globaltimer, warp items}; null otherwise
+  u32 trace_cap;         // rounds the trace holds
+  u32 reserved2;
 };
+
+constexpr u32 kRoundTraceCap = 65536;
 
 __device__ __forceinline__ u32 engine_of(const LaunchParams& p, u32 b) {
   return p.engines ? p.engines[b] : p.engine;
@@ -251,5 +256,6 @@ struct bfx_workspace {
   bfx::DeviceBuffer deltas_dev;
   bfx::PinnedBuffer deltas_host;
   bfx::DeviceBuffer engines_dev;
+  bfx::DeviceBuffer round_trace;  // instrumentation 2 only
 };
 

@@ -337,6 +337,11 @@ int bfx_fetch_work_statistics(bfx_workspace *ws, bfx_device_work_statistics *sta
  * above, [7] rounds, [8..11] Jacobi pull {vertex-lane items, in-edge records,
  * relaxations, changes}, [12..15] zero. */
 int bfx_fetch_engine_work(bfx_workspace *ws, uint64_t counters[16]);
+/* Round trace of the most recent persistent run with instrumentation 2 (bfx
+ * extension): per round {%globaltimer ns at the round's start, warp items of
+ * the round}, up to 65,536 rounds; *rounds = rounds executed.  trace may be
+ * NULL to query the count. */
+int bfx_fetch_round_trace(bfx_workspace *ws, uint32_t capacity, uint64_t *trace, uint32_t *rounds);
 
 /* ---- plain per-query engine ----------------------------------------------
  * Replaces GpuSsspEngine::run(RouteQuery, GpuRunOptions) (gpu_api.hpp:203-211)
