@@ -337,3 +337,22 @@ def test_plain_query_after_autotune_ignores_batch_settings(gpu):
     assert all(s.stop_reason == bfx.STOP_CONVERGED for s in ws.fetch_statuses())
     ws.close()
     res.close()
+
+
+def test_round_trace_at_debug_instrumentation(gpu, c1):
+    """instrumentation 2 records one {start time, warp items} pair per round
+    of a persistent launch: as many rounds as the work counters report, start
+    times non-decreasing, every traced round with work."""
+    d = bfx.make_description(c1.layout, c1.queries, 8)
+    res = bfx.ResidentDeviceGraph.upload_once(c1.layout)
+    ws = bfx.Workspace(res)
+    ws.prepare([d])
+    ws.execute(bfx.GpuRunOptions(instrumentation=2))
+    st = ws.fetch_statuses()[0]
+    assert st.stop_reason == bfx.STOP_CONVERGED
+    tr = ws.round_trace()
+    assert tr.shape[0] == ws.work_counters()["rounds"] > 0
+    assert np.all(np.diff(tr[:, 0].astype(np.int64)) >= 0)
+    assert np.all(tr[:, 1] > 0)
+    ws.close()
+    res.close()
