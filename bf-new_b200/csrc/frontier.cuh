@@ -286,8 +286,9 @@ __device__ __forceinline__ void enqueue_claims(bool claim, u32 v, u32 cv, u32* c
   }
 }
 
-// Flat frontier round body: one warp item covers up to 32 queue entries.
-// Every thread loads one entry's header (queue word, pending lanes, row
+// Flat frontier round body: one warp item covers `epi` queue entries (a
+// power of two <= 32 chosen per round so that small frontiers spread over
+// more warps).  Every thread below epi loads one entry's header (queue word, pending lanes, row
 // bounds) -- 32 independent header chains per warp -- and the entries'
 // (lane, out-edge) pairs are flattened into one work list, entry-major, then
 // lane, then edge.  The warp walks the list 64 items per iteration, two per
@@ -370,14 +371,14 @@ __device__ __forceinline__ void stage_claims(bool claim, u32 v, u32 cv, u64* sta
 
 template <bool kCount, u32 kItems>
 __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
-                                              u32 rd, u32 widx, u32 tau_bits, u32 pile, Work& wk) {
+                                              u32 epi, u32 rd, u32 widx, u32 tau_bits, u32 pile, Work& wk) {
   __shared__ u64 s_stage[16][kStage];  // blocks of up to 512 threads
   u64* const stage = s_stage[threadIdx.x >> 5];
   u32 staged = 0u;
   const u32 lane = lane_id();
-  const u32 entry = item * 32u + lane;
+  const u32 entry = item * epi + lane;  // epi entries per item (a power of two <= 32)
   u32 v = 0u, cv = 0u, m = 0u, rb = 0u, deg = 0u;
-  if (entry < count) {
+  if (lane < epi && entry < count) {
     const u64 q = dev::ld_cg(B.queue_r + entry);
     v = static_cast<u32>(q);
     cv = static_cast<u32>(q >> 32);
