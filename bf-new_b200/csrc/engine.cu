@@ -1039,6 +1039,13 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
         ranges[i] = make_uint4(d.union_tiles[i], r.begin, r.end, r.lane_mask);
         roff[i + 1] = roff[i] + (r.end - r.begin);
       }
+      // Full-graph batch: every tile in order, each selected by every valid
+      // lane -- the frontier then needs no tile-table lookup per edge.
+      bool full = s.R == g.T;
+      for (std::uint32_t i = 0; full && i < s.R; ++i) {
+        full = ranges[i].x == i && ranges[i].y == roff[i] && ranges[i].w == d.valid_lane_mask;
+      }
+      B.full = full ? 1u : 0u;
       B.ranges = static_cast<const uint4*>(put(ranges.data(), size_t{s.R} * 16));
       B.range_off = static_cast<const std::uint32_t*>(put(roff.data(), (size_t{s.R} + 1) * 4));
       char* a = ab + arena_off[b];

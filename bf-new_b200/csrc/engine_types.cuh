@@ -44,7 +44,8 @@ struct DGraph {
 
 struct DBatch {
   u32 W, shift, valid, U;
-  u32 src_count, tgt_count, range_count, reserved;
+  u32 src_count, tgt_count, range_count;
+  u32 full;            // every tile selected by every valid lane, compact index == vertex id
   u64* dist[2];        // [U*W] labels (slot 1 only for Jacobi)
   u32* mask[2];        // [U] pending lane masks (frontier)
   u64* queue[2];       // [U] frontier entries {vertex, compact index << 32}

@@ -32,7 +32,7 @@ struct FrontierView {
   u32* fmask;
   u64* pile;      // near round: far pile being filled; split round: pile read
   u64* pile_out;  // split round: pile written
-  u32 shift, valid, U;
+  u32 shift, valid, U, full;
 };
 
 __device__ __forceinline__ FrontierView frontier_view(const DBatch& b, u32 rd, u32 pile, u32 pile_out) {
@@ -49,6 +49,7 @@ __device__ __forceinline__ FrontierView frontier_view(const DBatch& b, u32 rd, u
   v.shift = b.shift;
   v.valid = b.valid;
   v.U = b.U;
+  v.full = b.full;
   return v;
 }
 
@@ -440,7 +441,8 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
 #pragma unroll
     for (u32 u = 0; u < kItems; ++u) {
       if (it[u].live) {
-        dt[u] = B.tiles[rec[u].w];
+        // full-graph batch: compact index = vertex id, every lane admitted
+        dt[u] = B.full ? make_uint2(B.valid, 0u) : B.tiles[rec[u].w];
         cdst[u] = rec[u].x - dt[u].y;
         dstv[u] = rec[u].x;
       }
