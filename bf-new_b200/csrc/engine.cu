@@ -342,29 +342,14 @@ __device__ __forceinline__ u32 batch_exec(const LaunchParams& p, u32 b, u32 ridx
 
 __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
   const u32 ridx = r % 3u;
-  // Flat layout: entries per warp item for this round, a power of two <= 32
-  // chosen so that the round has at least two items per warp of the grid --
-  // a round with a small frontier is spread over more warps instead of
-  // leaving a few warps with long items.  Every block computes the same
-  // value from the same counts; it is kept in prefix[nb + 1].
-  u32 epi = 32u;
-  if (p.flat) {
-    block_prefix(prefix, p.nb, [&](u32 b) {
-      if (engine_of(p, b) != BFX_ENGINE_FRONTIER_PUSH) return 0u;
-      return min(dev::ld_cg(&p.ctl[b].count[ridx]), p.batches[b].U);
-    });
-    const u32 entries = prefix[p.nb];
-    const u32 warps = gridDim.x * (blockDim.x >> 5);
-    while (epi > 1u && entries / epi < 2u * warps) epi >>= 1;
-    __syncthreads();  // every thread has read the entry total before the next scan
-    if (threadIdx.x == 0) prefix[p.nb + 1] = epi;
-  }
   block_prefix(prefix, p.nb, [&](u32 b) {
     const DBatch& B = p.batches[b];
     if (engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH) {
       const DCtl& C = p.ctl[b];
       const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
-      if (n != 0u) return p.flat ? (n + epi - 1u) / epi : (B.W <= 8u ? (n + 3u) >> 2 : n);  // entries per warp item: epi, 4 or 1
+      if (n != 0u) {  // entries per warp item: flat_entries_per_item(n), 4 or 1
+        return p.flat ? (n + flat_entries_per_item(n) - 1u) / flat_entries_per_item(n) : (B.W <= 8u ? (n + 3u) >> 2 : n);
+      }
       const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
       return (f + 31u) >> 5;  // split round: 32 far entries per warp item
     }
@@ -407,7 +392,7 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
       const FrontierView V = frontier_view(B, r & 1u, g % 3u, (g + 1u) % 3u);
       if (n != 0u) {
         if (p.flat) {
-          frontier_flat<kCount, kItems>(p, V, C, item, n, prefix[p.nb + 1], r & 1u, widx, tau, g % 3u, wk);
+          frontier_flat<kCount, kItems>(p, V, C, item, n, flat_entries_per_item(n), r & 1u, widx, tau, g % 3u, wk);
         } else if (B.W <= 8u) {
           frontier_group<kCount, 8>(p, V, C, item, n, r & 1u, widx, tau, g % 3u, wk);
         } else {
@@ -1197,7 +1182,7 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
     p.engine = BFX_ENGINE_FRONTIER_PUSH;
   }
   const int block = static_cast<int>(o.block_size);
-  const size_t smem = (size_t{ws->nb} + 2) * 4;  // per-batch prefix + entries per flat warp item
+  const size_t smem = (size_t{ws->nb} + 1) * 4;
   std::uint64_t launches = 0;
   ws->last_host_checks = 0;
   BFX_CUDA(cudaEventRecord(ws->ev[0], ws->stream));

@@ -287,9 +287,17 @@ __device__ __forceinline__ void enqueue_claims(bool claim, u32 v, u32 cv, u32* c
   }
 }
 
-// Flat frontier round body: one warp item covers `epi` queue entries (a
-// power of two <= 32 chosen per round so that small frontiers spread over
-// more warps).  Every thread below epi loads one entry's header (queue word, pending lanes, row
+// Entries per flat warp item for a batch frontier of n entries: 32 from 2,048
+// entries up, otherwise the power of two nearest below n / 64 (at least 1),
+// so a small frontier is spread over up to 64 warps instead of a few.
+__device__ __forceinline__ u32 flat_entries_per_item(u32 n) {
+  const u32 e = n >> 6;
+  if (e >= 32u) return 32u;
+  return e == 0u ? 1u : 1u << (31u - __clz(e));
+}
+
+// Flat frontier round body: one warp item covers `epi` queue entries
+// (flat_entries_per_item of the batch's frontier size).  Every thread below epi loads one entry's header (queue word, pending lanes, row
 // bounds) -- 32 independent header chains per warp -- and the entries'
 // (lane, out-edge) pairs are flattened into one work list, entry-major, then
 // lane, then edge.  The warp walks the list 64 items per iteration, two per
