@@ -182,6 +182,8 @@ def main():
                     help="register budget of the persistent kernel")
     ap.add_argument("--items", type=int, default=2, choices=[2, 3, 4],
                     help="flat layout: work items per thread per iteration")
+    ap.add_argument("--policy", default=None,
+                    help="planner policy jaccard_num,jaccard_den,inflation_num,inflation_den (default per workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=None)
     args = ap.parse_args()
@@ -232,6 +234,9 @@ def main():
         policy = bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True)
         workload_desc = ("c5: 4,096 regional queries (box side U[2,16] tiles) + 16 full-graph sources on 256x256 "
                          "tiles x 256 nodes, 16,777,216 V / 167,772,160 E, uint costs U[1,255]")
+    if args.policy:
+        jn, jd, inn, ind = (int(x) for x in args.policy.split(","))
+        policy = bfx.BatchPlannerPolicy(32, jn, jd, inn, ind, narrow_lanes=True)
     t1 = time.time()
     plan = bfx.make_overlapping_batch_plan(layout, queries, policy)
     descs = plan.descriptions()
@@ -382,6 +387,9 @@ def main():
         "config": {"workload": workload_desc,
                    "queries_per_gpu": len(queries), "batches": plan.batch_count,
                    "lane_widths": sorted({d.lane_width for d in descs}), "engine": args.engine,
+                   "planner_policy": [policy.minimum_jaccard_numerator, policy.minimum_jaccard_denominator,
+                                      policy.maximum_union_inflation_numerator,
+                                      policy.maximum_union_inflation_denominator],
                    "frontier_layout": args.frontier, "registers": args.regs, "flat_items": args.items,
                    "engines_chosen": None if engines_chosen is None else
                    {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
