@@ -184,6 +184,8 @@ def main():
                     help="flat layout: work items per thread per iteration")
     ap.add_argument("--policy", default=None,
                     help="planner policy jaccard_num,jaccard_den,inflation_num,inflation_den (default per workload)")
+    ap.add_argument("--amin", type=int, default=0, choices=[0, 1],
+                    help="flat frontier: 1 = one returning min per relaxation")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=None)
     args = ap.parse_args()
@@ -251,6 +253,7 @@ def main():
     ws.set_frontier_layout(bfx.FRONTIER_FLAT if args.frontier == "flat" else bfx.FRONTIER_GROUPS)
     ws.set_register_budget(args.regs)
     ws.set_flat_items(args.items)
+    ws.set_relax_atomic(args.amin)
     engine_id = {"auto": bfx.ENGINE_AUTO, "frontier": bfx.ENGINE_FRONTIER_PUSH, "jacobi": bfx.ENGINE_JACOBI_PULL,
                  "dense": bfx.ENGINE_DENSE_CHAOTIC_PUSH}[args.engine]
     engines_chosen = None
@@ -390,7 +393,7 @@ def main():
                    "planner_policy": [policy.minimum_jaccard_numerator, policy.minimum_jaccard_denominator,
                                       policy.maximum_union_inflation_numerator,
                                       policy.maximum_union_inflation_denominator],
-                   "frontier_layout": args.frontier, "registers": args.regs, "flat_items": args.items,
+                   "frontier_layout": args.frontier, "registers": args.regs, "flat_items": args.items, "returning_min": args.amin,
                    "engines_chosen": None if engines_chosen is None else
                    {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
                    "frontier_steps_chosen": None if engines_chosen is None else

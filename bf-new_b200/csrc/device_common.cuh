@@ -39,6 +39,13 @@ __device__ __forceinline__ void red_min(u64* p, u64 v) {
   asm volatile("red.relaxed.gpu.global.min.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// Returning 64-bit min at L2: the label before the reduction.
+__device__ __forceinline__ u64 atom_min(u64* p, u64 v) {
+  u64 old;
+  asm volatile("atom.relaxed.gpu.global.min.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+
 __device__ __forceinline__ u64 global_ns() {
   u64 t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

@@ -1154,6 +1154,7 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   p.flat = ws->frontier_layout == BFX_FRONTIER_FLAT ? 1u : 0u;
   p.round_trace = nullptr;
   p.trace_cap = 0u;
+  p.amin = ws->relax_atomic;
   if (o.instrumentation == 2u && o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
     ws->round_trace.reserve(size_t{kRoundTraceCap} * 16u, ws->graph->device);
     p.round_trace = static_cast<u64*>(ws->round_trace.ptr);
@@ -1282,6 +1283,14 @@ int bfx_set_register_budget(bfx_workspace* ws, uint32_t registers) {
     bfx::require(ws != nullptr, "null argument");
     bfx::require(registers == 40u || registers == 64u, "register budget must be 40 or 64");
     ws->register_budget = registers;
+  });
+}
+
+int bfx_set_relax_atomic(bfx_workspace* ws, uint32_t mode) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null argument");
+    bfx::require(mode <= 1u, "relaxation mode must be 0 or 1");
+    ws->relax_atomic = mode;
   });
 }
 

@@ -134,7 +134,7 @@ struct LaunchParams {
   const u32* deltas;     // [nb] near/far threshold steps (float bits) or null (plain frontier)
   u64* round_trace;      // instrumentation 2: per round {start %globaltimer, warp items}; null otherwise
   u32 trace_cap;         // rounds the trace holds
-  u32 reserved2;
+  u32 amin;              // flat frontier: 1 = returning min per relaxation, 0 = pre-read + min on success
 };
 
 constexpr u32 kRoundTraceCap = 65536;
@@ -252,6 +252,7 @@ struct bfx_workspace {
   std::vector<std::uint32_t> batch_engines;  // per-batch engine for BFX_ENGINE_AUTO launches
   std::vector<float> batch_deltas;           // per-batch near/far steps (empty: plain frontier)
   std::uint32_t frontier_layout = 1;         // BFX_FRONTIER_FLAT (default) / BFX_FRONTIER_GROUPS
+  std::uint32_t relax_atomic = 0;            // flat frontier relaxation: 0 pre-read + min, 1 returning min
   std::uint32_t flat_items = 2;              // flat layout: work items per thread per iteration (2..4)
   std::uint32_t register_budget = 64;        // persistent kernel: 64 (default) or 40 registers per thread
   bfx::DeviceBuffer deltas_dev;

@@ -462,7 +462,9 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
       relax[u] = it[u].live && ((dt[u].x >> it[u].ql) & 1u) && src[u] != dev::kInfBits;
       if (relax[u]) {
         cand[u] = dev::candidate(src[u], rec[u].y, rec[u].z);
-        cur[u] = dev::ld_cg(B.dist + ((static_cast<u64>(cdst[u]) << B.shift) + it[u].ql));
+        u64* const target = B.dist + ((static_cast<u64>(cdst[u]) << B.shift) + it[u].ql);
+        // returning min (one L2 read-modify-write) or pre-read + min on success
+        cur[u] = p.amin ? dev::atom_min(target, cand[u]) : dev::ld_cg(target);
       }
     }
 #pragma unroll
@@ -470,7 +472,7 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
       if (relax[u]) {
         if (kCount) wk.c[3] += 1;
         if (cand[u] < cur[u]) {
-          dev::red_min(B.dist + ((static_cast<u64>(cdst[u]) << B.shift) + it[u].ql), cand[u]);
+          if (!p.amin) dev::red_min(B.dist + ((static_cast<u64>(cdst[u]) << B.shift) + it[u].ql), cand[u]);
           if (dev::hi(cand[u]) < dev::hi(cur[u])) {
             if (dev::hi(cand[u]) < tau_bits) {
               bits[u] = 1u << it[u].ql;

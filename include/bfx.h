@@ -310,6 +310,11 @@ int bfx_set_register_budget(bfx_workspace *ws, uint32_t registers);
  * independent memory chains against more register spills.  Other
  * configurations use 2. */
 int bfx_set_flat_items(bfx_workspace *ws, uint32_t items);
+/* Flat layout: how a relaxation updates the target label -- 0 (default)
+ * pre-reads it and issues a non-returning 64-bit min only for a smaller
+ * candidate; 1 issues one returning 64-bit min per relaxation and takes the
+ * returned label as the comparison. */
+int bfx_set_relax_atomic(bfx_workspace *ws, uint32_t mode);
 /* {mean edge weight, edge count} of the workspace's resident graph. */
 int bfx_workspace_graph_stats(bfx_workspace *ws, double out[2]);
 
