@@ -973,15 +973,18 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
     const size_t o_up = bfx::align256(o_ctrl + count * sizeof(bfx_device_controller));
     const size_t meta_total = o_up + up_bytes;
     // Arena: per batch labels (2 slots reserved so one prepare serves every
-    // engine), masks, queues, c2g, tile table.
+    // engine), masks, queues, c2g; then the tile tables of all batches in one
+    // contiguous block, cleared by a single memset.
     std::vector<size_t> arena_off(count);
     size_t arena_total = 0;
     for (std::uint32_t b = 0; b < count; ++b) {
       arena_off[b] = arena_total;
       const size_t U = sz[b].U;
-      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 4 + bfx::align256(U * 8) * 5 +
-                     bfx::align256(size_t{g.T} * 8);
+      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 4 + bfx::align256(U * 8) * 5;
     }
+    const size_t tiles_off = arena_total;
+    const size_t tile_table_bytes = bfx::align256(size_t{g.T} * 8);
+    arena_total += tile_table_bytes * count;
     const bool grew = meta_total > ws->meta.bytes || arena_total > ws->arena.bytes;
     ws->meta.reserve(meta_total, ws->graph->device);
     ws->arena.reserve(arena_total, ws->graph->device);
@@ -1055,7 +1058,7 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
         B.fpile[k] = reinterpret_cast<bfx::u64*>(a);
         a += bfx::align256(U * 8);
       }
-      B.tiles = reinterpret_cast<uint2*>(a);
+      B.tiles = reinterpret_cast<uint2*>(ab + tiles_off + tile_table_bytes * b);
       ubase[b] = static_cast<std::uint32_t>(usum);
       sbase[b] = static_cast<std::uint32_t>(ssum);
       usum += U;
@@ -1068,9 +1071,7 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
     bfx::upload(db, hb, meta_total, ws->stream);
     ws->last_h2d = meta_total;
     // Tile tables must read 0 outside the union.
-    for (std::uint32_t b = 0; b < count; ++b) {
-      BFX_CUDA(cudaMemsetAsync(ws->batches[b].tiles, 0, size_t{g.T} * 8, ws->stream));
-    }
+    BFX_CUDA(cudaMemsetAsync(ab + tiles_off, 0, tile_table_bytes * count, ws->stream));
     ws->nb = count;
     ws->src_total = ssum;
     ws->params = bfx::LaunchParams{};
