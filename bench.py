@@ -409,7 +409,9 @@ def main():
         "plain_per_query": {"value": plain_qps, "unit": "queries/s", "sample": plain_sampled,
                             "batched_speedup": value / world / plain_qps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_src, "kernel": "persistent_kernel<false> (frontier)",
+                     "traffic": traffic, "peak_source": peak_src, "kernel": "persistent_kernel<0, %d, %d> (%s frontier%s)" % (
+                         2 if args.regs == 64 else 3, args.items if args.regs == 64 else 2, args.frontier,
+                         ", mixed engines" if engines_chosen and any(e != 2 for e in engines_chosen) else ""),
                      "kernel_ms": kernel_avg, "execute_ms": float(np.mean(execute_ms)),
                      "algorithmic_bytes_per_launch": alg_bytes, "work": work, "engine_work": engine_work},
         "clocks": clocks.summary(),
