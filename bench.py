@@ -176,7 +176,7 @@ def main():
     ap.add_argument("--impl", default="bfx", choices=["bfx", "reference"])
     ap.add_argument("--engine", default="auto", choices=["auto", "frontier", "jacobi", "dense"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"])
-    ap.add_argument("--frontier", default="flat", choices=["groups", "flat"],
+    ap.add_argument("--frontier", default="flat", choices=["groups", "flat", "chunked"],
                     help="frontier-push work layout (sub-warp groups or flat work list)")
     ap.add_argument("--regs", type=int, default=64, choices=[40, 64],
                     help="register budget of the persistent kernel")
@@ -250,7 +250,8 @@ def main():
     device = local if world > 1 else 0
     resident = bfx.ResidentDeviceGraph.upload_once(layout, device)
     ws = bfx.Workspace(resident)
-    ws.set_frontier_layout(bfx.FRONTIER_FLAT if args.frontier == "flat" else bfx.FRONTIER_GROUPS)
+    ws.set_frontier_layout({"flat": bfx.FRONTIER_FLAT, "groups": bfx.FRONTIER_GROUPS,
+                            "chunked": bfx.FRONTIER_CHUNKED}[args.frontier])
     ws.set_register_budget(args.regs)
     ws.set_flat_items(args.items)
     ws.set_relax_atomic(args.amin)

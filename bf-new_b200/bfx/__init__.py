@@ -34,7 +34,7 @@ P = C.POINTER
 ENGINE_JACOBI_PULL, ENGINE_DENSE_CHAOTIC_PUSH, ENGINE_FRONTIER_PUSH = 0, 1, 2
 ENGINE_AUTO = 0xFFFFFFFF
 CONTROL_PERSISTENT, CONTROL_CHUNKED, CONTROL_PER_ROUND = 0, 1, 2
-FRONTIER_GROUPS, FRONTIER_FLAT = 0, 1
+FRONTIER_GROUPS, FRONTIER_FLAT, FRONTIER_CHUNKED = 0, 1, 2
 STOP_NONE, STOP_CONVERGED, STOP_MAXIMUM_ROUNDS, STOP_QUEUE_OVERFLOW, STOP_INVALID, STOP_FAILURE = range(6)
 INF_BITS = 0x7F800000
 NO_EDGE = 0xFFFFFFFF

@@ -39,6 +39,10 @@ __device__ __forceinline__ void red_min(u64* p, u64 v) {
   asm volatile("red.relaxed.gpu.global.min.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+__device__ __forceinline__ void red_or(u32* p, u32 v) {
+  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Returning 64-bit min at L2: the label before the reduction.
 __device__ __forceinline__ u64 atom_min(u64* p, u64 v) {
   u64 old;

@@ -150,6 +150,10 @@ __global__ void init_kernel(LaunchParams p) {
     B.mask[0][cv] = 0u;
     B.mask[1][cv] = 0u;
     B.fmask[cv] = 0u;
+    if (p.flat == 2u && (cv & 1023u) == 0u) {  // chunk bitmap words, one per 1,024 vertices
+      B.cmask[0][cv >> 10] = 0u;
+      B.cmask[1][cv >> 10] = 0u;
+    }
     for (u32 l = 0; l < B.W; ++l) {
       B.dist[0][(static_cast<u64>(cv) << B.shift) + l] = dev::kUnreached;
       if (engine_of(p, b) == BFX_ENGINE_JACOBI_PULL) B.dist[1][(static_cast<u64>(cv) << B.shift) + l] = dev::kUnreached;
@@ -212,7 +216,21 @@ __global__ void seed_kernel(LaunchParams p, const u32* src_base) {
     B.dist[0][(static_cast<u64>(cv) << B.shift) + lane] = dev::kSourceWord;
     const u32 eng = engine_of(p, b);
     if (eng == BFX_ENGINE_JACOBI_PULL) B.dist[1][(static_cast<u64>(cv) << B.shift) + lane] = dev::kSourceWord;
-    if (eng == BFX_ENGINE_FRONTIER_PUSH) {
+    if (eng == BFX_ENGINE_FRONTIER_PUSH && p.flat == 2u) {
+      // chunked frontier: pending lane, then the chunk's bit; the thread that
+      // sets the bit queues the chunk
+      atomicOr(&B.mask[0][cv], 1u << lane);
+      const u32 chunk = cv >> 5;
+      const u32 bit = 1u << (chunk & 31u);
+      if ((atomicOr(&B.cmask[0][chunk >> 5], bit) & bit) == 0u) {
+        const u32 slot = atomicAdd(&p.ctl[b].count[0], 1u);
+        if (slot < B.U) {
+          B.queue[0][slot] = chunk;
+        } else {
+          atomicOr(&p.ctl[b].error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
+        }
+      }
+    } else if (eng == BFX_ENGINE_FRONTIER_PUSH) {
       const u32 old = atomicOr(&B.mask[0][cv], 1u << lane);
       if (old == 0u) {
         const u32 slot = atomicAdd(&p.ctl[b].count[0], 1u);
@@ -347,7 +365,8 @@ __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
     if (engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH) {
       const DCtl& C = p.ctl[b];
       const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
-      if (n != 0u) {  // entries per warp item: flat_entries_per_item(n), 4 or 1
+      if (n != 0u) {  // warp items: one chunk (chunked), flat_entries_per_item(n) entries (flat), 4 or 1 entries
+        if (p.flat == 2u) return n;
         return p.flat ? (n + flat_entries_per_item(n) - 1u) / flat_entries_per_item(n) : (B.W <= 8u ? (n + 3u) >> 2 : n);
       }
       const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
@@ -358,7 +377,9 @@ __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
   return prefix[p.nb];
 }
 
-template <bool kCount, u32 kItems>
+// kChunked: compiled for the chunked frontier layout only (a separate
+// kernel instantiation, so the other layouts keep their register budget).
+template <bool kCount, u32 kItems, bool kChunked>
 __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work& wk) {
   const u32 ridx = r % 3u, widx = (r + 1u) % 3u;
   const u32 total = prefix[p.nb];
@@ -391,15 +412,19 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
       tau_next = __shfl_sync(0xFFFFFFFFu, tau_next, 0);
       const FrontierView V = frontier_view(B, r & 1u, g % 3u, (g + 1u) % 3u);
       if (n != 0u) {
-        if (p.flat) {
-          frontier_flat<kCount, kItems>(p, V, C, item, n, flat_entries_per_item(n), r & 1u, widx, tau, g % 3u, wk);
+        if (kChunked) {
+          frontier_flat<kCount, kItems, true>(p, V, C, item, n, 32u, r & 1u, widx, tau, g % 3u, wk);
+        } else if (p.flat) {
+          frontier_flat<kCount, kItems, false>(p, V, C, item, n, flat_entries_per_item(n), r & 1u, widx, tau, g % 3u, wk);
         } else if (B.W <= 8u) {
           frontier_group<kCount, 8>(p, V, C, item, n, r & 1u, widx, tau, g % 3u, wk);
         } else {
           frontier_group<kCount, 32>(p, V, C, item, n, r & 1u, widx, tau, g % 3u, wk);
         }
+      } else if (kChunked) {
+        split_group<kCount, true>(p, V, C, item, f, r & 1u, widx, tau_next, g % 3u, (g + 1u) % 3u, wk);
       } else {
-        split_group<kCount>(p, V, C, item, f, r & 1u, widx, tau_next, g % 3u, (g + 1u) % 3u, wk);
+        split_group<kCount, false>(p, V, C, item, f, r & 1u, widx, tau_next, g % 3u, (g + 1u) % 3u, wk);
       }
     } else if (eng == BFX_ENGINE_JACOBI_PULL) {
       jacobi_item<kCount>(p, B, C, item, r, widx, wk);
@@ -456,7 +481,7 @@ __device__ void flush_work(const LaunchParams& p, Work& wk) {
 // for: 3 -> 40 registers per thread (48 warps per SM), 2 -> 64 registers
 // (32 warps per SM; no spills in the group layout, a few in the flat one).
 // kItems = flat-layout work items per thread per iteration.
-template <bool kCount, int kMinBlocks, u32 kItems>
+template <bool kCount, int kMinBlocks, u32 kItems, bool kChunked = false>
 __global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParams p) {
   extern __shared__ u32 prefix[];
   const u32 nblocks = gridDim.x;
@@ -472,7 +497,7 @@ __global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParam
       p.round_trace[2u * r] = dev::global_ns();
       p.round_trace[2u * r + 1u] = total;
     }
-    round_body<kCount, kItems>(p, r, prefix, wk);
+    round_body<kCount, kItems, kChunked>(p, r, prefix, wk);
     // Past the launch budget block 0 raises the barrier's abort before it
     // arrives, so every block leaves after this round.
     if (blockIdx.x == 0 && threadIdx.x == 0 && dev::global_ns() - t0 > p.budget_ns) {
@@ -492,7 +517,7 @@ __global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParam
 }
 
 // Host-poll modes: one round per launch over a fixed grid ...
-template <bool kCount>
+template <bool kCount, bool kChunked = false>
 __global__ void __launch_bounds__(512, 3) round_kernel(LaunchParams p) {
   extern __shared__ u32 prefix[];
   if (dev::ld_cg(&p.run->done) != 0u) return;
@@ -501,7 +526,7 @@ __global__ void __launch_bounds__(512, 3) round_kernel(LaunchParams p) {
   if (total == 0u) return;
   Work wk;
   wk.zero();
-  round_body<kCount, 2>(p, r, prefix, wk);
+  round_body<kCount, 2, kChunked>(p, r, prefix, wk);
   if (kCount) flush_work(p, wk);
 }
 
@@ -980,7 +1005,8 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
     for (std::uint32_t b = 0; b < count; ++b) {
       arena_off[b] = arena_total;
       const size_t U = sz[b].U;
-      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 4 + bfx::align256(U * 8) * 5;
+      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 4 + bfx::align256(U * 8) * 5 +
+                     bfx::align256((U + 1023) / 1024 * 4) * 2;
     }
     const size_t tiles_off = arena_total;
     const size_t tile_table_bytes = bfx::align256(size_t{g.T} * 8);
@@ -1058,6 +1084,10 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
         B.fpile[k] = reinterpret_cast<bfx::u64*>(a);
         a += bfx::align256(U * 8);
       }
+      for (int k = 0; k < 2; ++k) {
+        B.cmask[k] = reinterpret_cast<std::uint32_t*>(a);
+        a += bfx::align256((U + 1023) / 1024 * 4);
+      }
       B.tiles = reinterpret_cast<uint2*>(ab + tiles_off + tile_table_bytes * b);
       ubase[b] = static_cast<std::uint32_t>(usum);
       sbase[b] = static_cast<std::uint32_t>(ssum);
@@ -1123,8 +1153,13 @@ int grid_blocks(bfx_workspace* ws, const void* kernel, int block, size_t smem, c
 }
 
 // Persistent kernel instantiation: 64 registers (two 512-thread blocks per
-// SM) with 2, 3 or 4 flat work items per thread, or 40 registers with 2.
-const void* persistent_entry(bool count, bool wide, std::uint32_t items) {
+// SM) with 2, 3 or 4 flat work items per thread, or 40 registers with 2;
+// the chunked layout has its own (64 registers, 2 items).
+const void* persistent_entry(bool count, bool wide, std::uint32_t items, bool chunked) {
+  if (chunked) {
+    return count ? reinterpret_cast<const void*>(persistent_kernel<true, 2, 2, true>)
+                 : reinterpret_cast<const void*>(persistent_kernel<false, 2, 2, true>);
+  }
   if (!wide) {
     return count ? reinterpret_cast<const void*>(persistent_kernel<true, 3, 2>)
                  : reinterpret_cast<const void*>(persistent_kernel<false, 3, 2>);
@@ -1152,7 +1187,7 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   p.budget_ns = kLaunchBudgetNs;
   p.engines = nullptr;
   p.deltas = nullptr;
-  p.flat = ws->frontier_layout == BFX_FRONTIER_FLAT ? 1u : 0u;
+  p.flat = ws->frontier_layout == BFX_FRONTIER_FLAT ? 1u : (ws->frontier_layout == BFX_FRONTIER_CHUNKED ? 2u : 0u);
   p.round_trace = nullptr;
   p.trace_cap = 0u;
   p.amin = ws->relax_atomic;
@@ -1200,15 +1235,20 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   BFX_CUDA(cudaGetLastError());
   BFX_CUDA(cudaEventRecord(ws->ev[1], ws->stream));
   if (o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
-    const void* kfn = persistent_entry(o.instrumentation != 0u, ws->register_budget == 64u, ws->flat_items);
+    const void* kfn = persistent_entry(o.instrumentation != 0u, ws->register_budget == 64u, ws->flat_items,
+                                       p.flat == 2u);
     const int grid = grid_blocks(ws, kfn, block, smem, o);
     void* args[] = {&p};
     BFX_CUDA(cudaLaunchCooperativeKernel(kfn, grid, block, args, smem, ws->stream));
     ++launches;
   } else {
     const std::uint32_t K = o.control_mode == BFX_CONTROL_PER_ROUND_HOST_POLL ? 1u : o.rounds_per_chunk;
-    const void* kfn = o.instrumentation ? reinterpret_cast<const void*>(round_kernel<true>)
-                                        : reinterpret_cast<const void*>(round_kernel<false>);
+    const bool chunked = p.flat == 2u;
+    const void* kfn = o.instrumentation
+                          ? (chunked ? reinterpret_cast<const void*>(round_kernel<true, true>)
+                                     : reinterpret_cast<const void*>(round_kernel<true, false>))
+                          : (chunked ? reinterpret_cast<const void*>(round_kernel<false, true>)
+                                     : reinterpret_cast<const void*>(round_kernel<false, false>));
     const int grid = grid_blocks(ws, kfn, block, smem, o);
     start_kernel<<<1, 1024, smem, ws->stream>>>(p);
     ++launches;
@@ -1224,9 +1264,17 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
       BFX_CUDA(cudaStreamBeginCapture(ws->stream, cudaStreamCaptureModeThreadLocal));
       for (std::uint32_t k = 0; k < K; ++k) {
         if (o.instrumentation) {
-          round_kernel<true><<<grid, block, smem, ws->stream>>>(p);
+          if (chunked) {
+            round_kernel<true, true><<<grid, block, smem, ws->stream>>>(p);
+          } else {
+            round_kernel<true, false><<<grid, block, smem, ws->stream>>>(p);
+          }
         } else {
-          round_kernel<false><<<grid, block, smem, ws->stream>>>(p);
+          if (chunked) {
+            round_kernel<false, true><<<grid, block, smem, ws->stream>>>(p);
+          } else {
+            round_kernel<false, false><<<grid, block, smem, ws->stream>>>(p);
+          }
         }
         advance_kernel<<<1, 1024, smem, ws->stream>>>(p);
       }
@@ -1306,7 +1354,8 @@ int bfx_set_flat_items(bfx_workspace* ws, uint32_t items) {
 int bfx_set_frontier_layout(bfx_workspace* ws, uint32_t layout) {
   return bfx::guarded([&] {
     bfx::require(ws != nullptr, "null argument");
-    bfx::require(layout == BFX_FRONTIER_GROUPS || layout == BFX_FRONTIER_FLAT, "invalid frontier layout");
+    bfx::require(layout == BFX_FRONTIER_GROUPS || layout == BFX_FRONTIER_FLAT || layout == BFX_FRONTIER_CHUNKED,
+                 "invalid frontier layout");
     ws->frontier_layout = layout;
   });
 }

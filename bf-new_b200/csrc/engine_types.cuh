@@ -59,6 +59,7 @@ struct DBatch {
   const u32* range_off;   // [R+1] compact offsets
   u32* fmask;             // [U] far lanes (near/far frontier)
   u64* fpile[3];          // [U] far piles, rotating by far generation
+  u32* cmask[2];          // [ceil(U/1024)] chunk bitmaps (chunked frontier): bit c = chunk c pending
 };
 
 struct DCtl {
@@ -127,7 +128,7 @@ struct LaunchParams {
   u32 nb;
   u32 engine;            // engine of every batch when `engines` is null
   u32 per_lane;
-  u32 flat;              // frontier layout: 0 sub-warp groups, 1 flat work list
+  u32 flat;              // frontier layout: 0 sub-warp groups, 1 flat work list, 2 chunked flat work list
   u64 max_rounds;
   u64 budget_ns;         // wall-clock budget of one relaxation launch; past it the launch stops (device_failure)
   const u32* engines;    // [nb] per-batch engine (autotuned launches) or null

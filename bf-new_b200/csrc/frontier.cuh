@@ -32,6 +32,9 @@ struct FrontierView {
   u32* fmask;
   u64* pile;      // near round: far pile being filled; split round: pile read
   u64* pile_out;  // split round: pile written
+  const u32* c2g;  // compact index -> vertex id (chunked layout)
+  u32* cmask_r;    // chunk bitmaps (chunked layout): read and write slots
+  u32* cmask_w;
   u32 shift, valid, U, full;
 };
 
@@ -46,6 +49,9 @@ __device__ __forceinline__ FrontierView frontier_view(const DBatch& b, u32 rd, u
   v.fmask = b.fmask;
   v.pile = b.fpile[pile];
   v.pile_out = b.fpile[pile_out];
+  v.c2g = b.c2g;
+  v.cmask_r = b.cmask[rd];
+  v.cmask_w = b.cmask[rd ^ 1u];
   v.shift = b.shift;
   v.valid = b.valid;
   v.U = b.U;
@@ -201,7 +207,7 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const Fron
 // pile.  One thread per far entry; claims are warp-aggregated.  The batch
 // runs no near round in the same round, so the far masks it reads are
 // stable and are cleared with plain stores.
-template <bool kCount>
+template <bool kCount, bool kChunked>
 __device__ __forceinline__ void split_group(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
                                             u32 rd, u32 widx, u32 tau_next, u32 pile_in, u32 pile_out, Work& wk) {
   const u32 lane = lane_id();
@@ -233,7 +239,18 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const Frontie
   // far lanes stay parked (next pile); near lanes join the next round
   bool fclaim = false, claim = false;
   if (far != 0u) fclaim = atomicOr(B.fmask + cv, far) == 0u;
-  if (near != 0u) claim = atomicOr(B.mask_w + cv, near) == 0u;
+  u32 qword = v;  // queue word: the vertex, or its chunk (chunked layout)
+  if (near != 0u) {
+    if (kChunked) {
+      dev::red_or(B.mask_w + cv, near);
+      const u32 chunk = cv >> 5;
+      const u32 bit = 1u << (chunk & 31u);
+      claim = (atomicOr(B.cmask_w + (chunk >> 5), bit) & bit) == 0u;
+      qword = chunk;
+    } else {
+      claim = atomicOr(B.mask_w + cv, near) == 0u;
+    }
+  }
   fd = __reduce_min_sync(0xFFFFFFFFu, fd);
   if (lane == 0u && fd != 0xFFFFFFFFu) atomicMin(&C.fmin[pile_out], fd);
   const u32 fm = __ballot_sync(0xFFFFFFFFu, fclaim);
@@ -257,8 +274,11 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const Frontie
     if (claim) {
       if (kCount) wk.c[4] += 1;
       const u32 at = pos + __popc(cm & ((1u << lane) - 1u));
-      if (at < B.U) B.queue_w[at] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
-      else atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
+      if (at < B.U) {
+        B.queue_w[at] = kChunked ? static_cast<u64>(qword) : static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
+      } else {
+        atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
+      }
     }
   }
 }
@@ -378,7 +398,11 @@ __device__ __forceinline__ void stage_claims(bool claim, u32 v, u32 cv, u64* sta
   n = 0u;
 }
 
-template <bool kCount, u32 kItems>
+// kChunked: the item is one queued 32-vertex chunk (compact indices
+// 32 c .. 32 c + 31) instead of `epi` queued vertices; successes set the
+// pending lane with a non-returning OR and claim the target's chunk through
+// the chunk bitmap.
+template <bool kCount, u32 kItems, bool kChunked>
 __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
                                               u32 epi, u32 rd, u32 widx, u32 tau_bits, u32 pile, Work& wk) {
   __shared__ u64 s_stage[16][kStage];  // blocks of up to 512 threads
@@ -387,7 +411,29 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
   const u32 lane = lane_id();
   const u32 entry = item * epi + lane;  // epi entries per item (a power of two <= 32)
   u32 v = 0u, cv = 0u, m = 0u, rb = 0u, deg = 0u;
-  if (lane < epi && entry < count) {
+  if (kChunked) {
+    const u32 chunk = static_cast<u32>(dev::ld_cg(B.queue_r + item));
+    if (chunk < (B.U + 31u) >> 5) {
+      cv = (chunk << 5) + lane;
+      if (cv < B.U) {
+        m = dev::ld_cg(B.mask_r + cv) & B.valid;
+        v = __ldg(B.c2g + cv);
+        if (m != 0u) {
+          rb = __ldg(p.g.csr_off + v);
+          deg = __ldg(p.g.csr_off + v + 1u) - rb;
+          B.mask_r[cv] = 0u;
+          if (kCount) {
+            wk.c[0] += 1;
+            wk.c[1] += deg;
+            wk.c[2] += __popc(m);
+          }
+        }
+      }
+      if (lane == 0u) atomicAnd(B.cmask_r + (chunk >> 5), ~(1u << (chunk & 31u)));
+    } else if (lane == 0u) {
+      atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
+    }
+  } else if (lane < epi && entry < count) {
     const u64 q = dev::ld_cg(B.queue_r + entry);
     v = static_cast<u32>(q);
     cv = static_cast<u32>(q >> 32);
@@ -501,9 +547,19 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
     // next iteration (or after the loop)
 #pragma unroll
     for (u32 u = 0; u < kItems; ++u) {
-      p_old[u] = bits[u] != 0u ? atomicOr(B.mask_w + cdst[u], bits[u]) : 1u;
-      p_v[u] = dstv[u];
-      p_cv[u] = cdst[u];
+      if (kChunked) {
+        // pending lane with a non-returning OR; the chunk bit's OR claims
+        const u32 chunk = cdst[u] >> 5;
+        const u32 bit = 1u << (chunk & 31u);
+        if (bits[u] != 0u) dev::red_or(B.mask_w + cdst[u], bits[u]);
+        p_old[u] = bits[u] != 0u ? (atomicOr(B.cmask_w + (chunk >> 5), bit) & bit) : 1u;
+        p_v[u] = chunk;
+        p_cv[u] = 0u;
+      } else {
+        p_old[u] = bits[u] != 0u ? atomicOr(B.mask_w + cdst[u], bits[u]) : 1u;
+        p_v[u] = dstv[u];
+        p_cv[u] = cdst[u];
+      }
     }
   }
 #pragma unroll

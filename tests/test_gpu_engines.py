@@ -283,7 +283,8 @@ def test_autotuner_with_near_far_candidates(gpu):
 
 
 @pytest.mark.parametrize("regs,items,amin", [(40, 2, 0), (64, 2, 0), (64, 3, 0), (64, 4, 0), (64, 2, 1)])
-@pytest.mark.parametrize("layout_kind", [bfx.FRONTIER_FLAT, bfx.FRONTIER_GROUPS], ids=["flat", "groups"])
+@pytest.mark.parametrize("layout_kind", [bfx.FRONTIER_FLAT, bfx.FRONTIER_GROUPS, bfx.FRONTIER_CHUNKED],
+                         ids=["flat", "groups", "chunked"])
 @pytest.mark.parametrize("step", [None, 3.0])
 @pytest.mark.parametrize("control", [bfx.CONTROL_PERSISTENT, bfx.CONTROL_PER_ROUND], ids=["persistent", "per_round"])
 def test_flat_frontier_layout_bit_exact(gpu, c1, step, control, layout_kind, regs, items, amin):
