@@ -176,7 +176,7 @@ def main():
     ap.add_argument("--impl", default="bfx", choices=["bfx", "reference"])
     ap.add_argument("--engine", default="auto", choices=["auto", "frontier", "jacobi", "dense"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"])
-    ap.add_argument("--frontier", default="flat", choices=["groups", "flat", "chunked"],
+    ap.add_argument("--frontier", default="chunked", choices=["groups", "flat", "chunked"],
                     help="frontier-push work layout (sub-warp groups or flat work list)")
     ap.add_argument("--regs", type=int, default=64, choices=[40, 64],
                     help="register budget of the persistent kernel")

@@ -252,7 +252,7 @@ struct bfx_workspace {
   bfx::DeviceBuffer adjoint;     // per-edge exact accumulators, upstream values, result
   std::vector<std::uint32_t> batch_engines;  // per-batch engine for BFX_ENGINE_AUTO launches
   std::vector<float> batch_deltas;           // per-batch near/far steps (empty: plain frontier)
-  std::uint32_t frontier_layout = 1;         // BFX_FRONTIER_FLAT (default) / BFX_FRONTIER_GROUPS
+  std::uint32_t frontier_layout = 2;         // BFX_FRONTIER_CHUNKED (default) / _FLAT / _GROUPS
   std::uint32_t relax_atomic = 0;            // flat frontier relaxation: 0 pre-read + min, 1 returning min
   std::uint32_t flat_items = 2;              // flat layout: work items per thread per iteration (2..4)
   std::uint32_t register_budget = 64;        // persistent kernel: 64 (default) or 40 registers per thread

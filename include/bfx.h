@@ -294,11 +294,11 @@ int bfx_set_batch_engines(bfx_workspace *ws, uint32_t count, const uint32_t *eng
  * count at execute time. */
 int bfx_set_batch_deltas(bfx_workspace *ws, uint32_t count, const float *deltas);
 /* Frontier-push work layout (a bfx scheduling option, results unchanged):
- * BFX_FRONTIER_FLAT (default) gives a warp 32 entries and walks their
+ * BFX_FRONTIER_FLAT gives a warp 32 entries and walks their
  * (lane, out-edge) pairs as one flat work list, two items per thread per
  * step; BFX_FRONTIER_GROUPS gives each queue entry a sub-warp group of 8
  * threads (batches of <= 8 lanes) or a whole warp; BFX_FRONTIER_CHUNKED
- * queues 32-vertex chunks instead of vertices (a chunk bitmap per round
+ * (default) queues 32-vertex chunks instead of vertices (a chunk bitmap per round
  * slot, pending lanes set with non-returning ORs) and runs the flat work list
  * over each chunk's vertices in index (spatial) order. */
 enum { BFX_FRONTIER_GROUPS = 0, BFX_FRONTIER_FLAT = 1, BFX_FRONTIER_CHUNKED = 2 };
