@@ -4,7 +4,7 @@
 // Three phases, all timed on the device with the library's own CUDA events
 // around the relaxation launch (best of `trials`):
 //  1. In context: the whole set on frontier push with one near/far step for
-//     every batch -- plain, and 1/2, 1, 2, 4, 8, 32 mean edge weights -- as it
+//     every batch -- plain, and 1/2, 1, 2, 4, 8, 32, 128 mean edge weights -- as it
 //     will run, in one launch; the fastest step wins.  (A batch timed alone
 //     favours few rounds; in one launch with others the work matters.)
 //  2. Per batch shape: Jacobi pull or dense chaotic push replaces frontier
@@ -91,7 +91,7 @@ extern "C" int bfx_autotune(bfx_workspace* ws, uint32_t count, const bfx_batch_d
 
     // Phase 1, in context: every batch on frontier push with one step, the
     // whole set relaxed together as it will run; keep the fastest step.
-    const float steps[] = {kPlain, 0.5f * w, 1.0f * w, 2.0f * w, 4.0f * w, 8.0f * w, 32.0f * w};
+    const float steps[] = {kPlain, 0.5f * w, 1.0f * w, 2.0f * w, 4.0f * w, 8.0f * w, 32.0f * w, 128.0f * w};
     bfx::check(bfx_prepare_batches(ws, count, batches));
     o.engine = BFX_ENGINE_FRONTIER_PUSH;
     float best_step = kPlain, best_set = 0.0f;

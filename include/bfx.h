@@ -263,7 +263,7 @@ int bfx_resident_graph_set_weights(bfx_resident_graph *graph, const float *weigh
 /* ---- engine autotuner ----------------------------------------------------------
  * No counterpart in the reference (its engine shootout, src/engine_shootout.cpp,
  * only catalogues configurations).  Picks the near/far step of frontier push
- * (plain, or 1/2, 1, 2, 4, 8 or 32 mean edge weights) by timing the whole set
+ * (plain, or 1/2, 1, 2, 4, 8, 32 or 128 mean edge weights) by timing the whole set
  * in one launch, then per batch shape Jacobi pull or dense chaotic push where
  * it is at least 1.5x faster on the batch alone (cached per lane width, valid
  * lanes, magnitude of union vertices and tiles), and keeps those engines only
