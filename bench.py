@@ -342,21 +342,31 @@ def main():
     h2d, d2h = ws.transfer_bytes()
 
     # ---- plain per-query engine (one query per launch sequence) on a sample
-    # of each query class; the whole set's time is extrapolated per class
-    plain_total_s, plain_sampled = 0.0, 0
-    for members, n in classes:
-        sample_q = members[:n]
-        barrier()
-        s3 = torch.cuda.Event(enable_timing=True)
-        e3 = torch.cuda.Event(enable_timing=True)
-        s3.record(stream)
-        for q in sample_q:
-            ws.run_query(q.sources, q.targets, q.selected_tiles, bfx.GpuRunOptions(engine=bfx.ENGINE_FRONTIER_PUSH))
-        e3.record(stream)
-        barrier()
-        plain_total_s += s3.elapsed_time(e3) / 1000 / len(sample_q) * len(members)
-        plain_sampled += len(sample_q)
-    plain_qps = len(queries) / plain_total_s
+    # of each query class; the whole set's time is extrapolated per class.
+    # The baseline is the faster of the frontier layouts for single queries.
+    plain_by_layout = {}
+    for lname, lid in (("chunked", bfx.FRONTIER_CHUNKED), ("flat", bfx.FRONTIER_FLAT)):
+        ws.set_frontier_layout(lid)
+        plain_total_s, plain_sampled = 0.0, 0
+        for members, n in classes:
+            sample_q = members[:n]
+            ws.run_query(sample_q[0].sources, sample_q[0].targets, sample_q[0].selected_tiles,
+                         bfx.GpuRunOptions(engine=bfx.ENGINE_FRONTIER_PUSH))  # warm-up
+            barrier()
+            s3 = torch.cuda.Event(enable_timing=True)
+            e3 = torch.cuda.Event(enable_timing=True)
+            s3.record(stream)
+            for q in sample_q:
+                ws.run_query(q.sources, q.targets, q.selected_tiles, bfx.GpuRunOptions(engine=bfx.ENGINE_FRONTIER_PUSH))
+            e3.record(stream)
+            barrier()
+            plain_total_s += s3.elapsed_time(e3) / 1000 / len(sample_q) * len(members)
+            plain_sampled += len(sample_q)
+        plain_by_layout[lname] = len(queries) / plain_total_s
+    ws.set_frontier_layout({"flat": bfx.FRONTIER_FLAT, "groups": bfx.FRONTIER_GROUPS,
+                            "chunked": bfx.FRONTIER_CHUNKED}[args.frontier])
+    plain_layout = max(plain_by_layout, key=plain_by_layout.get)
+    plain_qps = plain_by_layout[plain_layout]
 
     nq = len(queries) * world
     ms_per_step = dev_ms / args.steps
@@ -408,6 +418,7 @@ def main():
         "reached_lanes": reached,
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "plain_per_query": {"value": plain_qps, "unit": "queries/s", "sample": plain_sampled,
+                            "layout": plain_layout, "by_layout": plain_by_layout,
                             "batched_speedup": value / world / plain_qps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_src, "kernel": "persistent_kernel<0, %d, %d> (%s frontier%s)" % (
