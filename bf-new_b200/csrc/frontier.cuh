@@ -463,6 +463,7 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
   // Claims of the previous iteration: their pending-word ORs stay in flight
   // while this iteration decodes its items and issues its first loads.
   u32 p_old[kItems], p_v[kItems], p_cv[kItems];
+  u32 known_chunk = 0xFFFFFFFFu;  // chunked layout: last chunk whose bit this thread ORed
 #pragma unroll
   for (u32 u = 0; u < kItems; ++u) {
     p_old[u] = 1u;
@@ -548,11 +549,19 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
 #pragma unroll
     for (u32 u = 0; u < kItems; ++u) {
       if (kChunked) {
-        // pending lane with a non-returning OR; the chunk bit's OR claims
+        // pending lane with a non-returning OR; the chunk bit's OR claims.
+        // A chunk this thread already ORed in this item is known to be set
+        // for the round, so its bit is not ORed again.
         const u32 chunk = cdst[u] >> 5;
         const u32 bit = 1u << (chunk & 31u);
-        if (bits[u] != 0u) dev::red_or(B.mask_w + cdst[u], bits[u]);
-        p_old[u] = bits[u] != 0u ? (atomicOr(B.cmask_w + (chunk >> 5), bit) & bit) : 1u;
+        p_old[u] = 1u;
+        if (bits[u] != 0u) {
+          dev::red_or(B.mask_w + cdst[u], bits[u]);
+          if (chunk != known_chunk) {
+            p_old[u] = atomicOr(B.cmask_w + (chunk >> 5), bit) & bit;
+            known_chunk = chunk;
+          }
+        }
         p_v[u] = chunk;
         p_cv[u] = 0u;
       } else {
