@@ -552,6 +552,10 @@ class Workspace:
         """40 (three 512-thread blocks per SM) or 64 registers per thread for the persistent kernel."""
         _check(load().bfx_set_register_budget(self._h, u32(registers)))
 
+    def set_flat_order(self, edge_major: int):
+        """Flat/chunked work order: 0 entry-lane-edge, 1 entry-edge-lane."""
+        _check(load().bfx_set_flat_order(self._h, u32(edge_major)))
+
     def set_relax_atomic(self, mode: int):
         """Flat layout: 0 pre-read + min on success, 1 returning min per relaxation."""
         _check(load().bfx_set_relax_atomic(self._h, u32(mode)))

@@ -1191,6 +1191,7 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   p.round_trace = nullptr;
   p.trace_cap = 0u;
   p.amin = ws->relax_atomic;
+  p.edge_major = ws->edge_major;
   if (o.instrumentation == 2u && o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
     ws->round_trace.reserve(size_t{kRoundTraceCap} * 16u, ws->graph->device);
     p.round_trace = static_cast<u64*>(ws->round_trace.ptr);
@@ -1332,6 +1333,14 @@ int bfx_set_register_budget(bfx_workspace* ws, uint32_t registers) {
     bfx::require(ws != nullptr, "null argument");
     bfx::require(registers == 40u || registers == 64u, "register budget must be 40 or 64");
     ws->register_budget = registers;
+  });
+}
+
+int bfx_set_flat_order(bfx_workspace* ws, uint32_t edge_major) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null argument");
+    bfx::require(edge_major <= 1u, "flat work order must be 0 or 1");
+    ws->edge_major = edge_major;
   });
 }
 

@@ -136,6 +136,8 @@ struct LaunchParams {
   u64* round_trace;      // instrumentation 2: per round {start %globaltimer, warp items}; null otherwise
   u32 trace_cap;         // rounds the trace holds
   u32 amin;              // flat frontier: 1 = returning min per relaxation, 0 = pre-read + min on success
+  u32 edge_major;        // flat frontier work order: 1 = entry, edge, lane; 0 = entry, lane, edge
+  u32 reserved3;
 };
 
 constexpr u32 kRoundTraceCap = 65536;
@@ -253,7 +255,8 @@ struct bfx_workspace {
   std::vector<std::uint32_t> batch_engines;  // per-batch engine for BFX_ENGINE_AUTO launches
   std::vector<float> batch_deltas;           // per-batch near/far steps (empty: plain frontier)
   std::uint32_t frontier_layout = 2;         // BFX_FRONTIER_CHUNKED (default) / _FLAT / _GROUPS
-  std::uint32_t relax_atomic = 0;            // flat frontier relaxation: 0 pre-read + min, 1 returning min
+  std::uint32_t relax_atomic = 0;
+  std::uint32_t edge_major = 0;              // flat frontier work order (see bfx_set_flat_order)            // flat frontier relaxation: 0 pre-read + min, 1 returning min
   std::uint32_t flat_items = 2;              // flat layout: work items per thread per iteration (2..4)
   std::uint32_t register_budget = 64;        // persistent kernel: 64 (default) or 40 registers per thread
   bfx::DeviceBuffer deltas_dev;

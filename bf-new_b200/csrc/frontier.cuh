@@ -346,8 +346,11 @@ struct FlatItem {
   u32 ql, ed, cv;
 };
 
+// edge_major: work items ordered entry, then edge, then lane (consecutive
+// threads relax the lanes of one edge, whose labels are adjacent); otherwise
+// entry, then lane, then edge.
 __device__ __forceinline__ FlatItem flat_decode(u32 w, u32 total, u32 incl, u32 excl, u32 cv, u32 m, u32 rb,
-                                                u32 deg) {
+                                                u32 deg, bool edge_major) {
   u32 e = 0u;
   for (u32 s = 16u; s > 0u; s >>= 1) {
     if (__shfl_sync(0xFFFFFFFFu, incl, static_cast<int>(e + s - 1u)) <= w) e += s;
@@ -360,8 +363,16 @@ __device__ __forceinline__ FlatItem flat_decode(u32 w, u32 total, u32 incl, u32 
   FlatItem it{w < total, 0u, 0u, ecv};
   if (it.live) {
     const u32 r = w - eexcl;
-    const u32 j = r / edeg;  // lane ordinal within the entry
-    it.ed = erb + (r - j * edeg);
+    u32 j;  // lane ordinal within the entry
+    if (edge_major) {
+      const u32 k = static_cast<u32>(__popc(em));
+      const u32 edge = r / k;
+      j = r - edge * k;
+      it.ed = erb + edge;
+    } else {
+      j = r / edeg;
+      it.ed = erb + (r - j * edeg);
+    }
     u32 mm = em;
     for (u32 t = 0; t < j; ++t) mm &= mm - 1u;
     it.ql = __ffs(mm) - 1u;
@@ -477,7 +488,7 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
     u32 fd = 0xFFFFFFFFu;
 #pragma unroll
     for (u32 u = 0; u < kItems; ++u) {
-      it[u] = flat_decode(base + 32u * u + lane, total, incl, excl, cv, m, rb, deg);
+      it[u] = flat_decode(base + 32u * u + lane, total, incl, excl, cv, m, rb, deg, p.edge_major != 0u);
       bits[u] = fbits[u] = cdst[u] = dstv[u] = 0u;
       src[u] = dev::kInfBits;
     }

@@ -318,6 +318,10 @@ int bfx_set_flat_items(bfx_workspace *ws, uint32_t items);
  * candidate; 1 issues one returning 64-bit min per relaxation and takes the
  * returned label as the comparison. */
 int bfx_set_relax_atomic(bfx_workspace *ws, uint32_t mode);
+/* Flat and chunked layouts: order of an item's work list -- 0 (default)
+ * entry, lane, edge; 1 entry, edge, lane (neighbouring threads relax the
+ * lanes of one edge, whose target labels are adjacent). */
+int bfx_set_flat_order(bfx_workspace *ws, uint32_t edge_major);
 /* {mean edge weight, edge count} of the workspace's resident graph. */
 int bfx_workspace_graph_stats(bfx_workspace *ws, double out[2]);
 
