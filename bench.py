@@ -188,6 +188,8 @@ def main():
                     help="flat frontier: 1 = one returning min per relaxation")
     ap.add_argument("--edge-major", type=int, default=0, choices=[0, 1],
                     help="flat/chunked work order: 1 = entry, edge, lane")
+    ap.add_argument("--pairs", type=int, default=0, choices=[0, 1],
+                    help="chunked frontier: 1 = one (vertex, lane) pair per thread")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=None)
     args = ap.parse_args()
@@ -258,6 +260,7 @@ def main():
     ws.set_flat_items(args.items)
     ws.set_relax_atomic(args.amin)
     ws.set_flat_order(args.edge_major)
+    ws.set_chunk_pairs(args.pairs)
     engine_id = {"auto": bfx.ENGINE_AUTO, "frontier": bfx.ENGINE_FRONTIER_PUSH, "jacobi": bfx.ENGINE_JACOBI_PULL,
                  "dense": bfx.ENGINE_DENSE_CHAOTIC_PUSH}[args.engine]
     engines_chosen = None
@@ -407,7 +410,7 @@ def main():
                    "planner_policy": [policy.minimum_jaccard_numerator, policy.minimum_jaccard_denominator,
                                       policy.maximum_union_inflation_numerator,
                                       policy.maximum_union_inflation_denominator],
-                   "frontier_layout": args.frontier, "registers": args.regs, "flat_items": args.items, "returning_min": args.amin, "edge_major": args.edge_major,
+                   "frontier_layout": args.frontier, "registers": args.regs, "flat_items": args.items, "returning_min": args.amin, "edge_major": args.edge_major, "chunk_pairs": args.pairs,
                    "engines_chosen": None if engines_chosen is None else
                    {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
                    "frontier_steps_chosen": None if engines_chosen is None else

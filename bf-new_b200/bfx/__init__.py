@@ -552,6 +552,10 @@ class Workspace:
         """40 (three 512-thread blocks per SM) or 64 registers per thread for the persistent kernel."""
         _check(load().bfx_set_register_budget(self._h, u32(registers)))
 
+    def set_chunk_pairs(self, mode: int):
+        """Chunked layout: 0 work list, 1 (vertex, lane) pair per thread (persistent control)."""
+        _check(load().bfx_set_chunk_pairs(self._h, u32(mode)))
+
     def set_flat_order(self, edge_major: int):
         """Flat/chunked work order: 0 entry-lane-edge, 1 entry-edge-lane."""
         _check(load().bfx_set_flat_order(self._h, u32(edge_major)))

@@ -379,7 +379,7 @@ __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
 
 // kChunked: compiled for the chunked frontier layout only (a separate
 // kernel instantiation, so the other layouts keep their register budget).
-template <bool kCount, u32 kItems, bool kChunked>
+template <bool kCount, u32 kItems, bool kChunked, bool kPairs = false>
 __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work& wk) {
   const u32 ridx = r % 3u, widx = (r + 1u) % 3u;
   const u32 total = prefix[p.nb];
@@ -413,7 +413,7 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
       const FrontierView V = frontier_view(B, r & 1u, g % 3u, (g + 1u) % 3u);
       if (n != 0u) {
         if (kChunked) {
-          frontier_flat<kCount, kItems, true>(p, V, C, item, n, 32u, r & 1u, widx, tau, g % 3u, wk);
+          frontier_flat<kCount, kItems, true, kPairs>(p, V, C, item, n, 32u, r & 1u, widx, tau, g % 3u, wk);
         } else if (p.flat) {
           frontier_flat<kCount, kItems, false>(p, V, C, item, n, flat_entries_per_item(n), r & 1u, widx, tau, g % 3u, wk);
         } else if (B.W <= 8u) {
@@ -481,7 +481,7 @@ __device__ void flush_work(const LaunchParams& p, Work& wk) {
 // for: 3 -> 40 registers per thread (48 warps per SM), 2 -> 64 registers
 // (32 warps per SM; no spills in the group layout, a few in the flat one).
 // kItems = flat-layout work items per thread per iteration.
-template <bool kCount, int kMinBlocks, u32 kItems, bool kChunked = false>
+template <bool kCount, int kMinBlocks, u32 kItems, bool kChunked = false, bool kPairs = false>
 __global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParams p) {
   extern __shared__ u32 prefix[];
   const u32 nblocks = gridDim.x;
@@ -497,7 +497,7 @@ __global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParam
       p.round_trace[2u * r] = dev::global_ns();
       p.round_trace[2u * r + 1u] = total;
     }
-    round_body<kCount, kItems, kChunked>(p, r, prefix, wk);
+    round_body<kCount, kItems, kChunked, kPairs>(p, r, prefix, wk);
     // Past the launch budget block 0 raises the barrier's abort before it
     // arrives, so every block leaves after this round.
     if (blockIdx.x == 0 && threadIdx.x == 0 && dev::global_ns() - t0 > p.budget_ns) {
@@ -1155,7 +1155,11 @@ int grid_blocks(bfx_workspace* ws, const void* kernel, int block, size_t smem, c
 // Persistent kernel instantiation: 64 registers (two 512-thread blocks per
 // SM) with 2, 3 or 4 flat work items per thread, or 40 registers with 2;
 // the chunked layout has its own (64 registers, 2 items).
-const void* persistent_entry(bool count, bool wide, std::uint32_t items, bool chunked) {
+const void* persistent_entry(bool count, bool wide, std::uint32_t items, bool chunked, bool pairs) {
+  if (chunked && pairs) {
+    return count ? reinterpret_cast<const void*>(persistent_kernel<true, 2, 2, true, true>)
+                 : reinterpret_cast<const void*>(persistent_kernel<false, 2, 2, true, true>);
+  }
   if (chunked) {
     return count ? reinterpret_cast<const void*>(persistent_kernel<true, 2, 2, true>)
                  : reinterpret_cast<const void*>(persistent_kernel<false, 2, 2, true>);
@@ -1237,7 +1241,7 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   BFX_CUDA(cudaEventRecord(ws->ev[1], ws->stream));
   if (o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
     const void* kfn = persistent_entry(o.instrumentation != 0u, ws->register_budget == 64u, ws->flat_items,
-                                       p.flat == 2u);
+                                       p.flat == 2u, ws->chunk_pairs != 0u);
     const int grid = grid_blocks(ws, kfn, block, smem, o);
     void* args[] = {&p};
     BFX_CUDA(cudaLaunchCooperativeKernel(kfn, grid, block, args, smem, ws->stream));
@@ -1333,6 +1337,14 @@ int bfx_set_register_budget(bfx_workspace* ws, uint32_t registers) {
     bfx::require(ws != nullptr, "null argument");
     bfx::require(registers == 40u || registers == 64u, "register budget must be 40 or 64");
     ws->register_budget = registers;
+  });
+}
+
+int bfx_set_chunk_pairs(bfx_workspace* ws, uint32_t mode) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null argument");
+    bfx::require(mode <= 1u, "chunk pair mode must be 0 or 1");
+    ws->chunk_pairs = mode;
   });
 }
 

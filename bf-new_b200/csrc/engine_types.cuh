@@ -256,7 +256,8 @@ struct bfx_workspace {
   std::vector<float> batch_deltas;           // per-batch near/far steps (empty: plain frontier)
   std::uint32_t frontier_layout = 2;         // BFX_FRONTIER_CHUNKED (default) / _FLAT / _GROUPS
   std::uint32_t relax_atomic = 0;
-  std::uint32_t edge_major = 0;              // flat frontier work order (see bfx_set_flat_order)            // flat frontier relaxation: 0 pre-read + min, 1 returning min
+  std::uint32_t edge_major = 0;
+  std::uint32_t chunk_pairs = 0;             // chunked frontier pair mode (see bfx_set_chunk_pairs)              // flat frontier work order (see bfx_set_flat_order)            // flat frontier relaxation: 0 pre-read + min, 1 returning min
   std::uint32_t flat_items = 2;              // flat layout: work items per thread per iteration (2..4)
   std::uint32_t register_budget = 64;        // persistent kernel: 64 (default) or 40 registers per thread
   bfx::DeviceBuffer deltas_dev;

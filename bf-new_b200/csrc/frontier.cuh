@@ -413,7 +413,9 @@ __device__ __forceinline__ void stage_claims(bool claim, u32 v, u32 cv, u64* sta
 // 32 c .. 32 c + 31) instead of `epi` queued vertices; successes set the
 // pending lane with a non-returning OR and claim the target's chunk through
 // the chunk bitmap.
-template <bool kCount, u32 kItems, bool kChunked>
+// kPairs (chunked only): the warp walks the item's (entry, lane) pairs, one
+// per thread, each over its entry's out-edges -- no per-edge decode.
+template <bool kCount, u32 kItems, bool kChunked, bool kPairs = false>
 __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
                                               u32 epi, u32 rd, u32 widx, u32 tau_bits, u32 pile, Work& wk) {
   __shared__ u64 s_stage[16][kStage];  // blocks of up to 512 threads
@@ -463,16 +465,8 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
       wk.c[2] += __popc(m);
     }
   }
-  const u32 work = static_cast<u32>(__popc(m)) * deg;
-  u32 incl = work;
-  for (u32 o = 1; o < 32u; o <<= 1) {
-    const u32 y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-    if (lane >= o) incl += y;
-  }
-  const u32 excl = incl - work;
-  const u32 total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-  // Claims of the previous iteration: their pending-word ORs stay in flight
-  // while this iteration decodes its items and issues its first loads.
+  // Claims of the previous step: their pending-word ORs stay in flight
+  // while the next step decodes its items and issues its first loads.
   u32 p_old[kItems], p_v[kItems], p_cv[kItems];
   u32 known_chunk = 0xFFFFFFFFu;  // chunked layout: last chunk whose bit this thread ORed
 #pragma unroll
@@ -480,22 +474,18 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
     p_old[u] = 1u;
     p_v[u] = p_cv[u] = 0u;
   }
-  for (u32 base = 0; base < total; base += 32u * kItems) {
-    FlatItem it[kItems];
-    u32 src[kItems], bits[kItems], fbits[kItems], cdst[kItems], dstv[kItems];
+  // One step: kItems (lane, edge) items per thread, memory phases interleaved.
+  auto step = [&](const FlatItem (&it)[kItems], u32 (&src)[kItems], bool load_src) {
+    u32 bits[kItems], fbits[kItems], cdst[kItems], dstv[kItems];
     uint4 rec[kItems];
     uint2 dt[kItems];
     u32 fd = 0xFFFFFFFFu;
 #pragma unroll
-    for (u32 u = 0; u < kItems; ++u) {
-      it[u] = flat_decode(base + 32u * u + lane, total, incl, excl, cv, m, rb, deg, p.edge_major != 0u);
-      bits[u] = fbits[u] = cdst[u] = dstv[u] = 0u;
-      src[u] = dev::kInfBits;
-    }
+    for (u32 u = 0; u < kItems; ++u) bits[u] = fbits[u] = cdst[u] = dstv[u] = 0u;
 #pragma unroll
     for (u32 u = 0; u < kItems; ++u) {
       if (it[u].live) {
-        src[u] = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(it[u].cv) << B.shift) + it[u].ql)));
+        if (load_src) src[u] = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(it[u].cv) << B.shift) + it[u].ql)));
         rec[u] = __ldg(p.g.csr + it[u].ed);
       }
     }
@@ -580,6 +570,69 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
         p_v[u] = dstv[u];
         p_cv[u] = cdst[u];
       }
+    }
+  };
+  if (kPairs) {
+    // Pair mode: each thread takes one (entry, lane) pair of the item and
+    // walks that entry's edges kItems per step; one source read per pair,
+    // no per-edge decode.
+    const u32 k = static_cast<u32>(__popc(m));
+    u32 kincl = k;
+    for (u32 o = 1; o < 32u; o <<= 1) {
+      const u32 y = __shfl_up_sync(0xFFFFFFFFu, kincl, o);
+      if (lane >= o) kincl += y;
+    }
+    const u32 kexcl = kincl - k;
+    const u32 pairs = __shfl_sync(0xFFFFFFFFu, kincl, 31);
+    for (u32 pbase = 0; pbase < pairs; pbase += 32u) {
+      const u32 pi = pbase + lane;
+      u32 e = 0u;
+      for (u32 s = 16u; s > 0u; s >>= 1) {
+        if (__shfl_sync(0xFFFFFFFFu, kincl, static_cast<int>(e + s - 1u)) <= pi) e += s;
+      }
+      const u32 ecv = __shfl_sync(0xFFFFFFFFu, cv, static_cast<int>(e));
+      const u32 em = __shfl_sync(0xFFFFFFFFu, m, static_cast<int>(e));
+      const u32 erb = __shfl_sync(0xFFFFFFFFu, rb, static_cast<int>(e));
+      const u32 edeg = __shfl_sync(0xFFFFFFFFu, deg, static_cast<int>(e));
+      const u32 eexcl = __shfl_sync(0xFFFFFFFFu, kexcl, static_cast<int>(e));
+      const bool plive = pi < pairs;
+      u32 pql = 0u, psrc = dev::kInfBits;
+      if (plive) {
+        u32 mm = em;
+        for (u32 t = 0; t < pi - eexcl; ++t) mm &= mm - 1u;
+        pql = __ffs(mm) - 1u;
+        psrc = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(ecv) << B.shift) + pql)));
+      }
+      const u32 steps = __reduce_max_sync(0xFFFFFFFFu, plive ? edeg : 0u);
+      for (u32 s = 0; s < steps; s += kItems) {
+        FlatItem it[kItems];
+        u32 src[kItems];
+#pragma unroll
+        for (u32 u = 0; u < kItems; ++u) {
+          it[u] = FlatItem{plive && s + u < edeg, pql, erb + s + u, ecv};
+          src[u] = psrc;
+        }
+        step(it, src, false);
+      }
+    }
+  } else {
+    const u32 work = static_cast<u32>(__popc(m)) * deg;
+    u32 incl = work;
+    for (u32 o = 1; o < 32u; o <<= 1) {
+      const u32 y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const u32 excl = incl - work;
+    const u32 total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    for (u32 base = 0; base < total; base += 32u * kItems) {
+      FlatItem it[kItems];
+      u32 src[kItems];
+#pragma unroll
+      for (u32 u = 0; u < kItems; ++u) {
+        it[u] = flat_decode(base + 32u * u + lane, total, incl, excl, cv, m, rb, deg, p.edge_major != 0u);
+        src[u] = dev::kInfBits;
+      }
+      step(it, src, true);
     }
   }
 #pragma unroll

@@ -322,6 +322,11 @@ int bfx_set_relax_atomic(bfx_workspace *ws, uint32_t mode);
  * entry, lane, edge; 1 entry, edge, lane (neighbouring threads relax the
  * lanes of one edge, whose target labels are adjacent). */
 int bfx_set_flat_order(bfx_workspace *ws, uint32_t edge_major);
+/* Chunked layout, persistent control: how a chunk's work is spread over the
+ * warp -- 0 (default) the flat work list of (lane, edge) items; 1 one
+ * (vertex, lane) pair per thread walking the vertex's out-edges (no per-edge
+ * decode; idle threads where degrees differ).  Host-poll modes use 0. */
+int bfx_set_chunk_pairs(bfx_workspace *ws, uint32_t mode);
 /* {mean edge weight, edge count} of the workspace's resident graph. */
 int bfx_workspace_graph_stats(bfx_workspace *ws, double out[2]);
 

@@ -282,13 +282,14 @@ def test_autotuner_with_near_far_candidates(gpu):
     res.close()
 
 
-@pytest.mark.parametrize("regs,items,amin,order", [(40, 2, 0, 0), (64, 2, 0, 0), (64, 3, 0, 0), (64, 4, 0, 0),
-                                                   (64, 2, 1, 0), (64, 2, 0, 1)])
+@pytest.mark.parametrize("regs,items,amin,order,pairs", [(40, 2, 0, 0, 0), (64, 2, 0, 0, 0), (64, 3, 0, 0, 0),
+                                                         (64, 4, 0, 0, 0), (64, 2, 1, 0, 0), (64, 2, 0, 1, 0),
+                                                         (64, 2, 0, 0, 1)])
 @pytest.mark.parametrize("layout_kind", [bfx.FRONTIER_FLAT, bfx.FRONTIER_GROUPS, bfx.FRONTIER_CHUNKED],
                          ids=["flat", "groups", "chunked"])
 @pytest.mark.parametrize("step", [None, 3.0])
 @pytest.mark.parametrize("control", [bfx.CONTROL_PERSISTENT, bfx.CONTROL_PER_ROUND], ids=["persistent", "per_round"])
-def test_flat_frontier_layout_bit_exact(gpu, c1, step, control, layout_kind, regs, items, amin, order):
+def test_flat_frontier_layout_bit_exact(gpu, c1, step, control, layout_kind, regs, items, amin, order, pairs):
     """The flat work-list frontier (32 entries per warp, (lane, edge) pairs
     walked 32 per step) gives the oracle's labels on full-graph W=8, regional
     multi-batch W in {1, 8, 16, 32}, plain and near/far."""
@@ -308,6 +309,7 @@ def test_flat_frontier_layout_bit_exact(gpu, c1, step, control, layout_kind, reg
         ws.set_flat_items(items)
         ws.set_relax_atomic(amin)
         ws.set_flat_order(order)
+        ws.set_chunk_pairs(pairs)
         ws.prepare(descs)
         if step is not None:
             ws.set_batch_deltas([step] * len(descs))
