@@ -190,6 +190,8 @@ def main():
                     help="flat/chunked work order: 1 = entry, edge, lane")
     ap.add_argument("--pairs", type=int, default=0, choices=[0, 1],
                     help="chunked frontier: 1 = one (vertex, lane) pair per thread")
+    ap.add_argument("--tune-policy", action="store_true",
+                    help="choose the planner policy by timing each candidate's plan (bfx_autotune_policy)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=None)
     args = ap.parse_args()
@@ -264,6 +266,19 @@ def main():
     engine_id = {"auto": bfx.ENGINE_AUTO, "frontier": bfx.ENGINE_FRONTIER_PUSH, "jacobi": bfx.ENGINE_JACOBI_PULL,
                  "dense": bfx.ENGINE_DENSE_CHAOTIC_PUSH}[args.engine]
     engines_chosen = None
+    policy_times = None
+    if args.tune_policy:
+        # planner / autotuner co-design: the policy whose plan runs fastest
+        candidates = [policy] + [bfx.BatchPlannerPolicy(32, *c, narrow_lanes=True)
+                                 for c in ((1, 16, 4, 1), (1, 4, 2, 1), (1, 32, 8, 1))]
+        t4 = time.time()
+        best, policy_times = ws.autotune_policy(layout, queries, candidates)
+        policy = candidates[best]
+        plan = bfx.make_overlapping_batch_plan(layout, queries, policy)
+        descs = plan.descriptions()
+        lane_edges = sum(e[3] for e in plan.estimates)
+        log(f"[bench] policy tuning {time.time() - t4:.1f}s: times {policy_times}, best {best}, "
+            f"{plan.batch_count} batches")
     if engine_id == bfx.ENGINE_AUTO:
         t3 = time.time()
         engines_chosen, measured = ws.autotune(descs)
@@ -407,6 +422,7 @@ def main():
         "config": {"workload": workload_desc,
                    "queries_per_gpu": len(queries), "batches": plan.batch_count,
                    "lane_widths": sorted({d.lane_width for d in descs}), "engine": args.engine,
+                   "policy_times_ms": policy_times,
                    "planner_policy": [policy.minimum_jaccard_numerator, policy.minimum_jaccard_denominator,
                                       policy.maximum_union_inflation_numerator,
                                       policy.maximum_union_inflation_denominator],

@@ -543,6 +543,26 @@ class Workspace:
         self.tuned_deltas = [float(x) for x in deltas]
         return list(out), measured.value
 
+    def autotune_policy(self, layout, queries: Sequence["RouteQuery"], policies: Sequence["BatchPlannerPolicy"],
+                        base: GpuRunOptions | None = None, trials: int = 2) -> tuple[int, list[float]]:
+        """bfx_autotune_policy: plans, tunes and times the whole query set under each
+        candidate planner policy; returns (index of the fastest, relaxation ms per
+        candidate).  The workspace is left prepared and tuned with the winner;
+        make_overlapping_batch_plan(layout, queries, policies[best]) rebuilds its plan."""
+        v = layout.view()
+        tvo = np.ascontiguousarray(layout.tiles["tile_vertex_offsets"], np.uint32)
+        qs = list(queries)
+        qc = (RouteQueryC * len(qs))(*[q.c() for q in qs])
+        pc = (PlannerPolicyC * len(policies))(*[p.c() for p in policies])
+        best = u32()
+        times = (f32 * len(policies))()
+        _check(load().bfx_autotune_policy(self._h, C.byref(v), _ptr(tvo), u32(len(qs)), qc, u32(len(policies)), pc,
+                                          C.byref(base or GpuRunOptions()), u32(trials), C.byref(best), times))
+        plan = make_overlapping_batch_plan(layout, qs, policies[best.value])
+        self._keep = plan.descriptions()
+        self.batch_count = plan.batch_count
+        return best.value, [float(t) for t in times]
+
     def set_batch_deltas(self, deltas: Sequence[float]):
         """Near/far threshold steps per frontier batch (inf = plain frontier)."""
         arr = (f32 * len(deltas))(*deltas)

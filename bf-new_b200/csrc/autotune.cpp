@@ -17,12 +17,14 @@
 // execute with engine == BFX_ENGINE_AUTO runs each batch on its own engine
 // inside one launch.
 #include "bfx.h"
+#include "bfx_host.h"
 #include "bfx_internal.hpp"
 
 #include <algorithm>
 #include <bit>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <tuple>
 #include <vector>
@@ -178,5 +180,50 @@ extern "C" int bfx_autotune_reset(void) {
   return bfx::guarded([&] {
     std::lock_guard<std::mutex> lock(bfx::g_tune_mutex);
     bfx::g_tune_cache.clear();
+  });
+}
+
+extern "C" int bfx_autotune_policy(bfx_workspace* ws, const bfx_device_graph_layout32* layout,
+                                   const uint32_t* tile_vertex_offsets, uint32_t query_count,
+                                   const bfx_route_query* queries, uint32_t policy_count,
+                                   const bfx_planner_policy* policies, const bfx_gpu_run_options* base,
+                                   uint32_t trials, uint32_t* best, float* times_ms) {
+  return bfx::guarded([&] {
+    bfx::require(ws && layout && tile_vertex_offsets && queries && policies && base && best && query_count > 0 &&
+                     policy_count > 0,
+                 "null argument");
+    if (trials == 0) trials = 1;
+    bfx_gpu_run_options o;
+    std::memcpy(&o, base, sizeof(o));
+    o.instrumentation = 0;
+    o.engine = BFX_ENGINE_AUTO;
+    std::uint32_t best_i = 0;
+    float best_t = 0.0f;
+    // One candidate: plan, tune (engines and steps), time the whole set.
+    const auto measure = [&](std::uint32_t i) -> float {
+      bfx_plan* plan = nullptr;
+      bfx::check(bfx_plan_build(layout, tile_vertex_offsets, query_count, queries, &policies[i], &plan));
+      std::unique_ptr<bfx_plan, int (*)(bfx_plan*)> owner(plan, bfx_plan_destroy);
+      std::uint32_t n = 0;
+      bfx::check(bfx_plan_batch_count(plan, &n));
+      const bfx_batch_description* descs = nullptr;
+      bfx::check(bfx_plan_descriptions(plan, &descs));
+      std::vector<std::uint32_t> engines(n);
+      std::vector<float> deltas(n);
+      bfx::check(bfx_autotune(ws, n, descs, base, trials, engines.data(), deltas.data(), nullptr));
+      return bfx::time_set(ws, o, trials);
+    };
+    for (std::uint32_t i = 0; i < policy_count; ++i) {
+      const float t = measure(i);
+      if (times_ms) times_ms[i] = t;
+      if (i == 0 || t < best_t) {
+        best_t = t;
+        best_i = i;
+      }
+    }
+    // leave the workspace prepared and tuned with the winner (the engine
+    // cache makes the second tuning pass cheap)
+    if (best_i != policy_count - 1u) (void)measure(best_i);
+    *best = best_i;
   });
 }

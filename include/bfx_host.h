@@ -141,6 +141,19 @@ int bfx_synth_fill(const bfx_synth_config *config, int32_t *x, int32_t *y, uint8
                    uint64_t *provenance_record, bfx_spatial_order_config *order,
                    uint64_t stats[2]);
 
+/* Planner / autotuner co-design (no counterpart in the reference, whose
+ * planner takes one fixed policy, src/batch_plan.cpp:680): plans the queries
+ * with each candidate policy (bfx_plan_build), tunes and times the whole set
+ * as it would run (bfx_autotune, then the fastest of `trials` launches with
+ * BFX_ENGINE_AUTO), and reports the fastest.  times_ms[policy_count] receives
+ * each candidate's relaxation time, *best its index.  The workspace is left
+ * prepared and tuned with the best candidate's plan, which the caller can
+ * rebuild with bfx_plan_build and the same policy. */
+int bfx_autotune_policy(bfx_workspace *ws, const bfx_device_graph_layout32 *layout,
+                        const uint32_t *tile_vertex_offsets, uint32_t query_count, const bfx_route_query *queries,
+                        uint32_t policy_count, const bfx_planner_policy *policies, const bfx_gpu_run_options *base,
+                        uint32_t trials, uint32_t *best, float *times_ms);
+
 #ifdef __cplusplus
 }
 #endif

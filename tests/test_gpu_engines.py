@@ -362,3 +362,25 @@ def test_round_trace_at_debug_instrumentation(gpu, c1):
     assert np.all(tr[:, 1] > 0)
     ws.close()
     res.close()
+
+
+def test_planner_policy_autotune_picks_and_prepares_the_fastest(gpu):
+    """bfx_autotune_policy times the whole set under each planner policy and
+    leaves the workspace prepared with the fastest plan, whose labels are the
+    oracle's."""
+    layout, grid = workloads.build_graph("c2", scale_tiles=(32, 32))
+    qs = workloads.box_queries(layout, grid, 40, 2, 16, seed=41)
+    policies = [bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True),
+                bfx.BatchPlannerPolicy(32, 0, 1, 64, 1, narrow_lanes=True)]
+    res = bfx.ResidentDeviceGraph.upload_once(layout)
+    ws = bfx.Workspace(res)
+    best, times = ws.autotune_policy(layout, qs, policies)
+    assert best in (0, 1) and all(t > 0 for t in times) and times[best] == min(times)
+    descs = bfx.make_overlapping_batch_plan(layout, qs, policies[best]).descriptions()
+    ws.execute(bfx.GpuRunOptions(engine=bfx.ENGINE_AUTO))
+    st = ws.fetch_statuses()
+    labels = [ws.download_labels(b, x.lane_width) for b, x in enumerate(descs)]
+    lanes = [[qs[i] if i != bfx.NO_EDGE else None for i in x.query_index_by_lane] for x in descs]
+    check_batches(layout, descs, lanes, st, labels, Oracle.from_layout(layout))
+    ws.close()
+    res.close()
