@@ -41,7 +41,8 @@ import numpy as np  # noqa: E402
 METRIC = "batched SSSP queries/s (256 uneven regional queries, 2.1M V / 16.8M E, one persistent launch)"
 METRIC_C3 = "batched SSSP queries/s (64 full-graph sources, 16.8M V / 168M E, one persistent launch)"
 METRIC_C5 = "batched SSSP queries/s (4,096 regional + 16 full-graph queries, 16.8M V / 168M E, autotuned)"
-METRICS = {"c2": METRIC, "c3": METRIC_C3, "c5": METRIC_C5}
+METRICS = {"c2": METRIC, "c3": METRIC_C3, "c5": METRIC_C5,
+           "c3small": "batched SSSP queries/s (32 full-graph sources, 4.2M V / 42M E, profiling-sized c3)"}
 
 
 def log(*a):
@@ -175,7 +176,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="bfx", choices=["bfx", "reference"])
     ap.add_argument("--engine", default="auto", choices=["auto", "frontier", "jacobi", "dense"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5", "c3small"])
     ap.add_argument("--frontier", default="chunked", choices=["groups", "flat", "chunked"],
                     help="frontier-push work layout (sub-warp groups or flat work list)")
     ap.add_argument("--regs", type=int, default=64, choices=[40, 64],
@@ -215,7 +216,10 @@ def main():
     from bfx import replicas, workloads
 
     t0 = time.time()
-    g, order, gstats = bfx.synth_graph(**workloads.GRAPHS["c3" if args.workload == "c5" else args.workload])
+    spec = dict(workloads.GRAPHS["c3" if args.workload in ("c5", "c3small") else args.workload])
+    if args.workload == "c3small":  # c3 generator on 128x128 tiles: a profiling-sized case of the c3 kernel
+        spec["tiles_x"] = spec["tiles_y"] = 128
+    g, order, gstats = bfx.synth_graph(**spec)
     layout = bfx.build_device_graph_layout(g, order)
     # query classes: (queries, plain-engine sample size) -- the plain per-query
     # rate is extrapolated class by class from its sample
@@ -226,6 +230,13 @@ def main():
         policy = bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True)
         workload_desc = ("c2: 256 uneven regional queries (box side U[4,64] tiles) on 128x128 tiles x 128 nodes, "
                          "2,097,152 V / 16,777,216 E, f32 lognormal costs")
+    elif args.workload == "c3small":
+        grid = (128, 128)
+        queries = workloads.full_graph_queries(layout, grid, args.queries or 32, 303 + 1000 * rank)
+        classes = [(queries, 2)]
+        policy = bfx.BatchPlannerPolicy(32, 0, 1, 64, 1)
+        workload_desc = ("c3small: 32 full-graph sources in one batch of 32 on 128x128 tiles x 256 nodes, "
+                         "4,194,304 V / 41,943,040 E, uint costs U[1,255] (profiling-sized c3)")
     elif args.workload == "c3":
         grid = (256, 256)
         queries = workloads.full_graph_queries(layout, grid, args.queries or 64, 303 + 1000 * rank)
@@ -435,7 +446,7 @@ def main():
                     for d in sorted({x for e, x in zip(engines_chosen, ws.tuned_deltas) if e == 2})},
                    "control": "persistent_cooperative", "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (graph %s GB + labels), no flush" % (
-                       "0.54" if args.workload == "c2" else "5.4")},
+                       {"c2": "0.54", "c3small": "1.3"}.get(args.workload, "5.4"))},
         "gteps": lane_edges * world / (ms_per_step / 1000) / 1e9,
         "reached_lanes": reached,
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
