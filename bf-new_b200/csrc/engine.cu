@@ -18,10 +18,12 @@
 //     masks are materialised;
 //   * edges are 16-byte records {endpoint, weight bits, eid+1, endpoint tile}
 //     read with 128-bit non-coherent loads;
-//   * a frontier vertex is processed by one warp that flattens (edge, active
-//     lane) pairs over its 32 threads; improvements use a non-returning
-//     64-bit min after a coherent pre-read, success bits are OR-combined per
-//     edge with shuffles and queue claims are warp-aggregated;
+//   * the frontier is a queue of 32-vertex chunks by default (frontier.cuh:
+//     chunk bitmaps per round slot, pending lanes set with non-returning ORs,
+//     claims staged per warp); a warp item is one chunk whose (lane, edge)
+//     work is walked as a flat list, two items per thread in flight; the
+//     vertex-queue flat layout and the sub-warp group layout remain options;
+//     improvements use a non-returning 64-bit min after a coherent pre-read;
 //   * persistent mode runs all rounds of all batches in one cooperative
 //     launch with a grid barrier whose waits time out; host-poll modes run
 //     CUDA-graph-captured chunks of rounds.

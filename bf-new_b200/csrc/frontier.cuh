@@ -1,6 +1,9 @@
-// Frontier push round body (included by engine.cu after the device records).
+// Frontier push round bodies (included by engine.cu after the device records):
+// frontier_group (sub-warp groups per queued vertex), frontier_flat (flat
+// (lane, edge) work list over queued vertices or, with kChunked, over queued
+// 32-vertex chunks -- the default), split_group (near/far split rounds).
 //
-// One warp item covers EPW = 32 / S queue entries of one batch: a group of S
+// frontier_group: one warp item covers EPW = 32 / S queue entries of one batch: a group of S
 // threads per entry (S = 8 for batches of <= 8 lanes, 32 otherwise).  Within
 // a group the entry's k active lanes are spread over aligned sub-groups of
 // kp = 2^ceil(log2 k) threads, so a group relaxes S / kp edges per step and
