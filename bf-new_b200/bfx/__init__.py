@@ -681,10 +681,11 @@ class Workspace:
         return dict(zip(self.WORK_KEYS, (int(x) for x in out)))
 
     def round_trace(self) -> np.ndarray:
-        """(rounds, 2) array of {start ns, warp items} from the last instrumentation-2 persistent run."""
+        """(rounds, 4) array of {start ns, warp items | split batches << 32, active pairs,
+        lane-edge relaxations} from the last instrumentation-2 persistent run."""
         n = u32()
         _check(load().bfx_fetch_round_trace(self._h, u32(0), None, C.byref(n)))
-        out = np.zeros((max(n.value, 1), 2), np.uint64)
+        out = np.zeros((max(n.value, 1), 4), np.uint64)
         _check(load().bfx_fetch_round_trace(self._h, u32(n.value), _ptr(out, u64), C.byref(n)))
         return out[:n.value]
 
@@ -694,7 +695,8 @@ class Workspace:
         _check(load().bfx_fetch_engine_work(self._h, out))
         w = [int(x) for x in out]
         return {"push": dict(zip(self.WORK_KEYS[:7], w[:7])), "rounds": w[7],
-                "jacobi": {"items": w[8], "records": w[9], "relaxations": w[10], "changes": w[11]}}
+                "jacobi": {"items": w[8], "records": w[9], "relaxations": w[10], "changes": w[11]},
+                "split": {"entries": w[12], "lanes": w[13]}}
 
     def run_query(self, sources, targets, selected_tiles, options: GpuRunOptions) -> DeviceRunStatus:
         s = np.ascontiguousarray(np.unique(np.asarray(sources, np.uint32)))

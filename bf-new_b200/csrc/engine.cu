@@ -381,6 +381,9 @@ __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
 
 // kChunked: compiled for the chunked frontier layout only (a separate
 // kernel instantiation, so the other layouts keep their register budget).
+// The warp's claim stages and far-pile minimum (flat and chunked layouts)
+// serve one (round, batch): flushed when the warp moves to another batch and
+// at the end of the round, before the grid barrier.
 template <bool kCount, u32 kItems, bool kChunked, bool kPairs = false>
 __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work& wk) {
   const u32 ridx = r % 3u, widx = (r + 1u) % 3u;
@@ -388,6 +391,8 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
   const u32 warps_per_block = blockDim.x >> 5;
   const u32 gw = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
   const u32 nw = gridDim.x * warps_per_block;
+  Stages st{{0u, 0u}, 0xFFFFFFFFu};
+  u32 staged_batch = 0xFFFFFFFFu;
   for (u32 w = gw; w < total; w += nw) {
     const u32 b = find_batch(prefix, p.nb, w);
     const DBatch& B = p.batches[b];
@@ -413,20 +418,34 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
       f = __shfl_sync(0xFFFFFFFFu, f, 0);
       tau_next = __shfl_sync(0xFFFFFFFFu, tau_next, 0);
       const FrontierView V = frontier_view(B, r & 1u, g % 3u, (g + 1u) % 3u);
+      if (b != staged_batch) {
+        // near round: claims to the next queue, parked lanes to pile g % 3;
+        // split round: pile g % 3 is read and re-parked lanes go to g + 1
+        stages_flush(st);
+        staged_batch = b;
+        const u32 po = n != 0u ? g % 3u : (g + 1u) % 3u;
+        if (lane_id() == 0u) {
+          const u32 wib = threadIdx.x >> 5;
+          s_stage_queue[kNear][wib] = StageQueue{V.queue_w, &C.count[widx], &C.error_bits, V.U};
+          s_stage_queue[kFar][wib] = StageQueue{n != 0u ? V.pile : V.pile_out, &C.fcount[po], &C.error_bits, V.U};
+          s_fmin_target[wib] = &C.fmin[po];
+        }
+        __syncwarp();
+      }
       if (n != 0u) {
         if (kChunked) {
-          frontier_flat<kCount, kItems, true, kPairs>(p, V, C, item, n, 32u, r & 1u, widx, tau, g % 3u, wk);
+          frontier_flat<kCount, kItems, true, kPairs>(p, V, C, item, n, 32u, tau, st, wk);
         } else if (p.flat) {
-          frontier_flat<kCount, kItems, false>(p, V, C, item, n, flat_entries_per_item(n), r & 1u, widx, tau, g % 3u, wk);
+          frontier_flat<kCount, kItems, false>(p, V, C, item, n, flat_entries_per_item(n), tau, st, wk);
         } else if (B.W <= 8u) {
           frontier_group<kCount, 8>(p, V, C, item, n, r & 1u, widx, tau, g % 3u, wk);
         } else {
           frontier_group<kCount, 32>(p, V, C, item, n, r & 1u, widx, tau, g % 3u, wk);
         }
       } else if (kChunked) {
-        split_group<kCount, true>(p, V, C, item, f, r & 1u, widx, tau_next, g % 3u, (g + 1u) % 3u, wk);
+        split_group<kCount, true>(p, V, C, item, f, tau_next, st, wk);
       } else {
-        split_group<kCount, false>(p, V, C, item, f, r & 1u, widx, tau_next, g % 3u, (g + 1u) % 3u, wk);
+        split_group<kCount, false>(p, V, C, item, f, tau_next, st, wk);
       }
     } else if (eng == BFX_ENGINE_JACOBI_PULL) {
       jacobi_item<kCount>(p, B, C, item, r, widx, wk);
@@ -434,6 +453,7 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
       dense_item<kCount>(p, B, C, item, batch_exec(p, b, ridx), widx, wk);
     }
   }
+  stages_flush(st);
 }
 
 // Bookkeeping at the start of round r, done by one thread: rounds counter
@@ -469,9 +489,37 @@ __device__ void round_bookkeeping(const LaunchParams& p, u32 r) {
   }
 }
 
+// Frontier batches whose round r is a near/far split round (round trace
+// only; reads slots that the bookkeeping of round r does not write).
+__device__ u32 split_batches(const LaunchParams& p, u32 r) {
+  u32 n = 0u;
+  for (u32 b = 0; b < p.nb; ++b) {
+    if (engine_of(p, b) != BFX_ENGINE_FRONTIER_PUSH) continue;
+    const DCtl& C = p.ctl[b];
+    const u32 g = dev::ld_cg(&C.gen[r & 1u]);
+    n += dev::ld_cg(&C.count[r % 3u]) == 0u && dev::ld_cg(&C.fcount[g % 3u]) != 0u;
+  }
+  return n;
+}
+
+// Round trace words 2 and 3: the active (vertex, lane) pairs and lane-edge
+// relaxations of round r, added per warp from the counters' growth since the
+// previous round.
+__device__ void trace_round_work(const LaunchParams& p, u32 r, const Work& wk, u64 (&traced)[2]) {
+  u64 x[2] = {wk.c[2] - traced[0], wk.c[3] - traced[1]};
+  traced[0] = wk.c[2];
+  traced[1] = wk.c[3];
+  for (int i = 0; i < 2; ++i) {
+    for (int o = 16; o > 0; o >>= 1) x[i] += __shfl_down_sync(0xFFFFFFFFu, x[i], o);
+    if (lane_id() == 0 && x[i]) {
+      atomicAdd(reinterpret_cast<unsigned long long*>(&p.round_trace[4u * r + 2u + i]), x[i]);
+    }
+  }
+}
+
 // Adds each thread's counters into the launch-wide totals.
 __device__ void flush_work(const LaunchParams& p, Work& wk) {
-  for (int i = 0; i < 11; ++i) {
+  for (int i = 0; i < kWorkCounters; ++i) {
     u64 x = wk.c[i];
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xFFFFFFFFu, x, o);
     const int slot = i < 7 ? i : i + 1;  // work[7] holds the round count
@@ -489,6 +537,7 @@ __global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParam
   const u32 nblocks = gridDim.x;
   Work wk;
   wk.zero();
+  u64 traced[2] = {0u, 0u};
   const u64 t0 = dev::global_ns();
   u32 r = 0;
   for (;; ++r) {
@@ -496,10 +545,11 @@ __global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParam
     if (total == 0u || r >= p.max_rounds) break;
     if (blockIdx.x == 0) round_bookkeeping(p, r);
     if (p.round_trace != nullptr && blockIdx.x == 0 && threadIdx.x == 0 && r < p.trace_cap) {
-      p.round_trace[2u * r] = dev::global_ns();
-      p.round_trace[2u * r + 1u] = total;
+      p.round_trace[4u * r] = dev::global_ns();
+      p.round_trace[4u * r + 1u] = total | (static_cast<u64>(split_batches(p, r)) << 32);
     }
     round_body<kCount, kItems, kChunked, kPairs>(p, r, prefix, wk);
+    if (kCount && p.round_trace != nullptr && r < p.trace_cap) trace_round_work(p, r, wk, traced);
     // Past the launch budget block 0 raises the barrier's abort before it
     // arrives, so every block leaves after this round.
     if (blockIdx.x == 0 && threadIdx.x == 0 && dev::global_ns() - t0 > p.budget_ns) {
@@ -1199,7 +1249,8 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   p.amin = ws->relax_atomic;
   p.edge_major = ws->edge_major;
   if (o.instrumentation == 2u && o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
-    ws->round_trace.reserve(size_t{kRoundTraceCap} * 16u, ws->graph->device);
+    ws->round_trace.reserve(size_t{kRoundTraceCap} * 32u, ws->graph->device);
+    BFX_CUDA(cudaMemsetAsync(ws->round_trace.ptr, 0, size_t{kRoundTraceCap} * 32u, ws->stream));
     p.round_trace = static_cast<u64*>(ws->round_trace.ptr);
     p.trace_cap = kRoundTraceCap;
   }
@@ -1486,7 +1537,7 @@ int bfx_fetch_round_trace(bfx_workspace* ws, uint32_t capacity, uint64_t* trace,
     *rounds = n;
     if (trace && capacity) {
       const std::uint32_t m = std::min(n, capacity);
-      BFX_CUDA(cudaMemcpy(trace, ws->round_trace.ptr, size_t{m} * 16u, cudaMemcpyDeviceToHost));
+      BFX_CUDA(cudaMemcpy(trace, ws->round_trace.ptr, size_t{m} * 32u, cudaMemcpyDeviceToHost));
     }
   });
 }

@@ -97,7 +97,7 @@ struct DRun {
   u32 abort;       // device failure seen
   u64 max_rounds;
   u64 launches;
-  u64 work[16];    // launch-wide work counters: [0..6] push engines, [7] rounds, [8..11] Jacobi
+  u64 work[16];    // launch-wide work counters: [0..6] push engines, [7] rounds, [8..11] Jacobi, [12..13] splits
 };
 
 // Work counters of an instrumented run (instrumentation >= 1):
@@ -107,11 +107,13 @@ struct DRun {
 // Per-thread work counters of an instrumented run: c[0..6] frontier and
 // dense push (entries / vertex items, edge records, source reads, lane-edge
 // relaxations, queue claims, decreases, min-reductions), c[7..10] Jacobi
-// pull (vertex-lane items, in-edge records, relaxations, changes).
+// pull (vertex-lane items, in-edge records, relaxations, changes), c[11..12]
+// near/far split rounds (far pile entries scanned, parked lanes re-read).
+constexpr int kWorkCounters = 13;
 struct Work {
-  u64 c[11];
+  u64 c[kWorkCounters];
   __device__ void zero() {
-    for (int i = 0; i < 11; ++i) c[i] = 0;
+    for (int i = 0; i < kWorkCounters; ++i) c[i] = 0;
   }
 };
 
@@ -133,7 +135,8 @@ struct LaunchParams {
   u64 budget_ns;         // wall-clock budget of one relaxation launch; past it the launch stops (device_failure)
   const u32* engines;    // [nb] per-batch engine (autotuned launches) or null
   const u32* deltas;     // [nb] near/far threshold steps (float bits) or null (plain frontier)
-  u64* round_trace;      // instrumentation 2: per round {start %globaltimer, warp items}; null otherwise
+  u64* round_trace;      // instrumentation 2: per round {start %globaltimer, warp items | split batches << 32,
+                         // active pairs, lane-edge relaxations}; null otherwise
   u32 trace_cap;         // rounds the trace holds
   u32 amin;              // flat frontier: 1 = returning min per relaxation, 0 = pre-read + min on success
   u32 edge_major;        // flat frontier work order: 1 = entry, edge, lane; 0 = entry, lane, edge
@@ -255,9 +258,9 @@ struct bfx_workspace {
   std::vector<std::uint32_t> batch_engines;  // per-batch engine for BFX_ENGINE_AUTO launches
   std::vector<float> batch_deltas;           // per-batch near/far steps (empty: plain frontier)
   std::uint32_t frontier_layout = 2;         // BFX_FRONTIER_CHUNKED (default) / _FLAT / _GROUPS
-  std::uint32_t relax_atomic = 0;
-  std::uint32_t edge_major = 0;
-  std::uint32_t chunk_pairs = 0;             // chunked frontier pair mode (see bfx_set_chunk_pairs)              // flat frontier work order (see bfx_set_flat_order)            // flat frontier relaxation: 0 pre-read + min, 1 returning min
+  std::uint32_t relax_atomic = 0;            // flat frontier relaxation: 0 pre-read + min, 1 returning min
+  std::uint32_t edge_major = 0;              // flat frontier work order (see bfx_set_flat_order)
+  std::uint32_t chunk_pairs = 0;             // chunked frontier pair mode (see bfx_set_chunk_pairs)
   std::uint32_t flat_items = 2;              // flat layout: work items per thread per iteration (2..4)
   std::uint32_t register_budget = 64;        // persistent kernel: 64 (default) or 40 registers per thread
   bfx::DeviceBuffer deltas_dev;

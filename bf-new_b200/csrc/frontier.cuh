@@ -62,6 +62,83 @@ __device__ __forceinline__ FrontierView frontier_view(const DBatch& b, u32 rd, u
   return v;
 }
 
+// Claims staged per warp in shared memory and appended to their queue with
+// one atomicAdd per 32 or more entries.  A stage lives for the warp's items
+// of one (round, batch) -- round_body flushes it when the warp moves on to
+// another batch and at the end of the round -- so the queue counters, one
+// address per batch that every warp appends to, see one atomic per 32
+// claims instead of one per warp step.  Two stages per warp: kNear (the next
+// round's queue) and kFar (the far pile).  The buffers and the queue
+// descriptors live in shared memory; a thread keeps only the warp-uniform
+// entry counts in registers.
+constexpr u32 kStage = 64;  // entries per warp stage: < 32 before a push adds <= 32
+constexpr u32 kNear = 0u, kFar = 1u;
+
+struct StageQueue {
+  u64* queue;
+  u32* counter;  // queue size
+  u32* err;      // the batch's error bits (queue overflow)
+  u32 cap;       // queue capacity (the batch's union vertex count)
+};
+
+__shared__ u64 s_stage_buf[2][16][kStage];  // blocks of up to 512 threads
+__shared__ StageQueue s_stage_queue[2][16];
+__shared__ u32* s_fmin_target[16];           // FarMin: fmin of the pile the warp parks on
+
+struct Stages {
+  u32 n[2];  // staged entries per stage (warp-uniform)
+  u32 fd;    // smallest parked distance seen by this thread (FarMin)
+};
+
+// Executed by all 32 threads.
+__device__ __forceinline__ void stage_flush(Stages& st, u32 k) {
+  if (st.n[k] == 0u) return;  // warp-uniform
+  const u32 wib = threadIdx.x >> 5;
+  const StageQueue q = s_stage_queue[k][wib];
+  __syncwarp();
+  const u32 lane = lane_id();
+  u32 pos = 0u;
+  if (lane == 0u) pos = atomicAdd(q.counter, st.n[k]);
+  pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
+  for (u32 i = lane; i < st.n[k]; i += 32u) {
+    if (pos + i < q.cap) {
+      q.queue[pos + i] = s_stage_buf[k][wib][i];
+    } else {
+      atomicOr(q.err, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
+    }
+  }
+  __syncwarp();
+  st.n[k] = 0u;
+}
+
+// Appends the claiming threads' queue words to stage k; flushes at >= 32
+// staged.  Executed by all 32 threads.
+__device__ __forceinline__ void stage_push(Stages& st, u32 k, bool claim, u64 word) {
+  const u32 lane = lane_id();
+  const u32 cm = __ballot_sync(0xFFFFFFFFu, claim);
+  if (claim) s_stage_buf[k][threadIdx.x >> 5][st.n[k] + __popc(cm & ((1u << lane) - 1u))] = word;
+  st.n[k] += static_cast<u32>(__popc(cm));
+  if (st.n[k] >= 32u) stage_flush(st, k);
+}
+
+// Folds the threads' smallest parked distances into the pile's fmin (one
+// atomicMin per warp and (round, batch)).  Executed by all 32 threads.
+__device__ __forceinline__ void farmin_flush(Stages& st) {
+  const u32 x = __reduce_min_sync(0xFFFFFFFFu, st.fd);
+  if (lane_id() == 0u && x != 0xFFFFFFFFu) atomicMin(s_fmin_target[threadIdx.x >> 5], x);
+  st.fd = 0xFFFFFFFFu;
+}
+
+__device__ __forceinline__ void stages_flush(Stages& st) {
+  stage_flush(st, kNear);
+  stage_flush(st, kFar);
+  farmin_flush(st);
+}
+
+__device__ __forceinline__ u64 queue_word(u32 v, u32 cv) {
+  return static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
+}
+
 template <bool kCount, u32 S>
 __device__ __forceinline__ void frontier_group(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
                                                u32 rd, u32 widx, u32 tau_bits, u32 pile, Work& wk) {
@@ -212,7 +289,7 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const Fron
 // stable and are cleared with plain stores.
 template <bool kCount, bool kChunked>
 __device__ __forceinline__ void split_group(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
-                                            u32 rd, u32 widx, u32 tau_next, u32 pile_in, u32 pile_out, Work& wk) {
+                                            u32 tau_next, Stages& st, Work& wk) {
   const u32 lane = lane_id();
   const u32 entry = item * 32u + lane;
   u32 near = 0u, far = 0u, v = 0u, cv = 0u, fd = 0xFFFFFFFFu;
@@ -227,22 +304,41 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const Frontie
     } else {
       atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
     }
-    for (u32 m = bits; m != 0u; m &= m - 1u) {
-      const u32 l = __ffs(m) - 1u;
-      const u32 d = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(cv) << B.shift) + l)));
-      if (d < tau_next) {
-        near |= 1u << l;
-      } else {
-        far |= 1u << l;
-        fd = min(fd, d);
+    // Parked lanes are re-read eight at a time: the eight label loads are
+    // issued back to back, so an entry with k far lanes waits ceil(k / 8)
+    // memory latencies instead of k.
+    u64* const row = B.dist + (static_cast<u64>(cv) << B.shift);
+    for (u32 rest = bits; rest != 0u;) {
+      u32 ls[8], ds[8];
+#pragma unroll
+      for (u32 i = 0; i < 8u; ++i) {
+        ls[i] = rest != 0u ? static_cast<u32>(__ffs(rest)) - 1u : 32u;
+        rest &= rest - 1u;
+      }
+#pragma unroll
+      for (u32 i = 0; i < 8u; ++i) ds[i] = ls[i] < 32u ? dev::hi(dev::ld_cg(row + ls[i])) : 0u;
+#pragma unroll
+      for (u32 i = 0; i < 8u; ++i) {
+        if (ls[i] < 32u) {
+          if (ds[i] < tau_next) {
+            near |= 1u << ls[i];
+          } else {
+            far |= 1u << ls[i];
+            fd = min(fd, ds[i]);
+          }
+        }
       }
     }
-    if (kCount) wk.c[0] += 1;
+    if (kCount) {
+      wk.c[0] += 1;
+      wk.c[11] += 1;
+      wk.c[12] += static_cast<u32>(__popc(bits));
+    }
   }
   // far lanes stay parked (next pile); near lanes join the next round
   bool fclaim = false, claim = false;
   if (far != 0u) fclaim = atomicOr(B.fmask + cv, far) == 0u;
-  u32 qword = v;  // queue word: the vertex, or its chunk (chunked layout)
+  u64 qword = queue_word(v, cv);  // queue word: {vertex, compact index}, or the chunk (chunked layout)
   if (near != 0u) {
     if (kChunked) {
       dev::red_or(B.mask_w + cv, near);
@@ -254,60 +350,10 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const Frontie
       claim = atomicOr(B.mask_w + cv, near) == 0u;
     }
   }
-  fd = __reduce_min_sync(0xFFFFFFFFu, fd);
-  if (lane == 0u && fd != 0xFFFFFFFFu) atomicMin(&C.fmin[pile_out], fd);
-  const u32 fm = __ballot_sync(0xFFFFFFFFu, fclaim);
-  if (fm != 0u) {
-    const u32 first = __ffs(fm) - 1u;
-    u32 pos = 0u;
-    if (lane == first) pos = atomicAdd(&C.fcount[pile_out], static_cast<u32>(__popc(fm)));
-    pos = __shfl_sync(0xFFFFFFFFu, pos, static_cast<int>(first));
-    if (fclaim) {
-      const u32 at = pos + __popc(fm & ((1u << lane) - 1u));
-      if (at < B.U) B.pile_out[at] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
-      else atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
-    }
-  }
-  const u32 cm = __ballot_sync(0xFFFFFFFFu, claim);
-  if (cm != 0u) {
-    const u32 first = __ffs(cm) - 1u;
-    u32 pos = 0u;
-    if (lane == first) pos = atomicAdd(&C.count[widx], static_cast<u32>(__popc(cm)));
-    pos = __shfl_sync(0xFFFFFFFFu, pos, static_cast<int>(first));
-    if (claim) {
-      if (kCount) wk.c[4] += 1;
-      const u32 at = pos + __popc(cm & ((1u << lane) - 1u));
-      if (at < B.U) {
-        B.queue_w[at] = kChunked ? static_cast<u64>(qword) : static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
-      } else {
-        atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
-      }
-    }
-  }
-}
-
-// Warp-aggregated enqueue: the threads with `claim` set take consecutive
-// slots of `queue` from one atomicAdd on `*counter`; a slot beyond the batch
-// capacity raises queue_overflow.  Executed by all 32 threads.
-template <bool kCount>
-__device__ __forceinline__ void enqueue_claims(bool claim, u32 v, u32 cv, u32* counter, u64* queue, const FrontierView& B,
-                                               DCtl& C, bool near, Work& wk) {
-  const u32 lane = lane_id();
-  const u32 cm = __ballot_sync(0xFFFFFFFFu, claim);
-  if (cm == 0u) return;  // warp-uniform
-  const u32 first = __ffs(cm) - 1u;
-  u32 pos = 0u;
-  if (lane == first) pos = atomicAdd(counter, static_cast<u32>(__popc(cm)));
-  pos = __shfl_sync(0xFFFFFFFFu, pos, static_cast<int>(first));
-  if (claim) {
-    if (kCount && near) wk.c[4] += 1;
-    const u32 at = pos + __popc(cm & ((1u << lane) - 1u));
-    if (at < B.U) {
-      queue[at] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
-    } else {
-      atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
-    }
-  }
+  st.fd = min(st.fd, fd);
+  stage_push(st, kFar, fclaim, queue_word(v, cv));
+  if (kCount && claim) wk.c[4] += 1;
+  stage_push(st, kNear, claim, qword);
 }
 
 // Entries per flat warp item for a batch frontier of n entries: 32 from 2,048
@@ -329,20 +375,15 @@ __device__ __forceinline__ u32 flat_entries_per_item(u32 n) {
 // so each thread keeps two dependent chains in flight.  A thread finds the
 // entry of a work item by a binary search over the warp's inclusive work scan
 // (five shuffles).  Every thread ORs its own success into the next round's
-// pending word; the OR that turns the word non-zero claims the vertex.  The
-// ORs' results are read one iteration later (after the next items' first
-// loads are issued), and claimed vertices are staged in the warp's
-// shared-memory buffer and written to the next queue with one counter atomic
-// per 32 or more claims, off the per-step chain.  All loops are warp-uniform.
-constexpr u32 kStage = 64;  // staged claims per warp: < 32 before a call adds <= 32
-
-template <u32 N>
-__device__ __forceinline__ bool any_far(const u32 (&f)[N]) {
-  u32 x = 0u;
-#pragma unroll
-  for (u32 u = 0; u < N; ++u) x |= f[u];
-  return x != 0u;
-}
+// pending word; the OR that turns the word non-zero claims the vertex.  A
+// far success (near/far frontier) ORs its lane into the far mask the same
+// way and the OR that turns it non-zero parks the vertex on the far pile;
+// the smallest parked distance is kept per thread (FarMin).  The ORs'
+// results are read one iteration later (after the next items' first loads
+// are issued), and claimed vertices are staged in the warp's shared-memory
+// stages (Stage) and appended to the next queue or the far pile with one
+// counter atomic per 32 or more claims, off the per-step chain.  All loops
+// are warp-uniform.
 
 struct FlatItem {
   bool live;
@@ -383,35 +424,6 @@ __device__ __forceinline__ FlatItem flat_decode(u32 w, u32 total, u32 incl, u32 
   return it;
 }
 
-// Appends the claiming threads' vertices to the warp's stage; flushes the
-// stage to `queue` (one atomicAdd on `counter`) once it holds >= 32 entries,
-// or whenever `final` is set.  Executed by all 32 threads.
-template <bool kCount>
-__device__ __forceinline__ void stage_claims(bool claim, u32 v, u32 cv, u64* stage, u32& n, bool final, u32* counter,
-                                             u64* queue, const FrontierView& B, DCtl& C, Work& wk) {
-  const u32 lane = lane_id();
-  const u32 cm = __ballot_sync(0xFFFFFFFFu, claim);
-  if (claim) {
-    stage[n + __popc(cm & ((1u << lane) - 1u))] = static_cast<u64>(v) | (static_cast<u64>(cv) << 32);
-    if (kCount) wk.c[4] += 1;
-  }
-  n += static_cast<u32>(__popc(cm));
-  if (n == 0u || (n < 32u && !final)) return;  // warp-uniform
-  __syncwarp();
-  u32 pos = 0u;
-  if (lane == 0u) pos = atomicAdd(counter, n);
-  pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
-  for (u32 i = lane; i < n; i += 32u) {
-    if (pos + i < B.U) {
-      queue[pos + i] = stage[i];
-    } else {
-      atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
-    }
-  }
-  __syncwarp();
-  n = 0u;
-}
-
 // kChunked: the item is one queued 32-vertex chunk (compact indices
 // 32 c .. 32 c + 31) instead of `epi` queued vertices; successes set the
 // pending lane with a non-returning OR and claim the target's chunk through
@@ -420,10 +432,7 @@ __device__ __forceinline__ void stage_claims(bool claim, u32 v, u32 cv, u64* sta
 // per thread, each over its entry's out-edges -- no per-edge decode.
 template <bool kCount, u32 kItems, bool kChunked, bool kPairs = false>
 __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
-                                              u32 epi, u32 rd, u32 widx, u32 tau_bits, u32 pile, Work& wk) {
-  __shared__ u64 s_stage[16][kStage];  // blocks of up to 512 threads
-  u64* const stage = s_stage[threadIdx.x >> 5];
-  u32 staged = 0u;
+                                              u32 epi, u32 tau_bits, Stages& st, Work& wk) {
   const u32 lane = lane_id();
   const u32 entry = item * epi + lane;  // epi entries per item (a power of two <= 32)
   u32 v = 0u, cv = 0u, m = 0u, rb = 0u, deg = 0u;
@@ -468,21 +477,21 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
       wk.c[2] += __popc(m);
     }
   }
-  // Claims of the previous step: their pending-word ORs stay in flight
-  // while the next step decodes its items and issues its first loads.
-  u32 p_old[kItems], p_v[kItems], p_cv[kItems];
+  // Claims of the previous step: their pending-word and far-mask ORs stay
+  // in flight while the next step decodes its items and issues its first
+  // loads.  p_old / f_old == 0: the OR claimed the vertex (or its chunk).
+  u32 p_old[kItems], p_v[kItems], p_cv[kItems], f_old[kItems], f_v[kItems], f_cv[kItems];
   u32 known_chunk = 0xFFFFFFFFu;  // chunked layout: last chunk whose bit this thread ORed
 #pragma unroll
   for (u32 u = 0; u < kItems; ++u) {
-    p_old[u] = 1u;
-    p_v[u] = p_cv[u] = 0u;
+    p_old[u] = f_old[u] = 1u;
+    p_v[u] = p_cv[u] = f_v[u] = f_cv[u] = 0u;
   }
   // One step: kItems (lane, edge) items per thread, memory phases interleaved.
   auto step = [&](const FlatItem (&it)[kItems], u32 (&src)[kItems], bool load_src) {
     u32 bits[kItems], fbits[kItems], cdst[kItems], dstv[kItems];
     uint4 rec[kItems];
     uint2 dt[kItems];
-    u32 fd = 0xFFFFFFFFu;
 #pragma unroll
     for (u32 u = 0; u < kItems; ++u) bits[u] = fbits[u] = cdst[u] = dstv[u] = 0u;
 #pragma unroll
@@ -494,8 +503,9 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
     }
 #pragma unroll
     for (u32 u = 0; u < kItems; ++u) {
-      stage_claims<kCount>(p_old[u] == 0u, p_v[u], p_cv[u], stage, staged, false, &C.count[widx], B.queue_w, B, C,
-                           wk);
+      if (kCount && p_old[u] == 0u) wk.c[4] += 1;
+      stage_push(st, kNear, p_old[u] == 0u, queue_word(p_v[u], p_cv[u]));
+      stage_push(st, kFar, f_old[u] == 0u, queue_word(kChunked ? f_cv[u] : f_v[u], f_cv[u]));
     }
 #pragma unroll
     for (u32 u = 0; u < kItems; ++u) {
@@ -529,7 +539,7 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
               bits[u] = 1u << it[u].ql;
             } else {
               fbits[u] = 1u << it[u].ql;
-              fd = min(fd, dev::hi(cand[u]));
+              st.fd = min(st.fd, dev::hi(cand[u]));
             }
           }
           if (kCount) {
@@ -539,17 +549,14 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
         }
       }
     }
-    if (__any_sync(0xFFFFFFFFu, any_far(fbits))) {
-      fd = __reduce_min_sync(0xFFFFFFFFu, fd);
-      if (lane == 0u) atomicMin(&C.fmin[pile], fd);
+    // the far-mask and pending-word ORs are issued here; their results are
+    // read by the next iteration (or after the loop)
 #pragma unroll
-      for (u32 u = 0; u < kItems; ++u) {
-        const bool fclaim = fbits[u] != 0u && atomicOr(B.fmask + cdst[u], fbits[u]) == 0u;
-        enqueue_claims<kCount>(fclaim, dstv[u], cdst[u], &C.fcount[pile], B.pile, B, C, false, wk);
-      }
+    for (u32 u = 0; u < kItems; ++u) {
+      f_old[u] = fbits[u] != 0u ? atomicOr(B.fmask + cdst[u], fbits[u]) : 1u;
+      if (!kChunked) f_v[u] = dstv[u];  // the chunked layout's split rounds read only the compact index
+      f_cv[u] = cdst[u];
     }
-    // both pending-word ORs are issued here; their results are read by the
-    // next iteration (or after the loop)
 #pragma unroll
     for (u32 u = 0; u < kItems; ++u) {
       if (kChunked) {
@@ -640,7 +647,8 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
   }
 #pragma unroll
   for (u32 u = 0; u < kItems; ++u) {
-    stage_claims<kCount>(p_old[u] == 0u, p_v[u], p_cv[u], stage, staged, u == kItems - 1u, &C.count[widx], B.queue_w, B, C,
-                         wk);
+    if (kCount && p_old[u] == 0u) wk.c[4] += 1;
+    stage_push(st, kNear, p_old[u] == 0u, queue_word(p_v[u], p_cv[u]));
+    stage_push(st, kFar, f_old[u] == 0u, queue_word(kChunked ? f_cv[u] : f_v[u], f_cv[u]));
   }
 }

@@ -352,12 +352,16 @@ int bfx_fetch_work_statistics(bfx_workspace *ws, bfx_device_work_statistics *sta
 /* The same counters split by engine (bfx extension, for per-engine
  * algorithmic byte counts): [0..6] frontier and dense push in the order
  * above, [7] rounds, [8..11] Jacobi pull {vertex-lane items, in-edge records,
- * relaxations, changes}, [12..15] zero. */
+ * relaxations, changes}, [12..13] near/far split rounds {far pile entries
+ * scanned (also counted in [0]), parked lanes re-read}, [14..15] zero. */
 int bfx_fetch_engine_work(bfx_workspace *ws, uint64_t counters[16]);
 /* Round trace of the most recent persistent run with instrumentation 2 (bfx
- * extension): per round {%globaltimer ns at the round's start, warp items of
- * the round}, up to 65,536 rounds; *rounds = rounds executed.  trace may be
- * NULL to query the count. */
+ * extension): per round four words {%globaltimer ns at the round's start,
+ * warp items of the round in the low 32 bits | frontier batches in a near/far
+ * split round in the high 32 bits, active (vertex, lane) source reads of the
+ * round, lane-edge relaxations of the round}, up to 65,536 rounds; capacity
+ * counts rounds (4 words each); *rounds = rounds executed.  trace may be NULL
+ * to query the count. */
 int bfx_fetch_round_trace(bfx_workspace *ws, uint32_t capacity, uint64_t *trace, uint32_t *rounds);
 
 /* ---- plain per-query engine ----------------------------------------------

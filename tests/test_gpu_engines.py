@@ -346,9 +346,10 @@ def test_plain_query_after_autotune_ignores_batch_settings(gpu):
 
 
 def test_round_trace_at_debug_instrumentation(gpu, c1):
-    """instrumentation 2 records one {start time, warp items} pair per round
-    of a persistent launch: as many rounds as the work counters report, start
-    times non-decreasing, every traced round with work."""
+    """instrumentation 2 records one {start time, warp items | split batches,
+    pairs, relaxations} record per round of a persistent launch: as many
+    rounds as the work counters report, start times non-decreasing, every
+    traced round with work, per-round work summing to the launch totals."""
     d = bfx.make_description(c1.layout, c1.queries, 8)
     res = bfx.ResidentDeviceGraph.upload_once(c1.layout)
     ws = bfx.Workspace(res)
@@ -359,7 +360,22 @@ def test_round_trace_at_debug_instrumentation(gpu, c1):
     tr = ws.round_trace()
     assert tr.shape[0] == ws.work_counters()["rounds"] > 0
     assert np.all(np.diff(tr[:, 0].astype(np.int64)) >= 0)
-    assert np.all(tr[:, 1] > 0)
+    assert np.all((tr[:, 1] & 0xFFFFFFFF) > 0)
+    assert np.all((tr[:, 1] >> 32) == 0)  # plain frontier: no split rounds
+    assert ws.engine_work()["split"] == {"entries": 0, "lanes": 0}
+    w = ws.work_counters()
+    assert int(tr[:, 2].sum()) == w["active_pairs"] and int(tr[:, 3].sum()) == w["relaxations"]
+    # near/far frontier: split rounds are marked with their batch count and
+    # the split counters see the far pile
+    ws.set_batch_deltas([0.5 * float(np.mean(c1.layout.arrays["csr_weights"]))])
+    ws.execute(bfx.GpuRunOptions(engine=bfx.ENGINE_AUTO, instrumentation=2))
+    assert ws.fetch_statuses()[0].stop_reason == bfx.STOP_CONVERGED
+    tr = ws.round_trace()
+    splits = tr[:, 1] >> 32
+    assert np.all(splits <= 1) and splits.sum() > 0
+    assert np.all((tr[:, 1] & 0xFFFFFFFF) > 0)
+    sw = ws.engine_work()["split"]
+    assert sw["entries"] > 0 and sw["lanes"] >= sw["entries"]
     ws.close()
     res.close()
 
