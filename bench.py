@@ -50,12 +50,16 @@ def log(*a):
 
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) during the timed region."""
+    """nvidia-smi samples (every 50 ms) during the timed region.  Entering
+    waits (up to 5 s) for the sampler's first line, so sampling is running
+    when the timed region starts; only lines read inside the region count."""
 
     def __init__(self, device: int):
         self.device = device
         self.samples = []
         self._proc = None
+        self._first = threading.Event()
+        self._keep = False
 
     def __enter__(self):
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
@@ -63,21 +67,26 @@ class ClockSampler:
              "clocks_event_reasons.sw_power_cap")
         try:
             self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
-                                           "--format=csv,noheader,nounits", "-lms", "200"],
+                                           "--format=csv,noheader,nounits", "-lms", "50"],
                                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            self._first.wait(timeout=5.0)
         except FileNotFoundError:
             self._proc = None
+        self._keep = True
         return self
 
     def _read(self):
         for line in self._proc.stdout:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) >= 7:
-                self.samples.append(parts)
+                self._first.set()
+                if self._keep:
+                    self.samples.append(parts)
 
     def __exit__(self, *exc):
+        self._keep = False
         if self._proc:
             self._proc.terminate()
             try:
@@ -179,8 +188,8 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5", "c3small"])
     ap.add_argument("--frontier", default="chunked", choices=["groups", "flat", "chunked"],
                     help="frontier-push work layout (sub-warp groups or flat work list)")
-    ap.add_argument("--regs", type=int, default=64, choices=[40, 64],
-                    help="register budget of the persistent kernel")
+    ap.add_argument("--regs", type=int, default=0, choices=[0, 40, 64, 80],
+                    help="register budget of the persistent kernel (0: 80 for the chunked layout, else 64)")
     ap.add_argument("--items", type=int, default=2, choices=[2, 3, 4],
                     help="flat layout: work items per thread per iteration")
     ap.add_argument("--policy", default=None,
@@ -191,6 +200,8 @@ def main():
                     help="flat/chunked work order: 1 = entry, edge, lane")
     ap.add_argument("--pairs", type=int, default=0, choices=[0, 1],
                     help="chunked frontier: 1 = one (vertex, lane) pair per thread")
+    ap.add_argument("--step", type=float, default=None,
+                    help="with --engine frontier: near/far threshold step in mean edge weights (0 = plain frontier)")
     ap.add_argument("--tune-policy", action="store_true",
                     help="choose the planner policy by timing each candidate's plan (bfx_autotune_policy)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -270,6 +281,10 @@ def main():
     ws.set_frontier_layout({"flat": bfx.FRONTIER_FLAT, "groups": bfx.FRONTIER_GROUPS,
                             "chunked": bfx.FRONTIER_CHUNKED}[args.frontier])
     ws.set_register_budget(args.regs)
+    # the budget the library applies (blocks of 256 threads)
+    eff_regs = args.regs or (80 if args.frontier == "chunked" else 64)
+    if args.frontier != "chunked" and eff_regs == 80:
+        eff_regs = 64
     ws.set_flat_items(args.items)
     ws.set_relax_atomic(args.amin)
     ws.set_flat_order(args.edge_major)
@@ -295,6 +310,10 @@ def main():
         engines_chosen, measured = ws.autotune(descs)
         log(f"[bench] autotune {time.time() - t3:.1f}s ({measured} batches timed): "
             f"{ {e: engines_chosen.count(e) for e in set(engines_chosen)} } (0 jacobi, 1 dense, 2 frontier)")
+    elif args.step is not None:
+        # fixed near/far step for every batch (profiling a chosen step)
+        wbar = float(np.mean(layout.arrays["csr_weights"]))
+        ws.set_batch_deltas([float("inf") if args.step == 0 else args.step * wbar] * len(descs))
     opts = bfx.GpuRunOptions(engine=engine_id)
     opts_instr = bfx.GpuRunOptions(engine=engine_id, instrumentation=1)
 
@@ -437,7 +456,8 @@ def main():
                    "planner_policy": [policy.minimum_jaccard_numerator, policy.minimum_jaccard_denominator,
                                       policy.maximum_union_inflation_numerator,
                                       policy.maximum_union_inflation_denominator],
-                   "frontier_layout": args.frontier, "registers": args.regs, "flat_items": args.items, "returning_min": args.amin, "edge_major": args.edge_major, "chunk_pairs": args.pairs,
+                   "near_far_step": args.step,
+                   "frontier_layout": args.frontier, "registers": eff_regs, "flat_items": args.items, "returning_min": args.amin, "edge_major": args.edge_major, "chunk_pairs": args.pairs,
                    "engines_chosen": None if engines_chosen is None else
                    {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
                    "frontier_steps_chosen": None if engines_chosen is None else
@@ -454,8 +474,8 @@ def main():
                             "layout": plain_layout, "by_layout": plain_by_layout,
                             "batched_speedup": value / world / plain_qps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_src, "kernel": "persistent_kernel<0, %d, %d> (%s frontier%s)" % (
-                         2 if args.regs == 64 else 3, args.items if args.regs == 64 else 2, args.frontier,
+                     "traffic": traffic, "peak_source": peak_src, "kernel": "persistent_kernel (%s frontier, %d registers, %d items%s)" % (
+                         args.frontier, eff_regs, 2 if args.frontier == "chunked" or eff_regs == 40 else args.items,
                          ", mixed engines" if engines_chosen and any(e != 2 for e in engines_chosen) else ""),
                      "kernel_ms": kernel_avg, "execute_ms": float(np.mean(execute_ms)),
                      "algorithmic_bytes_per_launch": alg_bytes, "work": work, "engine_work": engine_work},

@@ -569,7 +569,8 @@ class Workspace:
         _check(load().bfx_set_batch_deltas(self._h, u32(len(deltas)), arr))
 
     def set_register_budget(self, registers: int):
-        """40 (three 512-thread blocks per SM) or 64 registers per thread for the persistent kernel."""
+        """40 (three 512-thread blocks per SM), 64 or -- chunked layout, blocks of <= 256 threads -- 80
+        registers per thread for the persistent kernel."""
         _check(load().bfx_set_register_budget(self._h, u32(registers)))
 
     def set_chunk_pairs(self, mode: int):

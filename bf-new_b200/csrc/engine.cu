@@ -152,9 +152,14 @@ __global__ void init_kernel(LaunchParams p) {
     B.mask[0][cv] = 0u;
     B.mask[1][cv] = 0u;
     B.fmask[cv] = 0u;
-    if (p.flat == 2u && (cv & 1023u) == 0u) {  // chunk bitmap words, one per 1,024 vertices
-      B.cmask[0][cv >> 10] = 0u;
-      B.cmask[1][cv >> 10] = 0u;
+    if (p.flat == 2u) {
+      if ((cv & 1023u) == 0u) {  // chunk bitmap words, one per 1,024 vertices
+        B.cmask[0][cv >> 10] = 0u;
+        B.cmask[1][cv >> 10] = 0u;
+      }
+      const u32 v = r.y + (cv - B.range_off[lo]);
+      const u32 rb = p.g.csr_off[v];
+      B.crow[cv] = make_uint2(rb, p.g.csr_off[v + 1u] - rb);
     }
     for (u32 l = 0; l < B.W; ++l) {
       B.dist[0][(static_cast<u64>(cv) << B.shift) + l] = dev::kUnreached;
@@ -368,7 +373,7 @@ __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
       const DCtl& C = p.ctl[b];
       const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
       if (n != 0u) {  // warp items: one chunk (chunked), flat_entries_per_item(n) entries (flat), 4 or 1 entries
-        if (p.flat == 2u) return n;
+        if (p.flat == 2u) return chunk_items(n, B.U);
         return p.flat ? (n + flat_entries_per_item(n) - 1u) / flat_entries_per_item(n) : (B.W <= 8u ? (n + 3u) >> 2 : n);
       }
       const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
@@ -434,7 +439,15 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
       }
       if (n != 0u) {
         if (kChunked) {
-          frontier_flat<kCount, kItems, true, kPairs>(p, V, C, item, n, 32u, tau, st, wk);
+          u32 chunk = kNoChunk;  // sparse round: the item's queue word names the chunk
+          if (chunk_dense(n, V.U)) {
+            // dense round: the item is chunk slot `item`; clear bit, no work
+            // (every lane reads the same word, so the skip is warp-uniform)
+            const u32 word = dev::ld_cg(V.cmask_r + (item >> 5));
+            if (((word >> (item & 31u)) & 1u) == 0u) continue;
+            chunk = item;
+          }
+          frontier_flat<kCount, kItems, true, kPairs>(p, V, C, item, n, 32u, tau, st, wk, chunk);
         } else if (p.flat) {
           frontier_flat<kCount, kItems, false>(p, V, C, item, n, flat_entries_per_item(n), tau, st, wk);
         } else if (B.W <= 8u) {
@@ -528,11 +541,15 @@ __device__ void flush_work(const LaunchParams& p, Work& wk) {
 }
 
 // kMinBlocks = resident 512-thread blocks per SM the register budget is set
+// for, or kBlocks256x3 = three 256-thread blocks per SM (80 registers, 24
+// warps per SM; chunked layout only).
 // for: 3 -> 40 registers per thread (48 warps per SM), 2 -> 64 registers
 // (32 warps per SM; no spills in the group layout, a few in the flat one).
 // kItems = flat-layout work items per thread per iteration.
+constexpr int kBlocks256x3 = 5;
 template <bool kCount, int kMinBlocks, u32 kItems, bool kChunked = false, bool kPairs = false>
-__global__ void __launch_bounds__(512, kMinBlocks) persistent_kernel(LaunchParams p) {
+__global__ void __launch_bounds__(kMinBlocks == kBlocks256x3 ? 256 : 512, kMinBlocks == kBlocks256x3 ? 3 : kMinBlocks)
+    persistent_kernel(LaunchParams p) {
   extern __shared__ u32 prefix[];
   const u32 nblocks = gridDim.x;
   Work wk;
@@ -737,9 +754,6 @@ __global__ void expand_kernel(DGraph g, DBatch B, u32 slot, u32* bits, u32* pred
 
 namespace bfx {
 namespace {
-
-std::mutex g_graph_mutex;
-
 
 void upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   if (bytes) BFX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
@@ -1057,7 +1071,7 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
     for (std::uint32_t b = 0; b < count; ++b) {
       arena_off[b] = arena_total;
       const size_t U = sz[b].U;
-      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 4 + bfx::align256(U * 8) * 5 +
+      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 4 + bfx::align256(U * 8) * 6 +
                      bfx::align256((U + 1023) / 1024 * 4) * 2;
     }
     const size_t tiles_off = arena_total;
@@ -1140,6 +1154,8 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
         B.cmask[k] = reinterpret_cast<std::uint32_t*>(a);
         a += bfx::align256((U + 1023) / 1024 * 4);
       }
+      B.crow = reinterpret_cast<uint2*>(a);
+      a += bfx::align256(U * 8);
       B.tiles = reinterpret_cast<uint2*>(ab + tiles_off + tile_table_bytes * b);
       ubase[b] = static_cast<std::uint32_t>(usum);
       sbase[b] = static_cast<std::uint32_t>(ssum);
@@ -1206,8 +1222,14 @@ int grid_blocks(bfx_workspace* ws, const void* kernel, int block, size_t smem, c
 
 // Persistent kernel instantiation: 64 registers (two 512-thread blocks per
 // SM) with 2, 3 or 4 flat work items per thread, or 40 registers with 2;
-// the chunked layout has its own (64 registers, 2 items).
-const void* persistent_entry(bool count, bool wide, std::uint32_t items, bool chunked, bool pairs) {
+// the chunked layout has its own (64 registers, or 80 with blocks of at
+// most 256 threads; 2 items).
+const void* persistent_entry(bool count, std::uint32_t registers, std::uint32_t items, bool chunked, bool pairs) {
+  const bool wide = registers != 40u;
+  if (chunked && !pairs && registers == 80u) {
+    return count ? reinterpret_cast<const void*>(persistent_kernel<true, kBlocks256x3, 2, true>)
+                 : reinterpret_cast<const void*>(persistent_kernel<false, kBlocks256x3, 2, true>);
+  }
   if (chunked && pairs) {
     return count ? reinterpret_cast<const void*>(persistent_kernel<true, 2, 2, true, true>)
                  : reinterpret_cast<const void*>(persistent_kernel<false, 2, 2, true, true>);
@@ -1293,8 +1315,14 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   BFX_CUDA(cudaGetLastError());
   BFX_CUDA(cudaEventRecord(ws->ev[1], ws->stream));
   if (o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
-    const void* kfn = persistent_entry(o.instrumentation != 0u, ws->register_budget == 64u, ws->flat_items,
-                                       p.flat == 2u, ws->chunk_pairs != 0u);
+    // register budget 0 (default): 80 for the chunked layout with blocks of
+    // at most 256 threads, 64 otherwise
+    const std::uint32_t regs =
+        ws->register_budget != 0u ? ws->register_budget : (p.flat == 2u && block <= 256 ? 80u : 64u);
+    const void* kfn = persistent_entry(o.instrumentation != 0u, regs, ws->flat_items, p.flat == 2u,
+                                       ws->chunk_pairs != 0u);
+    require(!(regs == 80u && p.flat == 2u && ws->chunk_pairs == 0u) || block <= 256,
+            "the 80-register chunked kernel needs blocks of at most 256 threads");
     const int grid = grid_blocks(ws, kfn, block, smem, o);
     void* args[] = {&p};
     BFX_CUDA(cudaLaunchCooperativeKernel(kfn, grid, block, args, smem, ws->stream));
@@ -1388,7 +1416,8 @@ extern "C" {
 int bfx_set_register_budget(bfx_workspace* ws, uint32_t registers) {
   return bfx::guarded([&] {
     bfx::require(ws != nullptr, "null argument");
-    bfx::require(registers == 40u || registers == 64u, "register budget must be 40 or 64");
+    bfx::require(registers == 0u || registers == 40u || registers == 64u || registers == 80u,
+                 "register budget must be 0 (automatic), 40, 64 or 80");
     ws->register_budget = registers;
   });
 }

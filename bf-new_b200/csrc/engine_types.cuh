@@ -60,6 +60,7 @@ struct DBatch {
   u32* fmask;             // [U] far lanes (near/far frontier)
   u64* fpile[3];          // [U] far piles, rotating by far generation
   u32* cmask[2];          // [ceil(U/1024)] chunk bitmaps (chunked frontier): bit c = chunk c pending
+  uint2* crow;            // [U] {CSR row begin, out-degree} per compact vertex (chunked frontier)
 };
 
 struct DCtl {
@@ -262,7 +263,7 @@ struct bfx_workspace {
   std::uint32_t edge_major = 0;              // flat frontier work order (see bfx_set_flat_order)
   std::uint32_t chunk_pairs = 0;             // chunked frontier pair mode (see bfx_set_chunk_pairs)
   std::uint32_t flat_items = 2;              // flat layout: work items per thread per iteration (2..4)
-  std::uint32_t register_budget = 64;        // persistent kernel: 64 (default) or 40 registers per thread
+  std::uint32_t register_budget = 0;         // persistent kernel registers per thread: 0 automatic, 40, 64, 80
   bfx::DeviceBuffer deltas_dev;
   bfx::PinnedBuffer deltas_host;
   bfx::DeviceBuffer engines_dev;

@@ -35,8 +35,8 @@ struct FrontierView {
   u32* fmask;
   u64* pile;      // near round: far pile being filled; split round: pile read
   u64* pile_out;  // split round: pile written
-  const u32* c2g;  // compact index -> vertex id (chunked layout)
-  u32* cmask_r;    // chunk bitmaps (chunked layout): read and write slots
+  const uint2* crow;  // compact index -> {CSR row begin, out-degree} (chunked layout)
+  u32* cmask_r;       // chunk bitmaps (chunked layout): read and write slots
   u32* cmask_w;
   u32 shift, valid, U, full;
 };
@@ -52,7 +52,7 @@ __device__ __forceinline__ FrontierView frontier_view(const DBatch& b, u32 rd, u
   v.fmask = b.fmask;
   v.pile = b.fpile[pile];
   v.pile_out = b.fpile[pile_out];
-  v.c2g = b.c2g;
+  v.crow = b.crow;
   v.cmask_r = b.cmask[rd];
   v.cmask_w = b.cmask[rd ^ 1u];
   v.shift = b.shift;
@@ -427,25 +427,38 @@ __device__ __forceinline__ FlatItem flat_decode(u32 w, u32 total, u32 incl, u32 
 // kChunked: the item is one queued 32-vertex chunk (compact indices
 // 32 c .. 32 c + 31) instead of `epi` queued vertices; successes set the
 // pending lane with a non-returning OR and claim the target's chunk through
-// the chunk bitmap.
+// the chunk bitmap.  The chunk is the item's queue word, or `chunk_in`
+// when the caller enumerates chunk slots (dense rounds, chunk_items); the
+// pending lanes and the compact row table {row begin, out-degree} of its 32
+// vertices are read together.
 // kPairs (chunked only): the warp walks the item's (entry, lane) pairs, one
 // per thread, each over its entry's out-edges -- no per-edge decode.
+constexpr u32 kNoChunk = 0xFFFFFFFFu;
+
+// Chunked near round of a batch with n queued chunks: sparse rounds walk
+// the queue (claim order); once at least half of the batch's chunk slots are
+// pending, the items are all chunk slots in index order and a warp skips the
+// slots whose bit is clear.  Concurrent warps then relax neighbouring
+// chunks, whose target labels (intra-tile edges) are shared in the L2.
+__device__ __forceinline__ bool chunk_dense(u32 n, u32 U) { return 2u * n >= ((U + 31u) >> 5); }
+__device__ __forceinline__ u32 chunk_items(u32 n, u32 U) { return chunk_dense(n, U) ? (U + 31u) >> 5 : n; }
+
 template <bool kCount, u32 kItems, bool kChunked, bool kPairs = false>
 __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
-                                              u32 epi, u32 tau_bits, Stages& st, Work& wk) {
+                                              u32 epi, u32 tau_bits, Stages& st, Work& wk, u32 chunk_in = kNoChunk) {
   const u32 lane = lane_id();
   const u32 entry = item * epi + lane;  // epi entries per item (a power of two <= 32)
   u32 v = 0u, cv = 0u, m = 0u, rb = 0u, deg = 0u;
   if (kChunked) {
-    const u32 chunk = static_cast<u32>(dev::ld_cg(B.queue_r + item));
+    const u32 chunk = chunk_in != kNoChunk ? chunk_in : static_cast<u32>(dev::ld_cg(B.queue_r + item));
     if (chunk < (B.U + 31u) >> 5) {
       cv = (chunk << 5) + lane;
       if (cv < B.U) {
         m = dev::ld_cg(B.mask_r + cv) & B.valid;
-        v = __ldg(B.c2g + cv);
+        const uint2 row = __ldg(B.crow + cv);
         if (m != 0u) {
-          rb = __ldg(p.g.csr_off + v);
-          deg = __ldg(p.g.csr_off + v + 1u) - rb;
+          rb = row.x;
+          deg = row.y;
           B.mask_r[cv] = 0u;
           if (kCount) {
             wk.c[0] += 1;
@@ -501,11 +514,16 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
         rec[u] = __ldg(p.g.csr + it[u].ed);
       }
     }
+    bool any_claim = false;
 #pragma unroll
-    for (u32 u = 0; u < kItems; ++u) {
-      if (kCount && p_old[u] == 0u) wk.c[4] += 1;
-      stage_push(st, kNear, p_old[u] == 0u, queue_word(p_v[u], p_cv[u]));
-      stage_push(st, kFar, f_old[u] == 0u, queue_word(kChunked ? f_cv[u] : f_v[u], f_cv[u]));
+    for (u32 u = 0; u < kItems; ++u) any_claim |= p_old[u] == 0u || f_old[u] == 0u;
+    if (__any_sync(0xFFFFFFFFu, any_claim)) {  // claims are rare: one vote skips the stage pushes
+#pragma unroll
+      for (u32 u = 0; u < kItems; ++u) {
+        if (kCount && p_old[u] == 0u) wk.c[4] += 1;
+        stage_push(st, kNear, p_old[u] == 0u, queue_word(p_v[u], p_cv[u]));
+        stage_push(st, kFar, f_old[u] == 0u, queue_word(kChunked ? f_cv[u] : f_v[u], f_cv[u]));
+      }
     }
 #pragma unroll
     for (u32 u = 0; u < kItems; ++u) {

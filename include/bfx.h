@@ -305,8 +305,11 @@ enum { BFX_FRONTIER_GROUPS = 0, BFX_FRONTIER_FLAT = 1, BFX_FRONTIER_CHUNKED = 2 
 int bfx_set_frontier_layout(bfx_workspace *ws, uint32_t layout);
 /* Register budget of the persistent relaxation kernel (a bfx tuning option,
  * results unchanged): 40 registers per thread (three 512-thread blocks per
- * SM) or 64 (two blocks per SM, the default: no spills in the group layout,
- * few in the flat one). */
+ * SM), 64 (two 512-thread blocks per SM: no spills in the group layout, few
+ * in the flat one) or 80 (three 256-thread blocks per SM, blocks of at most
+ * 256 threads; the chunked layout only -- the other layouts keep 64).  0, the
+ * default, picks 80 for the chunked layout with blocks of at most 256
+ * threads and 64 otherwise. */
 int bfx_set_register_budget(bfx_workspace *ws, uint32_t registers);
 /* Flat layout, persistent control with the 64-register budget: work items
  * each thread keeps in flight per iteration, 2 (default), 3 or 4 -- more

@@ -282,17 +282,20 @@ def test_autotuner_with_near_far_candidates(gpu):
     res.close()
 
 
-@pytest.mark.parametrize("regs,items,amin,order,pairs", [(40, 2, 0, 0, 0), (64, 2, 0, 0, 0), (64, 3, 0, 0, 0),
-                                                         (64, 4, 0, 0, 0), (64, 2, 1, 0, 0), (64, 2, 0, 1, 0),
-                                                         (64, 2, 0, 0, 1)])
+@pytest.mark.parametrize("regs,items,amin,order,pairs,instr", [(40, 2, 0, 0, 0, 1), (64, 2, 0, 0, 0, 1),
+                                                               (64, 3, 0, 0, 0, 1), (64, 4, 0, 0, 0, 1),
+                                                               (64, 2, 1, 0, 0, 1), (64, 2, 0, 1, 0, 1),
+                                                               (64, 2, 0, 0, 1, 1), (64, 2, 0, 0, 0, 0),
+                                                               (80, 2, 0, 0, 0, 1), (80, 2, 0, 0, 0, 0)])
 @pytest.mark.parametrize("layout_kind", [bfx.FRONTIER_FLAT, bfx.FRONTIER_GROUPS, bfx.FRONTIER_CHUNKED],
                          ids=["flat", "groups", "chunked"])
 @pytest.mark.parametrize("step", [None, 3.0])
 @pytest.mark.parametrize("control", [bfx.CONTROL_PERSISTENT, bfx.CONTROL_PER_ROUND], ids=["persistent", "per_round"])
-def test_flat_frontier_layout_bit_exact(gpu, c1, step, control, layout_kind, regs, items, amin, order, pairs):
+def test_flat_frontier_layout_bit_exact(gpu, c1, step, control, layout_kind, regs, items, amin, order, pairs, instr):
     """The flat work-list frontier (32 entries per warp, (lane, edge) pairs
     walked 32 per step) gives the oracle's labels on full-graph W=8, regional
-    multi-batch W in {1, 8, 16, 32}, plain and near/far."""
+    multi-batch W in {1, 8, 16, 32}, plain and near/far, with the counting
+    (instr 1) and the production (instr 0) kernel instantiations."""
     layout = c1.layout
     d = bfx.make_description(layout, c1.queries, 8)
     layout2, grid = workloads.build_graph("c2", scale_tiles=(32, 32))
@@ -313,7 +316,7 @@ def test_flat_frontier_layout_bit_exact(gpu, c1, step, control, layout_kind, reg
         ws.prepare(descs)
         if step is not None:
             ws.set_batch_deltas([step] * len(descs))
-        ws.execute(bfx.GpuRunOptions(instrumentation=1, control_mode=control, maximum_rounds=1 << 20))
+        ws.execute(bfx.GpuRunOptions(instrumentation=instr, control_mode=control, maximum_rounds=1 << 20))
         st = ws.fetch_statuses()
         labels = [ws.download_labels(b, x.lane_width) for b, x in enumerate(descs)]
         check_batches(lay, descs, lanes, st, labels, Oracle.from_layout(lay))
