@@ -475,7 +475,8 @@ def main():
                             "batched_speedup": value / world / plain_qps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_src, "kernel": "persistent_kernel (%s frontier, %d registers, %d items%s)" % (
-                         args.frontier, eff_regs, 2 if args.frontier == "chunked" or eff_regs == 40 else args.items,
+                         args.frontier, eff_regs, args.items if (eff_regs == 64 and args.frontier != "chunked") or (
+                             eff_regs == 80 and args.frontier == "chunked" and not args.pairs) else 2,
                          ", mixed engines" if engines_chosen and any(e != 2 for e in engines_chosen) else ""),
                      "kernel_ms": kernel_avg, "execute_ms": float(np.mean(execute_ms)),
                      "algorithmic_bytes_per_launch": alg_bytes, "work": work, "engine_work": engine_work},

@@ -504,15 +504,16 @@ __device__ void round_bookkeeping(const LaunchParams& p, u32 r) {
 
 // Frontier batches whose round r is a near/far split round (round trace
 // only; reads slots that the bookkeeping of round r does not write).
+// Executed by one whole warp, lanes striding over the batches.
 __device__ u32 split_batches(const LaunchParams& p, u32 r) {
   u32 n = 0u;
-  for (u32 b = 0; b < p.nb; ++b) {
+  for (u32 b = lane_id(); b < p.nb; b += 32u) {
     if (engine_of(p, b) != BFX_ENGINE_FRONTIER_PUSH) continue;
     const DCtl& C = p.ctl[b];
     const u32 g = dev::ld_cg(&C.gen[r & 1u]);
     n += dev::ld_cg(&C.count[r % 3u]) == 0u && dev::ld_cg(&C.fcount[g % 3u]) != 0u;
   }
-  return n;
+  return __reduce_add_sync(0xFFFFFFFFu, n);
 }
 
 // Round trace words 2 and 3: the active (vertex, lane) pairs and lane-edge
@@ -561,9 +562,13 @@ __global__ void __launch_bounds__(kMinBlocks == kBlocks256x3 ? 256 : 512, kMinBl
     const u32 total = round_work(p, r, prefix);
     if (total == 0u || r >= p.max_rounds) break;
     if (blockIdx.x == 0) round_bookkeeping(p, r);
-    if (p.round_trace != nullptr && blockIdx.x == 0 && threadIdx.x == 0 && r < p.trace_cap) {
-      p.round_trace[4u * r] = dev::global_ns();
-      p.round_trace[4u * r + 1u] = total | (static_cast<u64>(split_batches(p, r)) << 32);
+    if (p.round_trace != nullptr && blockIdx.x == 0 && threadIdx.x < 32u && r < p.trace_cap) {
+      const u64 t = dev::global_ns();
+      const u32 splits = split_batches(p, r);
+      if (threadIdx.x == 0u) {
+        p.round_trace[4u * r] = t;
+        p.round_trace[4u * r + 1u] = total | (static_cast<u64>(splits) << 32);
+      }
     }
     round_body<kCount, kItems, kChunked, kPairs>(p, r, prefix, wk);
     if (kCount && p.round_trace != nullptr && r < p.trace_cap) trace_round_work(p, r, wk, traced);
@@ -1222,11 +1227,19 @@ int grid_blocks(bfx_workspace* ws, const void* kernel, int block, size_t smem, c
 
 // Persistent kernel instantiation: 64 registers (two 512-thread blocks per
 // SM) with 2, 3 or 4 flat work items per thread, or 40 registers with 2;
-// the chunked layout has its own (64 registers, or 80 with blocks of at
-// most 256 threads; 2 items).
+// the chunked layout has its own: 64 registers with 2 items, or 80 (blocks
+// of at most 256 threads) with 2, 3 or 4.
 const void* persistent_entry(bool count, std::uint32_t registers, std::uint32_t items, bool chunked, bool pairs) {
   const bool wide = registers != 40u;
   if (chunked && !pairs && registers == 80u) {
+    if (items == 3u) {
+      return count ? reinterpret_cast<const void*>(persistent_kernel<true, kBlocks256x3, 3, true>)
+                   : reinterpret_cast<const void*>(persistent_kernel<false, kBlocks256x3, 3, true>);
+    }
+    if (items == 4u) {
+      return count ? reinterpret_cast<const void*>(persistent_kernel<true, kBlocks256x3, 4, true>)
+                   : reinterpret_cast<const void*>(persistent_kernel<false, kBlocks256x3, 4, true>);
+    }
     return count ? reinterpret_cast<const void*>(persistent_kernel<true, kBlocks256x3, 2, true>)
                  : reinterpret_cast<const void*>(persistent_kernel<false, kBlocks256x3, 2, true>);
   }

@@ -311,10 +311,10 @@ int bfx_set_frontier_layout(bfx_workspace *ws, uint32_t layout);
  * default, picks 80 for the chunked layout with blocks of at most 256
  * threads and 64 otherwise. */
 int bfx_set_register_budget(bfx_workspace *ws, uint32_t registers);
-/* Flat layout, persistent control with the 64-register budget: work items
- * each thread keeps in flight per iteration, 2 (default), 3 or 4 -- more
- * independent memory chains against more register spills.  Other
- * configurations use 2. */
+/* Work items each thread keeps in flight per iteration, 2 (default), 3 or 4
+ * -- more independent memory chains against more register spills: the flat
+ * layout with the 64-register budget and the chunked layout with the
+ * 80-register budget (persistent control).  Other configurations use 2. */
 int bfx_set_flat_items(bfx_workspace *ws, uint32_t items);
 /* Flat layout: how a relaxation updates the target label -- 0 (default)
  * pre-reads it and issues a non-returning 64-bit min only for a smaller

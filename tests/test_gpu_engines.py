@@ -286,7 +286,8 @@ def test_autotuner_with_near_far_candidates(gpu):
                                                                (64, 3, 0, 0, 0, 1), (64, 4, 0, 0, 0, 1),
                                                                (64, 2, 1, 0, 0, 1), (64, 2, 0, 1, 0, 1),
                                                                (64, 2, 0, 0, 1, 1), (64, 2, 0, 0, 0, 0),
-                                                               (80, 2, 0, 0, 0, 1), (80, 2, 0, 0, 0, 0)])
+                                                               (80, 2, 0, 0, 0, 1), (80, 2, 0, 0, 0, 0),
+                                                               (80, 3, 0, 0, 0, 0), (80, 4, 0, 0, 0, 1)])
 @pytest.mark.parametrize("layout_kind", [bfx.FRONTIER_FLAT, bfx.FRONTIER_GROUPS, bfx.FRONTIER_CHUNKED],
                          ids=["flat", "groups", "chunked"])
 @pytest.mark.parametrize("step", [None, 3.0])
