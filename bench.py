@@ -438,12 +438,21 @@ def main():
     else:
         peak, peak_src = 6650.0, "fallback"
     achieved = alg_bytes / (kernel_avg / 1000) / 1e9
-    traffic = None
-    tpath = REPO / "profiles" / "frontier_push_c2_traffic.txt"
+    # DRAM traffic of one launch, scaled from an ncu capture by relaxations
+    # (profiles/frontier_push_traffic.txt: workload, bytes, relaxations)
+    traffic, traffic_source = None, None
+    tpath = REPO / "profiles" / "frontier_push_traffic.txt"
     if tpath.exists():
+        captured = {}
         for line in tpath.read_text().splitlines():
-            if line.startswith("dram_bytes_per_launch:"):
-                traffic = int(float(line.split(":")[1]))
+            parts = line.split()
+            if len(parts) == 4 and not line.startswith("#"):
+                captured[parts[0]] = (int(parts[1]), int(parts[2]), parts[3])
+        key = "c2" if args.workload == "c2" else "c3small"
+        if key in captured and work["relaxations"]:
+            b, rl, src = captured[key]
+            traffic = int(b / rl * work["relaxations"])
+            traffic_source = f"{src}: {b / rl:.1f} bytes per relaxation x {work['relaxations']:,} relaxations"
 
     line = {
         "metric": METRICS[args.workload], "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
@@ -474,7 +483,7 @@ def main():
                             "layout": plain_layout, "by_layout": plain_by_layout,
                             "batched_speedup": value / world / plain_qps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_src, "kernel": "persistent_kernel (%s frontier, %d registers, %d items%s)" % (
+                     "traffic": traffic, "traffic_source": traffic_source, "peak_source": peak_src, "kernel": "persistent_kernel (%s frontier, %d registers, %d items%s)" % (
                          args.frontier, eff_regs, args.items if (eff_regs == 64 and args.frontier != "chunked") or (
                              eff_regs == 80 and args.frontier == "chunked" and not args.pairs) else 2,
                          ", mixed engines" if engines_chosen and any(e != 2 for e in engines_chosen) else ""),

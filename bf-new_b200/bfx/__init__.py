@@ -410,10 +410,22 @@ class BatchDescription:
                    arr(d.union_tiles, d.union_tile_count), arr(d.tile_lane_masks, d.tile_count), rg, qidx)
 
     def c(self) -> BatchDescriptionC:
-        return BatchDescriptionC(self.lane_width, self.valid_lane_mask, _ptr(self.source_offsets), _ptr(self.sources),
-                                 _ptr(self.target_offsets), _ptr(self.targets), len(self.union_tiles),
-                                 len(self.tile_lane_masks), _ptr(self.union_tiles), _ptr(self.tile_lane_masks),
-                                 self.ranges.shape[0], 0, C.cast(_ptr(self.ranges), P(BatchVertexRange)))
+        """The C view (pointers into this object's arrays), rebuilt only when a
+        field was replaced since the last call."""
+        # the key holds the arrays themselves, so none of them can be freed
+        # (and its address reused) while the view points at it
+        key = (self.lane_width, self.valid_lane_mask, self.source_offsets, self.sources, self.target_offsets,
+               self.targets, self.union_tiles, self.tile_lane_masks, self.ranges)
+        cached = getattr(self, "_c_view", None)
+        if cached is None or len(cached[0]) != len(key) or any(a is not b for a, b in zip(cached[0], key)):
+            view = BatchDescriptionC(self.lane_width, self.valid_lane_mask, _ptr(self.source_offsets),
+                                     _ptr(self.sources), _ptr(self.target_offsets), _ptr(self.targets),
+                                     len(self.union_tiles), len(self.tile_lane_masks), _ptr(self.union_tiles),
+                                     _ptr(self.tile_lane_masks), self.ranges.shape[0], 0,
+                                     C.cast(_ptr(self.ranges), P(BatchVertexRange)))
+            cached = (key, view)
+            self._c_view = cached
+        return cached[1]
 
     @property
     def union_vertex_count(self) -> int:

@@ -389,16 +389,27 @@ __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
 // The warp's claim stages and far-pile minimum (flat and chunked layouts)
 // serve one (round, batch): flushed when the warp moves to another batch and
 // at the end of the round, before the grid barrier.
+// Work distribution: block k owns the warp items k, k + G, k + 2G, ... (G
+// blocks), and its warps take them one at a time from a shared-memory
+// counter, so a warp that drew cheap items takes more of them and the
+// block's warps finish together; consecutive items stay on neighbouring
+// blocks at the same time (the index order of dense chunked rounds).
 template <bool kCount, u32 kItems, bool kChunked, bool kPairs = false>
 __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work& wk) {
+  __shared__ u32 s_next_item;
   const u32 ridx = r % 3u, widx = (r + 1u) % 3u;
   const u32 total = prefix[p.nb];
-  const u32 warps_per_block = blockDim.x >> 5;
-  const u32 gw = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
-  const u32 nw = gridDim.x * warps_per_block;
   Stages st{{0u, 0u}, 0xFFFFFFFFu};
   u32 staged_batch = 0xFFFFFFFFu;
-  for (u32 w = gw; w < total; w += nw) {
+  if (threadIdx.x == 0u) s_next_item = 0u;
+  __syncthreads();
+  for (;;) {
+    u32 k = 0u;
+    if (lane_id() == 0u) k = atomicAdd(&s_next_item, 1u);
+    k = __shfl_sync(0xFFFFFFFFu, k, 0);
+    const u64 wl = blockIdx.x + static_cast<u64>(k) * gridDim.x;
+    if (wl >= total) break;
+    const u32 w = static_cast<u32>(wl);
     const u32 b = find_batch(prefix, p.nb, w);
     const DBatch& B = p.batches[b];
     DCtl& C = p.ctl[b];
