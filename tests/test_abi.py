@@ -83,3 +83,22 @@ def test_upload_without_device_fails_loudly():
     layout = bfx.build_device_graph_layout(g, order)
     with pytest.raises(bfx.BfxNoDevice):
         bfx.ResidentDeviceGraph.upload_once(layout)
+
+
+def test_description_c_view_is_cached_until_a_field_is_replaced():
+    """BatchDescription.c() hands the C ABI pointers into its own arrays; the
+    view is reused across calls (the e2e step prepares the same set every
+    step) and rebuilt when a field is replaced."""
+    W = 8
+    d = bfx.BatchDescription(W, 0x3, np.array([0, 1, 2] + [2] * (W - 2), np.uint32), np.array([5, 9], np.uint32),
+                             np.array([0, 1, 2] + [2] * (W - 2), np.uint32), np.array([6, 7], np.uint32),
+                             np.array([0], np.uint32), np.array([3], np.uint32),
+                             np.array([[0, 16, 3]], np.uint32))
+    a = d.c()
+    assert d.c() is a
+    assert C.addressof(a.sources.contents) == d.sources.ctypes.data
+    d.sources = np.array([4, 9], np.uint32)
+    b = d.c()
+    assert b is not a
+    assert C.addressof(b.sources.contents) == d.sources.ctypes.data
+    assert b.lane_width == W and b.valid_lane_mask == 0x3 and b.range_count == 1
