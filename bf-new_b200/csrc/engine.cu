@@ -20,10 +20,12 @@
 //     read with 128-bit non-coherent loads;
 //   * the frontier is a queue of 32-vertex chunks by default (frontier.cuh:
 //     chunk bitmaps per round slot, pending lanes set with non-returning ORs,
-//     claims staged per warp); a warp item is one chunk whose (lane, edge)
-//     work is walked as a flat list, two items per thread in flight; the
-//     vertex-queue flat layout and the sub-warp group layout remain options;
-//     improvements use a non-returning 64-bit min after a coherent pre-read;
+//     near and far claims staged per warp and (round, batch)); a warp item
+//     is one chunk whose (lane, edge) work is walked as a flat list, two
+//     items per thread in flight, and dense rounds take the chunk slots in
+//     index order; the vertex-queue flat layout and the sub-warp group
+//     layout remain options; improvements use a non-returning 64-bit min
+//     after a coherent pre-read;
 //   * persistent mode runs all rounds of all batches in one cooperative
 //     launch with a grid barrier whose waits time out; host-poll modes run
 //     CUDA-graph-captured chunks of rounds.
