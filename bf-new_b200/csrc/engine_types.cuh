@@ -48,7 +48,7 @@ struct DBatch {
   u32 full;            // every tile selected by every valid lane, compact index == vertex id
   u64* dist[2];        // [U*W] labels (slot 1 only for Jacobi)
   u32* mask[2];        // [U] pending lane masks (frontier)
-  u64* queue[2];       // [U] frontier entries {vertex, compact index << 32}
+  u64* queue[2];       // [U] frontier entries {vertex, compact index << 32}, or chunk ids (chunked layout)
   u32* c2g;            // [U] compact -> global vertex
   uint2* tiles;        // [T] {lane mask, compact bias}
   const u32* src_off;  // [W+1]
@@ -58,7 +58,8 @@ struct DBatch {
   const uint4* ranges;    // [R] {tile, begin, end, lane mask}
   const u32* range_off;   // [R+1] compact offsets
   u32* fmask;             // [U] far lanes (near/far frontier)
-  u64* fpile[3];          // [U] far piles, rotating by far generation
+  u64* fpile[3];          // [U] far piles {vertex, compact index << 32}, rotating by far generation
+                          // (chunked layout: the vertex field holds the compact index)
   u32* cmask[2];          // [ceil(U/1024)] chunk bitmaps (chunked frontier): bit c = chunk c pending
   uint2* crow;            // [U] {CSR row begin, out-degree} per compact vertex (chunked frontier)
 };
