@@ -49,6 +49,39 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+def traffic_estimate(workload: str, relaxations: int, kernel_ms: float, path: Path | None = None):
+    """DRAM traffic of one relaxation launch, scaled by relaxations from one
+    ncu capture per workload class (profiles/frontier_push_traffic.txt:
+    `workload bytes relaxations summary` lines; c2 from the c2 capture, c3 and
+    c5 from the c3-shaped capture), and the launch's DRAM rate against the
+    random-sector ceiling (`ceiling bytes_per_s summary`).  Returns (bytes or
+    None, source text or None, ceiling dict or None)."""
+    path = path or REPO / "profiles" / "frontier_push_traffic.txt"
+    if not path.exists():
+        return None, None, None
+    captured, ceiling = {}, None
+    for line in path.read_text().splitlines():
+        parts = line.split()
+        if line.startswith("#"):
+            continue
+        if len(parts) == 4:
+            captured[parts[0]] = (int(parts[1]), int(parts[2]), parts[3])
+        elif len(parts) == 3 and parts[0] == "ceiling":
+            ceiling = (int(parts[1]), parts[2])
+    key = "c2" if workload == "c2" else "c3small"
+    if key not in captured or not relaxations:
+        return None, None, None
+    b, rl, src = captured[key]
+    traffic = int(b / rl * relaxations)
+    source = f"{src}: {b / rl:.1f} bytes per relaxation x {relaxations:,} relaxations"
+    random_ceiling = None
+    if ceiling is not None and kernel_ms > 0:
+        dram_gbs = traffic / (kernel_ms / 1000) / 1e9
+        random_ceiling = {"dram_gbs": dram_gbs, "peak_gbs": ceiling[0] / 1e9, "frac": dram_gbs * 1e9 / ceiling[0],
+                          "source": ceiling[1] + " (random 32-byte sectors beyond the L2, 41 G/s)"}
+    return traffic, source, random_ceiling
+
+
 class ClockSampler:
     """nvidia-smi samples (every 50 ms) during the timed region.  Entering
     waits (up to 5 s) for the sampler's first line, so sampling is running
@@ -438,21 +471,7 @@ def main():
     else:
         peak, peak_src = 6650.0, "fallback"
     achieved = alg_bytes / (kernel_avg / 1000) / 1e9
-    # DRAM traffic of one launch, scaled from an ncu capture by relaxations
-    # (profiles/frontier_push_traffic.txt: workload, bytes, relaxations)
-    traffic, traffic_source = None, None
-    tpath = REPO / "profiles" / "frontier_push_traffic.txt"
-    if tpath.exists():
-        captured = {}
-        for line in tpath.read_text().splitlines():
-            parts = line.split()
-            if len(parts) == 4 and not line.startswith("#"):
-                captured[parts[0]] = (int(parts[1]), int(parts[2]), parts[3])
-        key = "c2" if args.workload == "c2" else "c3small"
-        if key in captured and work["relaxations"]:
-            b, rl, src = captured[key]
-            traffic = int(b / rl * work["relaxations"])
-            traffic_source = f"{src}: {b / rl:.1f} bytes per relaxation x {work['relaxations']:,} relaxations"
+    traffic, traffic_source, random_ceiling = traffic_estimate(args.workload, work["relaxations"], kernel_avg)
 
     line = {
         "metric": METRICS[args.workload], "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
@@ -483,7 +502,8 @@ def main():
                             "layout": plain_layout, "by_layout": plain_by_layout,
                             "batched_speedup": value / world / plain_qps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "traffic_source": traffic_source, "peak_source": peak_src, "kernel": "persistent_kernel (%s frontier, %d registers, %d items%s)" % (
+                     "traffic": traffic, "traffic_source": traffic_source, "peak_source": peak_src,
+                     "random_sector_ceiling": random_ceiling, "kernel": "persistent_kernel (%s frontier, %d registers, %d items%s)" % (
                          args.frontier, eff_regs, args.items if (eff_regs == 64 and args.frontier != "chunked") or (
                              eff_regs == 80 and args.frontier == "chunked" and not args.pairs) else 2,
                          ", mixed engines" if engines_chosen and any(e != 2 for e in engines_chosen) else ""),

@@ -1,0 +1,39 @@
+"""CPU checks of bench.py's reporting helpers (no GPU work)."""
+import importlib.util
+from pathlib import Path
+
+import pytest
+
+REPO = Path(__file__).resolve().parent.parent
+
+
+def load_bench():
+    spec = importlib.util.spec_from_file_location("bench_under_test", REPO / "bench.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_traffic_estimate_scales_the_committed_captures():
+    """Traffic = the capture's bytes per relaxation x this launch's
+    relaxations (c2 from the c2 capture, c3/c5 from the c3-shaped one), and
+    the DRAM rate is reported against the random-sector ceiling."""
+    bench = load_bench()
+    rows = {}
+    for line in (REPO / "profiles" / "frontier_push_traffic.txt").read_text().splitlines():
+        parts = line.split()
+        if parts and not line.startswith("#") and len(parts) == 4:
+            rows[parts[0]] = (int(parts[1]), int(parts[2]))
+    for workload, key in (("c2", "c2"), ("c3", "c3small"), ("c5", "c3small")):
+        b, rl = rows[key]
+        t, src, ceil = bench.traffic_estimate(workload, 2 * rl, 10.0)
+        assert t == pytest.approx(2 * b, rel=1e-9)
+        assert src.endswith(f"{2 * rl:,} relaxations")
+        assert ceil["dram_gbs"] == pytest.approx(2 * b / 0.010 / 1e9)
+        assert 0 < ceil["frac"] and ceil["peak_gbs"] > 0
+    assert bench.traffic_estimate("c2", 0, 10.0) == (None, None, None)
+
+
+def test_traffic_estimate_without_file(tmp_path):
+    bench = load_bench()
+    assert bench.traffic_estimate("c2", 10, 1.0, tmp_path / "absent.txt") == (None, None, None)
