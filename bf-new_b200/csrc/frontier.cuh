@@ -83,11 +83,11 @@ struct StageQueue {
 
 __shared__ u64 s_stage_buf[2][16][kStage];  // blocks of up to 512 threads
 __shared__ StageQueue s_stage_queue[2][16];
-__shared__ u32* s_fmin_target[16];           // FarMin: fmin of the pile the warp parks on
+__shared__ u32* s_fmin_target[16];           // fmin of the far pile the warp parks on
 
 struct Stages {
   u32 n[2];  // staged entries per stage (warp-uniform)
-  u32 fd;    // smallest parked distance seen by this thread (FarMin)
+  u32 fd;    // smallest parked distance seen by this thread (folded by farmin_flush)
 };
 
 // Executed by all 32 threads.
@@ -378,10 +378,10 @@ __device__ __forceinline__ u32 flat_entries_per_item(u32 n) {
 // pending word; the OR that turns the word non-zero claims the vertex.  A
 // far success (near/far frontier) ORs its lane into the far mask the same
 // way and the OR that turns it non-zero parks the vertex on the far pile;
-// the smallest parked distance is kept per thread (FarMin).  The ORs'
+// the smallest parked distance is kept per thread (Stages::fd).  The ORs'
 // results are read one iteration later (after the next items' first loads
 // are issued), and claimed vertices are staged in the warp's shared-memory
-// stages (Stage) and appended to the next queue or the far pile with one
+// stages (Stages) and appended to the next queue or the far pile with one
 // counter atomic per 32 or more claims, off the per-step chain.  All loops
 // are warp-uniform.
 
