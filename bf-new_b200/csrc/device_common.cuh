@@ -29,6 +29,10 @@ __device__ __forceinline__ u32 hi(u64 w) { return static_cast<u32>(w >> 32); }
 __device__ __forceinline__ u64 ld_cg(const u64* p) { return __ldcg(reinterpret_cast<const unsigned long long*>(p)); }
 __device__ __forceinline__ u32 ld_cg(const u32* p) { return __ldcg(p); }
 
+__device__ __forceinline__ void red_min_u32(u32* p, u32 v) {
+  asm volatile("red.relaxed.gpu.global.min.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ u32 ld_acquire_gpu(const u32* p) {
   u32 v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");

@@ -154,6 +154,7 @@ __global__ void init_kernel(LaunchParams p) {
     B.mask[0][cv] = 0u;
     B.mask[1][cv] = 0u;
     B.fmask[cv] = 0u;
+    B.fbound[cv] = 0xFFFFFFFFu;
     if (p.flat == 2u) {
       if ((cv & 1023u) == 0u) {  // chunk bitmap words, one per 1,024 vertices
         B.cmask[0][cv >> 10] = 0u;
@@ -1089,7 +1090,7 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
     for (std::uint32_t b = 0; b < count; ++b) {
       arena_off[b] = arena_total;
       const size_t U = sz[b].U;
-      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 4 + bfx::align256(U * 8) * 6 +
+      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 5 + bfx::align256(U * 8) * 6 +
                      bfx::align256((U + 1023) / 1024 * 4) * 2;
     }
     const size_t tiles_off = arena_total;
@@ -1163,6 +1164,8 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
       B.c2g = reinterpret_cast<std::uint32_t*>(a);
       a += bfx::align256(U * 4);
       B.fmask = reinterpret_cast<std::uint32_t*>(a);
+      a += bfx::align256(U * 4);
+      B.fbound = reinterpret_cast<std::uint32_t*>(a);
       a += bfx::align256(U * 4);
       for (int k = 0; k < 3; ++k) {
         B.fpile[k] = reinterpret_cast<bfx::u64*>(a);
@@ -1842,7 +1845,8 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
     const size_t o_q1 = bfx::align256(o_q0 + U * 8);
     const size_t o_c2g = bfx::align256(o_q1 + U * 8);
     const size_t o_fmask = bfx::align256(o_c2g + U * 4);
-    const size_t o_fp0 = bfx::align256(o_fmask + U * 4);
+    const size_t o_fbound = bfx::align256(o_fmask + U * 4);
+    const size_t o_fp0 = bfx::align256(o_fbound + U * 4);
     const size_t o_fp1 = bfx::align256(o_fp0 + U * 8);
     const size_t o_fp2 = bfx::align256(o_fp1 + U * 8);
     const size_t o_tiles = bfx::align256(o_fp2 + U * 8);
@@ -1872,6 +1876,7 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
     B.queue[1] = reinterpret_cast<u64*>(base + o_q1);
     B.c2g = reinterpret_cast<u32*>(base + o_c2g);
     B.fmask = reinterpret_cast<u32*>(base + o_fmask);
+    B.fbound = reinterpret_cast<u32*>(base + o_fbound);
     B.fpile[0] = reinterpret_cast<u64*>(base + o_fp0);
     B.fpile[1] = reinterpret_cast<u64*>(base + o_fp1);
     B.fpile[2] = reinterpret_cast<u64*>(base + o_fp2);

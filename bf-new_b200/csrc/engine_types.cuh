@@ -58,6 +58,7 @@ struct DBatch {
   const uint4* ranges;    // [R] {tile, begin, end, lane mask}
   const u32* range_off;   // [R+1] compact offsets
   u32* fmask;             // [U] far lanes (near/far frontier)
+  u32* fbound;            // [U] lower bound of the vertex's parked labels (float bits; 0xffffffff: none)
   u64* fpile[3];          // [U] far piles {vertex, compact index << 32}, rotating by far generation
                           // (chunked layout: the vertex field holds the compact index)
   u32* cmask[2];          // [ceil(U/1024)] chunk bitmaps (chunked frontier): bit c = chunk c pending

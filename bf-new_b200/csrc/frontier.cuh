@@ -33,6 +33,7 @@ struct FrontierView {
   u64* queue_w;
   const uint2* tiles;
   u32* fmask;
+  u32* fbound;    // lower bound of each vertex's parked labels
   u64* pile;      // near round: far pile being filled; split round: pile read
   u64* pile_out;  // split round: pile written
   const uint2* crow;  // compact index -> {CSR row begin, out-degree} (chunked layout)
@@ -50,6 +51,7 @@ __device__ __forceinline__ FrontierView frontier_view(const DBatch& b, u32 rd, u
   v.queue_w = b.queue[rd ^ 1u];
   v.tiles = b.tiles;
   v.fmask = b.fmask;
+  v.fbound = b.fbound;
   v.pile = b.fpile[pile];
   v.pile_out = b.fpile[pile_out];
   v.crow = b.crow;
@@ -220,6 +222,7 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const Fron
             } else {
               fbits = 1u << ql;
               fd = dev::hi(cand);
+              dev::red_min_u32(B.fbound + cdst, fd);
             }
           }
           if (kCount) {
@@ -293,22 +296,35 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const Frontie
   const u32 lane = lane_id();
   const u32 entry = item * 32u + lane;
   u32 near = 0u, far = 0u, v = 0u, cv = 0u, fd = 0xFFFFFFFFu;
+  bool claim_far = false;  // the entry is re-parked unread (its far mask stays set)
   if (entry < count) {
     const u64 q = dev::ld_cg(B.pile + entry);
     v = static_cast<u32>(q);
     cv = static_cast<u32>(q >> 32);
-    u32 bits = 0u;
+    u32 bits = 0u, bound = 0xFFFFFFFFu;
     if (cv < B.U) {
       bits = dev::ld_cg(B.fmask + cv) & B.valid;
-      B.fmask[cv] = 0u;
+      bound = dev::ld_cg(B.fbound + cv);
     } else {
       atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
+    }
+    // Every parked label of the vertex is at least `bound` (each far
+    // improvement lowers it; a split stores the exact minimum of the lanes
+    // it re-parks).  When the bound is finite and not below the new
+    // threshold, all lanes stay parked: the entry moves to the next pile
+    // unread and its far mask stays set.
+    const bool stays = bits != 0u && bound < dev::kInfBits && bound >= tau_next;
+    if (stays) {
+      far = bits;
+      fd = bound;
+    } else if (cv < B.U) {
+      B.fmask[cv] = 0u;
     }
     // Parked lanes are re-read eight at a time: the eight label loads are
     // issued back to back, so an entry with k far lanes waits ceil(k / 8)
     // memory latencies instead of k.
     u64* const row = B.dist + (static_cast<u64>(cv) << B.shift);
-    for (u32 rest = bits; rest != 0u;) {
+    for (u32 rest = stays ? 0u : bits; rest != 0u;) {
       u32 ls[8], ds[8];
 #pragma unroll
       for (u32 i = 0; i < 8u; ++i) {
@@ -329,15 +345,18 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const Frontie
         }
       }
     }
+    // the bound of the lanes that stay parked (none: cleared)
+    if (!stays && cv < B.U) B.fbound[cv] = far != 0u ? fd : 0xFFFFFFFFu;
     if (kCount) {
       wk.c[0] += 1;
       wk.c[11] += 1;
-      wk.c[12] += static_cast<u32>(__popc(bits));
+      if (!stays) wk.c[12] += static_cast<u32>(__popc(bits));
     }
+    claim_far = stays;
   }
   // far lanes stay parked (next pile); near lanes join the next round
-  bool fclaim = false, claim = false;
-  if (far != 0u) fclaim = atomicOr(B.fmask + cv, far) == 0u;
+  bool fclaim = claim_far, claim = false;
+  if (far != 0u && !claim_far) fclaim = atomicOr(B.fmask + cv, far) == 0u;
   u64 qword = queue_word(v, cv);  // queue word: {vertex, compact index}, or the chunk (chunked layout)
   if (near != 0u) {
     if (kChunked) {
@@ -558,6 +577,7 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
             } else {
               fbits[u] = 1u << it[u].ql;
               st.fd = min(st.fd, dev::hi(cand[u]));
+              dev::red_min_u32(B.fbound + cdst[u], dev::hi(cand[u]));
             }
           }
           if (kCount) {
