@@ -1717,14 +1717,17 @@ int bfx_run_query(bfx_workspace* ws, uint32_t source_count, const uint32_t* sour
 // ---------------------------------------------------------------------------
 // Static-scratch single-query entry point (bfx_run_query_static).
 //
-// For callers that must not allocate device memory at call time: code that
-// runs while a CUDA graph is being captured (cudaMalloc is not allowed
-// there), processes whose device memory is carved up and owned by another
-// runtime, and latency-critical loops that cannot afford an allocation's
-// implicit synchronisation.  bfx_run_query allocates its workspace on first
-// use and grows it; this variant keeps every scratch buffer (labels, pending
-// masks, frontier queues, tile table, batch records, launch state) in one
-// file-scope device array of fixed size, so a call allocates nothing.
+// For callers that must not allocate device memory at call time: processes
+// whose device memory is carved up and owned by another runtime (a host
+// application or framework that hands the GPU's memory to its own pool and
+// forbids other allocations), and latency-critical loops that cannot afford
+// an allocation's implicit synchronisation.  bfx_run_query allocates its
+// workspace on first use and grows it; this variant keeps every scratch
+// buffer (labels, pending masks, frontier queues, tile table, batch records,
+// launch state) in one file-scope device array of fixed size, so a call
+// allocates nothing.  It runs the persistent cooperative control mode only,
+// without instrumentation, on the legacy default stream with synchronous
+// copies.
 // ---------------------------------------------------------------------------
 
 namespace bfx {
@@ -1748,7 +1751,9 @@ void* g_static_base[kMaxStaticDevices] = {};
 
 // Device address of bfx_static_scratch on the current device, resolved once
 // per device with cudaGetSymbolAddress (the host-side name is only a
-// stand-in; kernels must be given this address).
+// stand-in; kernels must be given this address).  The address is kept for
+// the life of the process, so a cudaDeviceReset between calls is not
+// supported (the module, and with it the array, may move).
 cudaError_t static_scratch_base(int device, void** out) {
   std::lock_guard<std::mutex> lock(g_static_mutex);
   if (g_static_base[device] == nullptr) {
@@ -1796,6 +1801,9 @@ extern "C" int bfx_run_query_static(const bfx_resident_graph* graph, uint32_t so
     bfx::require(source_count > 0 && target_count > 0, "route queries require sources and targets");
     bfx::require(sources && targets && selected_tiles && selected_tile_count > 0, "null query array");
     bfx::validate_options(*options);
+    bfx::require(options->control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE,
+                 "the static-scratch query runs the persistent cooperative control mode only");
+    bfx::require(options->instrumentation == 0u, "the static-scratch query has no instrumentation");
     if (graph->device < 0 || graph->device >= bfx::kMaxStaticDevices) throw std::out_of_range("device index");
     const std::vector<std::uint32_t>& tvo = graph->tile_vertex_offsets;
     const u32 T = graph->g.T, V = graph->g.V;

@@ -378,27 +378,34 @@ int bfx_run_query(bfx_workspace *ws, uint32_t source_count, const uint32_t *sour
 
 /* ---- single query without device allocation --------------------------------
  * No counterpart in the reference: a libbfx addition for callers that cannot
- * allocate device memory when they run a query -- code running inside CUDA
- * graph capture (cudaMalloc is not permitted there), processes whose device
- * memory is owned and carved up by another runtime, and latency-critical
- * loops that cannot afford an allocation's implicit synchronisation.
+ * allocate device memory when they run a query -- processes whose device
+ * memory is owned and carved up by another runtime (a host application or
+ * framework that hands the whole GPU to its own pool and forbids further
+ * allocations), and latency-critical loops that cannot afford an
+ * allocation's implicit synchronisation.
  *
- * Same query semantics and status as bfx_run_query, but every scratch buffer
- * (labels, pending masks, frontier queues, tile table, batch records, launch
- * state) lives in one fixed 32 MiB array in the library's device memory, so
- * the call allocates nothing.  Limits and rules:
- *  - the whole query image must fit in 32 MiB (about 72 bytes per selected
+ * Same query semantics and status as bfx_run_query under the persistent
+ * cooperative control mode, but every scratch buffer (labels, pending masks,
+ * frontier queues, tile table, batch records, launch state) lives in one
+ * fixed 32 MiB array in the library's device memory, so the call allocates
+ * nothing.  Limits and rules:
+ *  - the whole query image must fit in 32 MiB (about 76 bytes per selected
  *    vertex plus 8 bytes per graph tile); larger queries fail with
  *    BFX_ERR_OVERFLOW and a message -- use bfx_run_query for them;
+ *  - options->control_mode must be BFX_CONTROL_PERSISTENT_COOPERATIVE and
+ *    options->instrumentation 0 (otherwise BFX_ERR_INVALID_ARGUMENT); the
+ *    engine, block size, grid policy, round limit and per-lane convergence
+ *    are honoured;
  *  - every GPU that loads libbfx.so holds the 32 MiB array until exit;
  *  - the first call on a device resolves the array's device address once
- *    (cudaGetSymbolAddress); make that first call before any stream capture;
+ *    (cudaGetSymbolAddress) and keeps it for the process, so resetting the
+ *    device (cudaDeviceReset) between calls is not supported;
  *  - all calls on a device share the array and leave their data in it (each
  *    call re-initialises what it reads); calls that overlap on the GPU --
  *    from several host threads at once -- race and must be serialised by the
  *    caller;
- *  - work runs on the legacy default stream and the call returns after the
- *    results are on the host.
+ *  - work runs on the legacy default stream with synchronous copies, and the
+ *    call returns after the results are on the host.
  * Outputs: the status, and per target (canonical order) its distance bits and
  * predecessor stable edge id (0xffffffff for sources and unreached targets). */
 int bfx_run_query_static(const bfx_resident_graph *graph, uint32_t source_count, const uint32_t *sources,
