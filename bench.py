@@ -1,23 +1,37 @@
 """Benchmark: batched regional SSSP on B200 (queries/s, GTEPS, HBM roofline).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bfx|reference]
+                    [--workload c2|c3|c5|c3small] [--shard] [--no-c3]
 
 Workload (default c2): 128x128 tiles x 128 nodes (2,097,152 vertices,
 16,777,216 edges), float costs base(span) * lognormal(0, 0.5); 256 regional
 queries with box sides U[4,64] tiles, one source and one target each; the
 planner groups overlapping queries into batches (narrowed to 1/8/16/32
-lanes) and one persistent cooperative launch relaxes all of them.
+lanes) and one persistent cooperative launch relaxes all of them.  On one GPU
+the default run also times c3 (64 full-graph sources on 256x256 tiles x 256
+nodes, 16.8M V / 168M E, uint costs) and reports it in the line's `c3`
+object with its own roofline.
 
 A step is one pass of the hot path over the whole query set: labels reset,
 seeded, relaxed to convergence, targets classified.  `value` times the steps
 with inputs resident in HBM (device events on the launching stream);
 `e2e.value` times the same steps through the C ABI from host buffers
-(descriptions H2D from pinned staging, statuses D2H).  Inputs (graph 0.5 GB
-+ labels) exceed the 126 MB L2, so no flush is needed between steps.
+(descriptions H2D from pinned staging, statuses D2H).  The host planner and
+the autotuner run before the timed regions; their times are reported as
+`host.plan_s` / `host.tune_s`.  Inputs (graph 0.5 GB + labels) exceed the
+126 MB L2, so no flush is needed between steps.
+
+The cpu_baseline leg times the reference's own CPU engine (oracle/_ref:
+dijkstra_oracle on induced graphs) on a sample of the same queries and
+checks the GPU's labels of those queries against it: distances bit for bit
+against the reference, predecessors against the oracle's min-eid tight
+in-edge (`parity` in the line).
 
 Multi-GPU (torchrun): replicas -- each rank holds the graph and relaxes its
-own query set (weak scaling, no data-path collective); only the timing
-max-reduction uses torch.distributed.
+own query set (weak scaling, no data-path collective); with --shard the one
+query set is planned once and its batches are split over the ranks by
+estimated lane-edges (strong scaling).  Only the timing max-reduction and the
+final status gather use torch.distributed.
 """
 from __future__ import annotations
 
@@ -38,24 +52,31 @@ for _p in (REPO, REPO / "bf-new_b200"):
 
 import numpy as np  # noqa: E402
 
-METRIC = "batched SSSP queries/s (256 uneven regional queries, 2.1M V / 16.8M E, one persistent launch)"
-METRIC_C3 = "batched SSSP queries/s (64 full-graph sources, 16.8M V / 168M E, one persistent launch)"
-METRIC_C5 = "batched SSSP queries/s (4,096 regional + 16 full-graph queries, 16.8M V / 168M E, autotuned)"
-METRICS = {"c2": METRIC, "c3": METRIC_C3, "c5": METRIC_C5,
-           "c3small": "batched SSSP queries/s (32 full-graph sources, 4.2M V / 42M E, profiling-sized c3)"}
+METRICS = {
+    "c2": "batched SSSP queries/s (256 uneven regional queries, 2.1M V / 16.8M E, one persistent launch)",
+    "c3": "batched SSSP queries/s (64 full-graph sources, 16.8M V / 168M E, one persistent launch)",
+    "c5": "batched SSSP queries/s (4,096 regional + 16 full-graph queries, 16.8M V / 168M E, autotuned)",
+    "c3small": "batched SSSP queries/s (32 full-graph sources, 4.2M V / 42M E, profiling-sized c3)",
+}
+GRAPH_GB = {"c2": "0.54", "c3small": "1.3", "c3": "5.4", "c5": "5.4"}
+INF_BITS = 0x7F800000
 
 
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def traffic_estimate(workload: str, relaxations: int, kernel_ms: float, path: Path | None = None):
+def traffic_estimate(workload: str, relaxations: int, kernel_ms: float, step: str | None = None,
+                     path: Path | None = None):
     """DRAM traffic of one relaxation launch, scaled by relaxations from one
     ncu capture per workload class (profiles/frontier_push_traffic.txt:
-    `workload bytes relaxations summary` lines; c2 from the c2 capture, c3 and
-    c5 from the c3-shaped capture), and the launch's DRAM rate against the
-    random-sector ceiling (`ceiling bytes_per_s summary`).  Returns (bytes or
-    None, source text or None, ceiling dict or None)."""
+    `workload bytes relaxations step summary` lines; c2 from the c2 capture,
+    c3 and c5 from the c3-shaped capture), and the launch's DRAM rate against
+    the random-sector ceiling (`ceiling bytes_per_s summary`).  The near/far
+    step changes the relaxations per sector, so a capture is scaled only to a
+    launch run at its own step (`step` = the launch's steps, e.g. "1" or
+    "plain"; None accepts any).  Returns (bytes or None, source text or None,
+    ceiling dict or None)."""
     path = path or REPO / "profiles" / "frontier_push_traffic.txt"
     if not path.exists():
         return None, None, None
@@ -64,22 +85,32 @@ def traffic_estimate(workload: str, relaxations: int, kernel_ms: float, path: Pa
         parts = line.split()
         if line.startswith("#"):
             continue
-        if len(parts) == 4:
-            captured[parts[0]] = (int(parts[1]), int(parts[2]), parts[3])
+        if len(parts) == 5:
+            captured[parts[0]] = (int(parts[1]), int(parts[2]), parts[3], parts[4])
         elif len(parts) == 3 and parts[0] == "ceiling":
             ceiling = (int(parts[1]), parts[2])
     key = "c2" if workload == "c2" else "c3small"
     if key not in captured or not relaxations:
         return None, None, None
-    b, rl, src = captured[key]
+    b, rl, cstep, src = captured[key]
+    if step is not None and step != cstep:
+        return None, f"{src}: captured at step {cstep}, launch ran at step {step}; not scaled", None
     traffic = int(b / rl * relaxations)
-    source = f"{src}: {b / rl:.1f} bytes per relaxation x {relaxations:,} relaxations"
+    source = f"{src} (step {cstep}): {b / rl:.1f} bytes per relaxation x {relaxations:,} relaxations"
     random_ceiling = None
     if ceiling is not None and kernel_ms > 0:
         dram_gbs = traffic / (kernel_ms / 1000) / 1e9
         random_ceiling = {"dram_gbs": dram_gbs, "peak_gbs": ceiling[0] / 1e9, "frac": dram_gbs * 1e9 / ceiling[0],
-                          "source": ceiling[1] + " (random 32-byte sectors beyond the L2, 41 G/s)"}
+                          "source": ceiling[1] + " (random 32-byte sectors beyond the L2)"}
     return traffic, source, random_ceiling
+
+
+def step_label(engines, deltas, mean_weight: float) -> str:
+    """The near/far step of the launch's frontier batches in mean edge
+    weights ("plain" without a threshold, "mixed" when batches differ)."""
+    steps = {("plain" if not np.isfinite(d) else f"{d / mean_weight:.3g}")
+             for e, d in zip(engines, deltas) if e == 2}
+    return steps.pop() if len(steps) == 1 else ("none" if not steps else "mixed")
 
 
 class ClockSampler:
@@ -140,75 +171,356 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def cpu_reference_baseline(graph_input, order, queries, sample: int, threads: int):
-    """The reference's own CPU engine (oracle/_ref: dijkstra_oracle on each
-    query's induced graph, one query per host thread) on a bounded sample."""
+# ---------------------------------------------------------------------------
+# Reference arm and CPU baseline (the reference's own CPU engine)
+# ---------------------------------------------------------------------------
+
+def reference_case(workload: str, query_count: int | None = None):
+    """The reference's own case for a timed workload: the synthetic graph from
+    the generator restated in the reference driver, partitioned and laid out
+    by the reference, and the query set drawn from the reference's tile table
+    by the same samplers as the GPU arm (bfx.workloads is pure Python here:
+    libbfx is not loaded)."""
+    from bfx import workloads
     from oracle.oracle import Ref
-    if not Ref.available():
-        return None
+    spec, grid = workloads.bench_graph_spec(workload)
     ref = Ref()
     t0 = time.time()
-    h = ref.case_from_input(graph_input, order)
+    h = ref.case_synth(spec)
     build_s = time.time() - t0
-    idx = []
-    for q in queries[:sample]:
-        idx.append(ref.query_add(h, q.query_id, q.sources, q.targets, q.selected_tiles))
-    r = ref.time_dijkstra(h, idx, threads)
-    ref.free(h)
-    return {"value": sample / r["wall_s"], "unit": "queries/s", "cores": threads, "kind": "reference",
-            "sample": f"first {sample} of the {len(queries)} queries, reference dijkstra_oracle on each induced "
-                      f"graph, one query per thread (induced-graph builds, {r['induced_s']:.2f} thread-s, excluded)",
-            "wall_s": r["wall_s"], "gteps": r["edges"] / r["wall_s"] / 1e9, "graph_build_s": build_s}
-
-
-def cpu_port_baseline(layout, queries, sample: int, threads: int):
-    """Fallback when the reference build is absent: the oracle's C restatement."""
-    from oracle.oracle import Oracle
-    orc = Oracle.from_layout(layout)
-    t0 = time.time()
-    orc.region_sssp_many(queries[:sample], threads)
-    wall = time.time() - t0
-    return {"value": sample / wall, "unit": "queries/s", "cores": threads, "kind": "port",
-            "sample": f"first {sample} of {len(queries)} queries, oracle bounded Dijkstra, one query per thread",
-            "wall_s": wall}
+    queries, _ = workloads.bench_queries(workload, ref.tiles(h), grid, 0, query_count)
+    idx = [ref.query_add(h, q.query_id, q.sources, q.targets, q.selected_tiles) for q in queries]
+    return ref, h, queries, idx, build_s
 
 
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    import bfx
-    from bfx import workloads
-    g, order, _ = bfx.synth_graph(**workloads.GRAPHS["c2"])
-    layout = bfx.build_device_graph_layout(g, order)
-    grid = (128, 128)
-    queries = workloads.box_queries(layout, grid, 256, 4, 64, 202)
-    threads = os.cpu_count() or 1
     from oracle.oracle import Ref
     if not Ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU library (oracle/_ref) was not built"}))
         return
-    ref = Ref()
-    h = ref.case_from_input(g, order)
-    idx = [ref.query_add(h, q.query_id, q.sources, q.targets, q.selected_tiles) for q in queries]
-    sample = 64
-    for _ in range(args.warmup):
-        ref.time_dijkstra(h, idx[:8], threads)
-    walls = []
-    for s in range(args.steps):
-        part = [idx[(s * sample + i) % len(idx)] for i in range(sample)]
-        walls.append(ref.time_dijkstra(h, part, threads)["wall_s"])
-    total = sum(walls)
-    v = sample * args.steps / total
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+    from bfx import workloads
+    ref, h, queries, idx, build_s = reference_case(args.workload, args.queries)
+    threads = os.cpu_count() or 1
+    # Full-graph queries build an induced copy of the whole graph each, so
+    # the full-graph workloads time a bounded sample of their queries.
+    full_graph = args.workload in ("c3", "c3small")
+    timed = idx if not full_graph else idx[:min(len(idx), 4)]
+    r = ref.time_dijkstra_steps(h, timed, threads, args.warmup, args.steps)
+    total = sum(r["step_s"])
+    nq = len(timed)
+    v = nq * args.steps / total
+    sample = (f"all {nq} queries of the set every step" if nq == len(queries) else
+              f"first {nq} of the {len(queries)} queries every step")
+    line = {"impl": "reference", "metric": METRICS[args.workload], "value": v, "unit": "queries/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "c2: 256 regional queries on 128x128x128 tiles (2.1M V, 16.8M E), f32 lognormal "
-                                   "costs; each step a bounded sample of 64 of those queries"},
+            "config": {"workload": workloads.BENCH_DESCRIPTIONS[args.workload], "queries_per_step": nq},
+            "gteps": r["edges"] * args.steps / total / 1e9,
+            "host": {"graph_build_s": build_s, "induced_graphs_s": r["induced_wall_s"],
+                     "note": "induced graphs are built once before the timed steps (their wall time is "
+                             "induced_graphs_s); each step runs dijkstra_oracle over every sampled query"},
+            "pipeline": {"value": nq / (r["induced_wall_s"] + total / args.steps), "unit": "queries/s",
+                         "what": "induced-graph builds + one step of dijkstra_oracle"},
             "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "reference",
-                             "sample": "64 queries per step, reference dijkstra_oracle on induced graphs"},
+                             "sample": f"{sample}; reference dijkstra_oracle on each query's induced graph, "
+                                       f"one query per host thread"},
             "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    ref.free(h)
     print(json.dumps(line))
+
+
+def cpu_baseline_and_parity(wl, lane_images, sample_ids, threads):
+    """The reference's own CPU engine timed on a sample of the queries (one
+    step, all host threads), and the GPU's labels of those queries checked
+    against it: distances bit for bit against the reference's
+    dijkstra_oracle, predecessors against the oracle's min-eid tight in-edge.
+    `lane_images` maps query index -> (distance bits, predecessors) of the
+    GPU run."""
+    from oracle.oracle import Oracle, Ref
+    checked = dist_bad = pred_bad = 0
+    if Ref.available():
+        ref, h, queries, idx, build_s = reference_case(wl.name, len(wl.queries))
+        r = ref.time_dijkstra_steps(h, [idx[i] for i in sample_ids], threads, 0, 1, want_dist=True)
+        wall = r["step_s"][0]
+        ref_dist = {q: r["dist"][k].view(np.uint32) for k, q in enumerate(sample_ids)}
+        ref.free(h)
+        cb = {"value": len(sample_ids) / wall, "unit": "queries/s", "cores": threads, "kind": "reference",
+              "sample": f"{len(sample_ids)} of the {len(wl.queries)} queries, reference dijkstra_oracle on each "
+                        f"induced graph, one query per thread (induced-graph builds, {r['induced_wall_s']:.2f} s "
+                        f"wall, excluded)",
+              "wall_s": wall, "gteps": r["edges"] / wall / 1e9, "graph_build_s": build_s}
+        checker = "reference dijkstra_oracle distances; oracle min-eid tight predecessors"
+    else:
+        ref_dist, cb = None, None
+        checker = "oracle bounded Dijkstra distances and min-eid tight predecessors"
+    orc = Oracle.from_layout(wl.layout)
+    t0 = time.time()
+    od, op = orc.region_sssp_many([wl.queries[i] for i in sample_ids], threads)
+    port_wall = time.time() - t0
+    if cb is None:
+        cb = {"value": len(sample_ids) / port_wall, "unit": "queries/s", "cores": threads, "kind": "port",
+              "sample": f"{len(sample_ids)} of {len(wl.queries)} queries, oracle bounded Dijkstra, one query per thread",
+              "wall_s": port_wall}
+    for k, q in enumerate(sample_ids):
+        bits, pred = lane_images[q]
+        want = ref_dist[q] if ref_dist is not None else od[k]
+        dist_bad += int(np.count_nonzero(bits != want))
+        pred_bad += int(np.count_nonzero(pred != op[k]))
+        checked += 1
+    parity = {"lanes_checked": checked, "distance_mismatches": dist_bad, "predecessor_mismatches": pred_bad,
+              "mismatches": dist_bad + pred_bad, "checker": checker}
+    return cb, parity
+
+
+# ---------------------------------------------------------------------------
+# The bfx arm
+# ---------------------------------------------------------------------------
+
+def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, sample_ids=()):
+    """Plans, tunes and times one workload; returns (line dict, lane images of
+    the sampled queries)."""
+    import bfx
+    import torch
+    from bfx import replicas
+
+    t0 = time.time()
+    plan = bfx.make_overlapping_batch_plan(wl.layout, wl.queries, wl.policy)
+    descs = plan.descriptions()
+    plan_s = time.time() - t0
+    estimates = [e[3] for e in plan.estimates]
+    if shard and world > 1:
+        mine = replicas.shard_batches(estimates, world)[rank]
+        descs = [descs[b] for b in mine]
+        estimates = [estimates[b] for b in mine]
+    queries_here = sum(bin(d.valid_lane_mask).count("1") for d in descs)
+    lane_edges = sum(estimates)
+    log(f"[bench] {wl.name}: plan {plan_s:.2f}s: {len(descs)} batches, widths "
+        f"{sorted({d.lane_width for d in descs})}, sum selected edges {lane_edges:,}")
+
+    resident = bfx.ResidentDeviceGraph.upload_once(wl.layout, device)
+    ws = bfx.Workspace(resident)
+    layout_ids = {"flat": bfx.FRONTIER_FLAT, "groups": bfx.FRONTIER_GROUPS, "chunked": bfx.FRONTIER_CHUNKED}
+    ws.set_frontier_layout(layout_ids[args.frontier])
+    ws.set_register_budget(args.regs)
+    eff_regs = args.regs or (80 if args.frontier == "chunked" else 64)
+    if args.frontier != "chunked" and eff_regs == 80:
+        eff_regs = 64
+    ws.set_flat_items(args.items)
+    ws.set_relax_atomic(args.amin)
+    ws.set_flat_order(args.edge_major)
+    ws.set_chunk_pairs(args.pairs)
+    engine_id = {"auto": bfx.ENGINE_AUTO, "frontier": bfx.ENGINE_FRONTIER_PUSH, "jacobi": bfx.ENGINE_JACOBI_PULL,
+                 "dense": bfx.ENGINE_DENSE_CHAOTIC_PUSH}[args.engine]
+    mean_w = float(np.mean(wl.layout.arrays["csr_weights"]))
+    engines_chosen, policy_times, tune_s = None, None, 0.0
+    if args.tune_policy and not shard:
+        candidates = [wl.policy] + [bfx.BatchPlannerPolicy(32, *c, narrow_lanes=True)
+                                    for c in ((1, 16, 4, 1), (1, 4, 2, 1), (1, 32, 8, 1))]
+        t4 = time.time()
+        best, policy_times = ws.autotune_policy(wl.layout, wl.queries, candidates)
+        plan = bfx.make_overlapping_batch_plan(wl.layout, wl.queries, candidates[best])
+        descs = plan.descriptions()
+        lane_edges = sum(e[3] for e in plan.estimates)
+        tune_s += time.time() - t4
+        log(f"[bench] policy tuning {time.time() - t4:.1f}s: times {policy_times}, best {best}")
+    if engine_id == bfx.ENGINE_AUTO:
+        t3 = time.time()
+        engines_chosen, measured = ws.autotune(descs)
+        tune_s += time.time() - t3
+        log(f"[bench] autotune {time.time() - t3:.1f}s ({measured} batches timed): "
+            f"{ {e: engines_chosen.count(e) for e in set(engines_chosen)} } (0 jacobi, 1 dense, 2 frontier)")
+        deltas = list(ws.tuned_deltas)
+    else:
+        deltas = [float("inf")] * len(descs)
+        if args.step is not None:
+            deltas = [float("inf") if args.step == 0 else args.step * mean_w] * len(descs)
+            ws.set_batch_deltas(deltas)
+    opts = bfx.GpuRunOptions(engine=engine_id)
+    opts_instr = bfx.GpuRunOptions(engine=engine_id, instrumentation=1)
+
+    torch.cuda.set_device(device)
+    stream = torch.cuda.ExternalStream(ws.stream, device=device)
+
+    def barrier():
+        torch.cuda.synchronize(device)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    def max_over_ranks(x: float) -> float:
+        return replicas.max_over_ranks(dist, x) if dist else x
+
+    # ---- instrumented pass (untimed): algorithmic work counts, label bound
+    ws.prepare(descs)
+    ws.execute(opts_instr)
+    statuses = ws.fetch_statuses()
+    work = ws.work_counters()
+    engine_work = ws.engine_work()
+    assert all(s.stop_reason == bfx.STOP_CONVERGED for s in statuses), "benchmark run did not converge"
+    reached = sum(bin(s.reached_target_mask).count("1") for s in statuses)
+    bound_bits = int(ws.label_bounds().max())
+    max_distance = float(np.uint32(bound_bits).view(np.float32))
+    if wl.uint_costs:
+        # integer costs are exact in float sums only below 2^24
+        assert bound_bits < 0x4B800000, f"largest distance {max_distance} is not below 2^24"
+
+    # ---- device-resident timing (value)
+    for _ in range(warmup):
+        ws.execute(opts)
+    barrier()
+    with ClockSampler(device) as clocks:
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        # NVTX range: lets a profiler select the timed launches
+        torch.cuda.nvtx.range_push("bench_timed")
+        for _ in range(steps):
+            ws.execute(opts)
+        torch.cuda.nvtx.range_pop()
+        end.record(stream)
+        barrier()
+    dev_ms = start.elapsed_time(end)
+    # Relaxation-kernel time per launch (library events on the same stream),
+    # sampled right after the timed region.
+    kernel_ms, execute_ms = [], []
+    for _ in range(3):
+        ws.execute(opts)
+        k, x = ws.last_execute_timing()
+        kernel_ms.append(k)
+        execute_ms.append(x)
+    launches_per_step = ws.last_launch_count()
+    dev_ms = max_over_ranks(dev_ms)
+    log(f"[bench] {wl.name} device-resident: {dev_ms / steps:.3f} ms/step, relaxation kernel "
+        f"{np.mean(kernel_ms):.3f} ms")
+    statuses = ws.fetch_statuses()
+    assert all(s.stop_reason == bfx.STOP_CONVERGED for s in statuses)
+    if dist:  # the job's one exchange: every rank's status records to every rank
+        all_statuses = replicas.gather_statuses(dist, statuses)
+        assert all(s.stop_reason == bfx.STOP_CONVERGED for part in all_statuses for s in part)
+
+    # ---- end-to-end timing through the C ABI from host buffers (e2e)
+    for _ in range(warmup):
+        ws.prepare(descs)
+        ws.execute(opts)
+        ws.fetch_statuses()
+    barrier()
+    s2 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(steps):
+        ws.prepare(descs)
+        ws.execute(opts)
+        ws.fetch_statuses()
+    e2.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(s2.elapsed_time(e2))
+    log(f"[bench] {wl.name} end-to-end: {e2e_ms / steps:.3f} ms/step")
+    h2d, d2h = ws.transfer_bytes()
+
+    # ---- the sampled queries' labels from the last launch (checked on the host)
+    lane_of = {int(d.query_index_by_lane[l]): (b, l) for b, d in enumerate(descs)
+               for l in range(d.lane_width) if (d.valid_lane_mask >> l) & 1}
+    lane_images = {q: ws.download_lane(*lane_of[q]) for q in sample_ids if q in lane_of}
+
+    # ---- plain per-query engine (one query per launch sequence) on a sample
+    # of each query class; the whole set's time is extrapolated per class.
+    # The baseline is the faster of the frontier layouts for single queries.
+    plain_by_layout, plain_sampled = {}, 0
+    classes = wl.classes if not (shard and world > 1) else []
+    for lname, lid in (("chunked", bfx.FRONTIER_CHUNKED), ("flat", bfx.FRONTIER_FLAT)):
+        if not classes:
+            break
+        ws.set_frontier_layout(lid)
+        plain_total_s, plain_sampled = 0.0, 0
+        for members, n in classes:
+            sample_q = members[:n]
+            ws.run_query(sample_q[0].sources, sample_q[0].targets, sample_q[0].selected_tiles,
+                         bfx.GpuRunOptions(engine=bfx.ENGINE_FRONTIER_PUSH))  # warm-up
+            barrier()
+            s3 = torch.cuda.Event(enable_timing=True)
+            e3 = torch.cuda.Event(enable_timing=True)
+            s3.record(stream)
+            for q in sample_q:
+                ws.run_query(q.sources, q.targets, q.selected_tiles, bfx.GpuRunOptions(engine=bfx.ENGINE_FRONTIER_PUSH))
+            e3.record(stream)
+            barrier()
+            plain_total_s += s3.elapsed_time(e3) / 1000 / len(sample_q) * len(members)
+            plain_sampled += len(sample_q)
+        plain_by_layout[lname] = len(wl.queries) / plain_total_s
+    ws.set_frontier_layout(layout_ids[args.frontier])
+
+    nq = (len(wl.queries) if shard else queries_here * world)
+    ms_per_step = dev_ms / steps
+    value = nq / (ms_per_step / 1000)
+    e2e_value = nq / (e2e_ms / steps / 1000)
+    kernel_avg = float(np.mean(kernel_ms))
+    # algorithmic bytes per launch, per engine class:
+    #   push (frontier, dense): 16 F + 12 S + 8 P + 16 L + 8 N (dense has N = 0)
+    #   Jacobi pull:            16 (vertex-lane items) + 12 (in-edge records) + 8 (relaxations)
+    pw, jw = engine_work["push"], engine_work["jacobi"]
+    F, S, Pp, L, N = (pw[k] for k in ("entries", "records", "active_pairs", "relaxations", "claims"))
+    alg_bytes = (16 * F + 12 * S + 8 * Pp + 16 * L + 8 * N +
+                 16 * jw["items"] + 12 * jw["records"] + 8 * jw["relaxations"])
+    peaks_path = REPO / "MEASURED_PEAKS.json"
+    if peaks_path.exists():
+        peak = json.loads(peaks_path.read_text())["hbm_gbs"]
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = alg_bytes / (kernel_avg / 1000) / 1e9
+    engines_for_step = engines_chosen or [2 if engine_id == bfx.ENGINE_FRONTIER_PUSH else engine_id] * len(descs)
+    step = step_label(engines_for_step, deltas, mean_w)
+    traffic, traffic_source, random_ceiling = traffic_estimate(wl.name, work["relaxations"], kernel_avg, step)
+    line = {
+        "metric": METRICS[wl.name], "value": value, "unit": "queries/s", "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "strong" if shard and world > 1 else "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": wl.description, "queries": nq, "batches": len(descs),
+                   "lane_widths": sorted({d.lane_width for d in descs}), "engine": args.engine,
+                   "policy_times_ms": policy_times,
+                   "planner_policy": [wl.policy.minimum_jaccard_numerator, wl.policy.minimum_jaccard_denominator,
+                                      wl.policy.maximum_union_inflation_numerator,
+                                      wl.policy.maximum_union_inflation_denominator],
+                   "near_far_step": step,
+                   "frontier_layout": args.frontier, "registers": eff_regs, "flat_items": args.items,
+                   "returning_min": args.amin, "edge_major": args.edge_major, "chunk_pairs": args.pairs,
+                   "engines_chosen": None if engines_chosen is None else
+                   {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
+                   "control": "persistent_cooperative",
+                   "parallelism": (f"shards{world}" if shard and world > 1 else f"replicas{world}"),
+                   "l2": f"inputs larger than L2 (graph {GRAPH_GB[wl.name]} GB + labels), no flush"},
+        "gteps": lane_edges * (1 if shard else world) / (ms_per_step / 1000) / 1e9,
+        "reached_lanes": reached,
+        "max_finite_distance": max_distance,
+        "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "host": {"plan_s": plan_s, "tune_s": tune_s,
+                 "note": "host planner (batch grouping + descriptions) and autotuner run once per query set, "
+                         "before both timed regions"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "traffic_source": traffic_source, "peak_source": peak_src,
+                     "random_sector_ceiling": random_ceiling, "kernel": "persistent_kernel (%s frontier, %d registers%s)" % (
+                         args.frontier, eff_regs,
+                         ", mixed engines" if engines_chosen and any(e != 2 for e in engines_chosen) else ""),
+                     "kernel_ms": kernel_avg, "execute_ms": float(np.mean(execute_ms)),
+                     "algorithmic_bytes_per_launch": alg_bytes, "work": work, "engine_work": engine_work},
+        "clocks": clocks.summary(),
+        "gpu_launches": launches_per_step * steps,
+    }
+    line["pipeline"] = {"value": nq / (plan_s + tune_s + e2e_ms / steps / 1000), "unit": "queries/s",
+                        "what": "host plan + autotune + one end-to-end step (a fresh query set, tuned once)"}
+    if plain_by_layout:
+        plain_layout = max(plain_by_layout, key=plain_by_layout.get)
+        plain_qps = plain_by_layout[plain_layout]
+        line["plain_per_query"] = {"value": plain_qps, "unit": "queries/s", "sample": plain_sampled,
+                                   "layout": plain_layout, "by_layout": plain_by_layout,
+                                   "batched_speedup": value / world / plain_qps}
+    ws.close()
+    resident.close()
+    return line, lane_images
 
 
 def main():
@@ -225,8 +537,6 @@ def main():
                     help="register budget of the persistent kernel (0: 80 for the chunked layout, else 64)")
     ap.add_argument("--items", type=int, default=2, choices=[2, 3, 4],
                     help="flat layout: work items per thread per iteration")
-    ap.add_argument("--policy", default=None,
-                    help="planner policy jaccard_num,jaccard_den,inflation_num,inflation_den (default per workload)")
     ap.add_argument("--amin", type=int, default=0, choices=[0, 1],
                     help="flat frontier: 1 = one returning min per relaxation")
     ap.add_argument("--edge-major", type=int, default=0, choices=[0, 1],
@@ -237,6 +547,10 @@ def main():
                     help="with --engine frontier: near/far threshold step in mean edge weights (0 = plain frontier)")
     ap.add_argument("--tune-policy", action="store_true",
                     help="choose the planner policy by timing each candidate's plan (bfx_autotune_policy)")
+    ap.add_argument("--shard", action="store_true",
+                    help="multi-GPU: split one query set's batches over the ranks (strong scaling)")
+    ap.add_argument("--no-c3", action="store_true", help="skip the c3 object of the default c2 run")
+    ap.add_argument("--c3-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=None)
     args = ap.parse_args()
@@ -256,275 +570,42 @@ def main():
         tdist.init_process_group("nccl", timeout=timedelta(seconds=300))
         dist = tdist
 
-    import bfx
-    from bfx import replicas, workloads
-
-    t0 = time.time()
-    spec = dict(workloads.GRAPHS["c3" if args.workload in ("c5", "c3small") else args.workload])
-    if args.workload == "c3small":  # c3 generator on 128x128 tiles: a profiling-sized case of the c3 kernel
-        spec["tiles_x"] = spec["tiles_y"] = 128
-    g, order, gstats = bfx.synth_graph(**spec)
-    layout = bfx.build_device_graph_layout(g, order)
-    # query classes: (queries, plain-engine sample size) -- the plain per-query
-    # rate is extrapolated class by class from its sample
-    if args.workload == "c2":
-        grid = (128, 128)
-        queries = workloads.box_queries(layout, grid, args.queries or 256, 4, 64, 202 + 1000 * rank)
-        classes = [(queries, 64)]
-        policy = bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True)
-        workload_desc = ("c2: 256 uneven regional queries (box side U[4,64] tiles) on 128x128 tiles x 128 nodes, "
-                         "2,097,152 V / 16,777,216 E, f32 lognormal costs")
-    elif args.workload == "c3small":
-        grid = (128, 128)
-        queries = workloads.full_graph_queries(layout, grid, args.queries or 32, 303 + 1000 * rank)
-        classes = [(queries, 2)]
-        policy = bfx.BatchPlannerPolicy(32, 0, 1, 64, 1)
-        workload_desc = ("c3small: 32 full-graph sources in one batch of 32 on 128x128 tiles x 256 nodes, "
-                         "4,194,304 V / 41,943,040 E, uint costs U[1,255] (profiling-sized c3)")
-    elif args.workload == "c3":
-        grid = (256, 256)
-        queries = workloads.full_graph_queries(layout, grid, args.queries or 64, 303 + 1000 * rank)
-        classes = [(queries, 4)]
-        policy = bfx.BatchPlannerPolicy(32, 0, 1, 64, 1)
-        workload_desc = ("c3: 64 full-graph sources in batches of 32 on 256x256 tiles x 256 nodes, "
-                         "16,777,216 V / 167,772,160 E, uint costs U[1,255]")
-    else:
-        grid = (256, 256)
-        regional = workloads.box_queries(layout, grid, args.queries or 4096, 2, 16, 505 + 1000 * rank)
-        full = workloads.full_graph_queries(layout, grid, 16, 506 + 1000 * rank, first_id=len(regional))
-        queries = regional + full
-        classes = [(regional, 64), (full, 2)]
-        policy = bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True)
-        workload_desc = ("c5: 4,096 regional queries (box side U[2,16] tiles) + 16 full-graph sources on 256x256 "
-                         "tiles x 256 nodes, 16,777,216 V / 167,772,160 E, uint costs U[1,255]")
-    if args.policy:
-        jn, jd, inn, ind = (int(x) for x in args.policy.split(","))
-        policy = bfx.BatchPlannerPolicy(32, jn, jd, inn, ind, narrow_lanes=True)
-    t1 = time.time()
-    plan = bfx.make_overlapping_batch_plan(layout, queries, policy)
-    descs = plan.descriptions()
-    t2 = time.time()
-    lane_edges = sum(e[3] for e in plan.estimates)
-    log(f"[bench] graph+layout {t1 - t0:.1f}s plan {t2 - t1:.1f}s: {plan.batch_count} batches, "
-        f"widths {sorted({d.lane_width for d in descs})}, sum selected edges {lane_edges:,}")
+    from bfx import workloads
 
     device = local if world > 1 else 0
-    resident = bfx.ResidentDeviceGraph.upload_once(layout, device)
-    ws = bfx.Workspace(resident)
-    ws.set_frontier_layout({"flat": bfx.FRONTIER_FLAT, "groups": bfx.FRONTIER_GROUPS,
-                            "chunked": bfx.FRONTIER_CHUNKED}[args.frontier])
-    ws.set_register_budget(args.regs)
-    # the budget the library applies (blocks of 256 threads)
-    eff_regs = args.regs or (80 if args.frontier == "chunked" else 64)
-    if args.frontier != "chunked" and eff_regs == 80:
-        eff_regs = 64
-    ws.set_flat_items(args.items)
-    ws.set_relax_atomic(args.amin)
-    ws.set_flat_order(args.edge_major)
-    ws.set_chunk_pairs(args.pairs)
-    engine_id = {"auto": bfx.ENGINE_AUTO, "frontier": bfx.ENGINE_FRONTIER_PUSH, "jacobi": bfx.ENGINE_JACOBI_PULL,
-                 "dense": bfx.ENGINE_DENSE_CHAOTIC_PUSH}[args.engine]
-    engines_chosen = None
-    policy_times = None
-    if args.tune_policy:
-        # planner / autotuner co-design: the policy whose plan runs fastest
-        candidates = [policy] + [bfx.BatchPlannerPolicy(32, *c, narrow_lanes=True)
-                                 for c in ((1, 16, 4, 1), (1, 4, 2, 1), (1, 32, 8, 1))]
-        t4 = time.time()
-        best, policy_times = ws.autotune_policy(layout, queries, candidates)
-        policy = candidates[best]
-        plan = bfx.make_overlapping_batch_plan(layout, queries, policy)
-        descs = plan.descriptions()
-        lane_edges = sum(e[3] for e in plan.estimates)
-        log(f"[bench] policy tuning {time.time() - t4:.1f}s: times {policy_times}, best {best}, "
-            f"{plan.batch_count} batches")
-    if engine_id == bfx.ENGINE_AUTO:
-        t3 = time.time()
-        engines_chosen, measured = ws.autotune(descs)
-        log(f"[bench] autotune {time.time() - t3:.1f}s ({measured} batches timed): "
-            f"{ {e: engines_chosen.count(e) for e in set(engines_chosen)} } (0 jacobi, 1 dense, 2 frontier)")
-    elif args.step is not None:
-        # fixed near/far step for every batch (profiling a chosen step)
-        wbar = float(np.mean(layout.arrays["csr_weights"]))
-        ws.set_batch_deltas([float("inf") if args.step == 0 else args.step * wbar] * len(descs))
-    opts = bfx.GpuRunOptions(engine=engine_id)
-    opts_instr = bfx.GpuRunOptions(engine=engine_id, instrumentation=1)
-
-    import torch
-    torch.cuda.set_device(device)
-    stream = torch.cuda.ExternalStream(ws.stream, device=device)
-
-    def barrier():
-        torch.cuda.synchronize(device)
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize(device)
-
-    def max_over_ranks(x: float) -> float:
-        return replicas.max_over_ranks(dist, x) if dist else x
-
-    # ---- instrumented pass (untimed): algorithmic work counts + parity spot check
-    ws.prepare(descs)
-    ws.execute(opts_instr)
-    statuses = ws.fetch_statuses()
-    work = ws.work_counters()
-    engine_work = ws.engine_work()
-    assert all(s.stop_reason == bfx.STOP_CONVERGED for s in statuses), "benchmark run did not converge"
-    reached = sum(bin(s.reached_target_mask).count("1") for s in statuses)
-
-    # ---- device-resident timing (value)
-    for _ in range(args.warmup):
-        ws.execute(opts)
-    barrier()
-    with ClockSampler(device) as clocks:
-        start = torch.cuda.Event(enable_timing=True)
-        end = torch.cuda.Event(enable_timing=True)
-        start.record(stream)
-        # NVTX range: lets a profiler select the timed launches
-        # (ncu --nvtx --nvtx-include "bench_timed/")
-        torch.cuda.nvtx.range_push("bench_timed")
-        for _ in range(args.steps):
-            ws.execute(opts)
-        torch.cuda.nvtx.range_pop()
-        end.record(stream)
-        barrier()
-    dev_ms = start.elapsed_time(end)
-    # Relaxation-kernel time per launch (library events on the same stream),
-    # sampled right after the timed region.
-    kernel_ms, execute_ms = [], []
-    for _ in range(3):
-        ws.execute(opts)
-        k, x = ws.last_execute_timing()
-        kernel_ms.append(k)
-        execute_ms.append(x)
-    launches_per_step = ws.last_launch_count()
-    dev_ms = max_over_ranks(dev_ms)
-    log(f"[bench] device-resident: {dev_ms / args.steps:.3f} ms/step, relaxation kernel {np.mean(kernel_ms):.3f} ms")
-    statuses = ws.fetch_statuses()
-    assert all(s.stop_reason == bfx.STOP_CONVERGED for s in statuses)
-    if dist:  # the job's one exchange: every rank's status records to every rank
-        all_statuses = replicas.gather_statuses(dist, statuses)
-        assert all(s.stop_reason == bfx.STOP_CONVERGED for part in all_statuses for s in part)
-
-    # ---- end-to-end timing through the C ABI from host buffers (e2e)
-    for _ in range(args.warmup):
-        ws.prepare(descs)
-        ws.execute(opts)
-        ws.fetch_statuses()
-    barrier()
-    s2 = torch.cuda.Event(enable_timing=True)
-    e2 = torch.cuda.Event(enable_timing=True)
-    s2.record(stream)
-    for _ in range(args.steps):
-        ws.prepare(descs)
-        ws.execute(opts)
-        ws.fetch_statuses()
-    e2.record(stream)
-    barrier()
-    e2e_ms = max_over_ranks(s2.elapsed_time(e2))
-    log(f"[bench] end-to-end: {e2e_ms / args.steps:.3f} ms/step")
-    h2d, d2h = ws.transfer_bytes()
-
-    # ---- plain per-query engine (one query per launch sequence) on a sample
-    # of each query class; the whole set's time is extrapolated per class.
-    # The baseline is the faster of the frontier layouts for single queries.
-    plain_by_layout = {}
-    for lname, lid in (("chunked", bfx.FRONTIER_CHUNKED), ("flat", bfx.FRONTIER_FLAT)):
-        ws.set_frontier_layout(lid)
-        plain_total_s, plain_sampled = 0.0, 0
-        for members, n in classes:
-            sample_q = members[:n]
-            ws.run_query(sample_q[0].sources, sample_q[0].targets, sample_q[0].selected_tiles,
-                         bfx.GpuRunOptions(engine=bfx.ENGINE_FRONTIER_PUSH))  # warm-up
-            barrier()
-            s3 = torch.cuda.Event(enable_timing=True)
-            e3 = torch.cuda.Event(enable_timing=True)
-            s3.record(stream)
-            for q in sample_q:
-                ws.run_query(q.sources, q.targets, q.selected_tiles, bfx.GpuRunOptions(engine=bfx.ENGINE_FRONTIER_PUSH))
-            e3.record(stream)
-            barrier()
-            plain_total_s += s3.elapsed_time(e3) / 1000 / len(sample_q) * len(members)
-            plain_sampled += len(sample_q)
-        plain_by_layout[lname] = len(queries) / plain_total_s
-    ws.set_frontier_layout({"flat": bfx.FRONTIER_FLAT, "groups": bfx.FRONTIER_GROUPS,
-                            "chunked": bfx.FRONTIER_CHUNKED}[args.frontier])
-    plain_layout = max(plain_by_layout, key=plain_by_layout.get)
-    plain_qps = plain_by_layout[plain_layout]
-
-    nq = len(queries) * world
-    ms_per_step = dev_ms / args.steps
-    value = nq / (ms_per_step / 1000)
-    e2e_value = nq / (e2e_ms / args.steps / 1000)
-    kernel_avg = float(np.mean(kernel_ms))
-    # algorithmic bytes per launch, per engine class:
-    #   push (frontier, dense): 16 F + 12 S + 8 P + 16 L + 8 N (dense has N = 0)
-    #   Jacobi pull:            16 (vertex-lane items) + 12 (in-edge records) + 8 (relaxations)
-    pw, jw = engine_work["push"], engine_work["jacobi"]
-    F, S, Pp, L, N = (pw[k] for k in ("entries", "records", "active_pairs", "relaxations", "claims"))
-    alg_bytes = (16 * F + 12 * S + 8 * Pp + 16 * L + 8 * N +
-                 16 * jw["items"] + 12 * jw["records"] + 8 * jw["relaxations"])
-    peaks_path = REPO / "MEASURED_PEAKS.json"
-    if peaks_path.exists():
-        peak = json.loads(peaks_path.read_text())["hbm_gbs"]
-        peak_src = "measured"
-    else:
-        peak, peak_src = 6650.0, "fallback"
-    achieved = alg_bytes / (kernel_avg / 1000) / 1e9
-    traffic, traffic_source, random_ceiling = traffic_estimate(args.workload, work["relaxations"], kernel_avg)
-
-    line = {
-        "metric": METRICS[args.workload], "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_desc,
-                   "queries_per_gpu": len(queries), "batches": plan.batch_count,
-                   "lane_widths": sorted({d.lane_width for d in descs}), "engine": args.engine,
-                   "policy_times_ms": policy_times,
-                   "planner_policy": [policy.minimum_jaccard_numerator, policy.minimum_jaccard_denominator,
-                                      policy.maximum_union_inflation_numerator,
-                                      policy.maximum_union_inflation_denominator],
-                   "near_far_step": args.step,
-                   "frontier_layout": args.frontier, "registers": eff_regs, "flat_items": args.items, "returning_min": args.amin, "edge_major": args.edge_major, "chunk_pairs": args.pairs,
-                   "engines_chosen": None if engines_chosen is None else
-                   {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
-                   "frontier_steps_chosen": None if engines_chosen is None else
-                   {("plain" if not np.isfinite(d) else f"{d:.4g}"): sum(
-                       1 for e, x in zip(engines_chosen, ws.tuned_deltas) if e == 2 and x == d)
-                    for d in sorted({x for e, x in zip(engines_chosen, ws.tuned_deltas) if e == 2})},
-                   "control": "persistent_cooperative", "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (graph %s GB + labels), no flush" % (
-                       {"c2": "0.54", "c3small": "1.3"}.get(args.workload, "5.4"))},
-        "gteps": lane_edges * world / (ms_per_step / 1000) / 1e9,
-        "reached_lanes": reached,
-        "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "plain_per_query": {"value": plain_qps, "unit": "queries/s", "sample": plain_sampled,
-                            "layout": plain_layout, "by_layout": plain_by_layout,
-                            "batched_speedup": value / world / plain_qps},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "traffic_source": traffic_source, "peak_source": peak_src,
-                     "random_sector_ceiling": random_ceiling, "kernel": "persistent_kernel (%s frontier, %d registers, %d items%s)" % (
-                         args.frontier, eff_regs, args.items if (eff_regs == 64 and args.frontier != "chunked") or (
-                             eff_regs == 80 and args.frontier == "chunked" and not args.pairs) else 2,
-                         ", mixed engines" if engines_chosen and any(e != 2 for e in engines_chosen) else ""),
-                     "kernel_ms": kernel_avg, "execute_ms": float(np.mean(execute_ms)),
-                     "algorithmic_bytes_per_launch": alg_bytes, "work": work, "engine_work": engine_work},
-        "clocks": clocks.summary(),
-        "gpu_launches": launches_per_step * args.steps,
-    }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
+    t0 = time.time()
+    wl = workloads.bench_workload(args.workload, 0 if args.shard else rank, args.queries)
+    log(f"[bench] graph+layout {time.time() - t0:.1f}s")
+    cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
+    threads = os.cpu_count() or 1
+    # the cpu_baseline sample: 32 queries spread over the set (regional
+    # workloads), or a few full-graph sources
+    nsample = 32 if args.workload in ("c2", "c5") else min(2, len(wl.queries))
+    sample_ids = sorted(np.random.default_rng(2024).choice(len(wl.queries), nsample, replace=False).tolist()) \
+        if cpu_leg else []
+    line, lane_images = measure(wl, args, rank=rank, world=world, dist=dist, device=device, steps=args.steps,
+                                warmup=args.warmup, shard=args.shard, sample_ids=sample_ids)
+    if cpu_leg:
         try:
-            cb = cpu_reference_baseline(g, order, queries, 32, threads) if args.workload == "c2" else None
+            cb, parity = cpu_baseline_and_parity(wl, lane_images, sample_ids, threads)
         except Exception as exc:  # reference build unusable here
-            log(f"[bench] reference baseline failed: {exc}")
-            cb = None
-        line["cpu_baseline"] = cb or cpu_port_baseline(layout, queries, 32 if args.workload == "c2" else threads,
-                                                       threads)
+            log(f"[bench] cpu baseline failed: {exc}")
+            cb, parity = None, None
+        line["cpu_baseline"] = cb
+        line["parity"] = parity
+    if args.workload == "c2" and world == 1 and not args.no_c3 and args.queries is None:
+        # the c3 full-graph configuration, timed in the same run (its own roofline)
+        del wl
+        t0 = time.time()
+        wl3 = workloads.bench_workload("c3")
+        log(f"[bench] c3 graph+layout {time.time() - t0:.1f}s")
+        c3, _ = measure(wl3, args, rank=rank, world=world, dist=dist, device=device, steps=args.c3_steps,
+                        warmup=3, shard=False)
+        line["c3"] = {k: c3[k] for k in ("metric", "value", "unit", "steps", "warmup", "ms_per_step", "gteps",
+                                          "e2e", "host", "roofline", "clocks", "config", "plain_per_query",
+                                          "max_finite_distance", "gpu_launches")}
     if rank == 0:
         print(json.dumps(line))
-    ws.close()
-    resident.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -622,6 +622,20 @@ class Workspace:
         _check(load().bfx_download_labels(self._h, u32(batch), _ptr(bits), _ptr(pred)))
         return bits.reshape(V, lane_width), pred.reshape(V, lane_width)
 
+    def download_lane(self, batch: int, lane: int):
+        """One lane of a batch as graph-sized (distance bits, predecessor edge ids)."""
+        V = self.graph.layout.vertex_count
+        bits = np.empty(V, np.uint32)
+        pred = np.empty(V, np.uint32)
+        _check(load().bfx_download_lane_labels(self._h, u32(batch), u32(lane), _ptr(bits), _ptr(pred)))
+        return bits, pred
+
+    def label_bounds(self) -> np.ndarray:
+        """Largest finite distance bits per prepared batch (0: nothing beyond the sources)."""
+        out = np.zeros(self.batch_count, np.uint32)
+        _check(load().bfx_fetch_label_bounds(self._h, _ptr(out)))
+        return out
+
     def last_launch_count(self) -> int:
         n = u64()
         _check(load().bfx_last_launch_count(self._h, C.byref(n)))

@@ -165,3 +165,74 @@ def shard_batches(lane_edge_estimates, world: int) -> list:
         shards[r].append(b)
         loads[r] += int(lane_edge_estimates[b])
     return [sorted(s) for s in shards]
+
+
+@dataclass
+class BenchWorkload:
+    """A timed configuration: graph input, layout, query set, the query
+    classes the plain per-query baseline samples (queries, sample size) and
+    the planner policy."""
+    name: str
+    graph_input: object
+    order: object
+    layout: DeviceGraphLayout
+    grid: tuple
+    queries: list
+    classes: list
+    policy: BatchPlannerPolicy
+    description: str
+    uint_costs: bool
+
+
+def bench_queries(name: str, tiles, grid, rank: int = 0, query_count: int | None = None):
+    """(queries, classes) of a timed configuration, from the tile table of its
+    layout (`tiles`: any object with the layout's `.tiles` dict and
+    `.vertex_count`), so the reference's own layout of the same input gives
+    the same queries.  Rank r of a replica run draws its own set (seed
+    offset 1000 r)."""
+    off = 1000 * rank
+    if name == "c2":
+        qs = box_queries(tiles, grid, query_count or 256, 4, 64, 202 + off)
+        return qs, [(qs, 64)]
+    if name in ("c3", "c3small"):
+        qs = full_graph_queries(tiles, grid, query_count or (64 if name == "c3" else 32), 303 + off)
+        return qs, [(qs, 4 if name == "c3" else 2)]
+    if name == "c5":
+        regional = box_queries(tiles, grid, query_count or 4096, 2, 16, 505 + off)
+        full = full_graph_queries(tiles, grid, 16, 506 + off, first_id=len(regional))
+        return regional + full, [(regional, 64), (full, 2)]
+    raise ValueError(f"unknown timed workload {name}")
+
+
+def bench_graph_spec(name: str) -> tuple[dict, tuple]:
+    """Synthetic graph parameters and tile grid of a timed configuration."""
+    spec = dict(GRAPHS["c3" if name in ("c5", "c3small") else name])
+    if name == "c3small":  # c3 generator on 128x128 tiles: a profiling-sized case of the c3 kernel
+        spec["tiles_x"] = spec["tiles_y"] = 128
+    return spec, (spec["tiles_x"], spec["tiles_y"])
+
+
+BENCH_DESCRIPTIONS = {
+    "c2": ("c2: 256 uneven regional queries (box side U[4,64] tiles) on 128x128 tiles x 128 nodes, "
+           "2,097,152 V / 16,777,216 E, f32 lognormal costs"),
+    "c3small": ("c3small: 32 full-graph sources in one batch of 32 on 128x128 tiles x 256 nodes, "
+                "4,194,304 V / 41,943,040 E, uint costs U[1,255] (profiling-sized c3)"),
+    "c3": ("c3: 64 full-graph sources in batches of 32 on 256x256 tiles x 256 nodes, "
+           "16,777,216 V / 167,772,160 E, uint costs U[1,255]"),
+    "c5": ("c5: 4,096 regional queries (box side U[2,16] tiles) + 16 full-graph sources on 256x256 "
+           "tiles x 256 nodes, 16,777,216 V / 167,772,160 E, uint costs U[1,255]"),
+}
+
+
+def bench_workload(name: str, rank: int = 0, query_count: int | None = None, threads: int = 0) -> BenchWorkload:
+    """The exact graph, query set and planner policy that bench.py times."""
+    spec, grid = bench_graph_spec(name)
+    g, order, _ = synth_graph(**spec)
+    layout = build_device_graph_layout(g, order, threads)
+    queries, classes = bench_queries(name, layout, grid, rank, query_count)
+    if name in ("c2", "c5"):
+        policy = BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True)
+    else:
+        policy = BatchPlannerPolicy(32, 0, 1, 64, 1)
+    return BenchWorkload(name, g, order, layout, grid, queries, classes, policy, BENCH_DESCRIPTIONS[name],
+                         spec["cost_kind"] == 0)

@@ -768,6 +768,45 @@ __global__ void expand_kernel(DGraph g, DBatch B, u32 slot, u32* bits, u32* pred
   }
 }
 
+// One lane of a batch as a graph-sized image.
+__global__ void expand_lane_kernel(DGraph g, DBatch B, u32 slot, u32 lane, u32* bits, u32* preds) {
+  for (u32 v = blockIdx.x * blockDim.x + threadIdx.x; v < g.V; v += gridDim.x * blockDim.x) {
+    const uint2 t = B.tiles[g.owner[v]];
+    u64 w = dev::kUnreached;
+    if ((t.x >> lane) & 1u) w = B.dist[slot][(static_cast<u64>(v - t.y) << B.shift) + lane];
+    if (bits) bits[v] = dev::hi(w);
+    if (preds) {
+      const u32 lo = static_cast<u32>(w);
+      preds[v] = (lo == 0u || lo == 0xFFFFFFFFu) ? 0xFFFFFFFFu : lo - 1u;
+    }
+  }
+}
+
+// Largest finite distance bits per batch over the final labels (grid-stride
+// over the union vertices of all batches, as init_kernel); out[b] starts at 0.
+__global__ void label_bound_kernel(LaunchParams p, const bfx_device_run_status* statuses, u32* out) {
+  const u64 tid = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+  const u32 total_units = p.unit_base[p.nb];
+  u32 best = 0u, best_b = 0xFFFFFFFFu;
+  for (u64 u = tid; u < total_units; u += stride) {
+    const u32 b = find_batch(p.unit_base, p.nb, static_cast<u32>(u));
+    if (b != best_b) {
+      if (best_b != 0xFFFFFFFFu && best != 0u) atomicMax(out + best_b, best);
+      best_b = b;
+      best = 0u;
+    }
+    const DBatch& B = p.batches[b];
+    const u32 cv = static_cast<u32>(u) - p.unit_base[b];
+    const u64* const d = B.dist[statuses[b].final_distance_slot] + (static_cast<u64>(cv) << B.shift);
+    for (u32 l = 0; l < B.W; ++l) {
+      const u32 h = dev::hi(d[l]);
+      if (h < dev::kInfBits && h > best) best = h;
+    }
+  }
+  if (best_b != 0xFFFFFFFFu && best != 0u) atomicMax(out + best_b, best);
+}
+
 // ---------------------------------------------------------------------------
 }  // namespace bfx
 
@@ -1548,6 +1587,55 @@ int bfx_download_labels(bfx_workspace* ws, uint32_t batch, uint32_t* distance_bi
     }
     cudaFreeAsync(d_out, ws->stream);
     BFX_CUDA(le);
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+  });
+}
+
+int bfx_download_lane_labels(bfx_workspace* ws, uint32_t batch, uint32_t lane, uint32_t* distance_bits,
+                             uint32_t* predecessor_edges) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null workspace");
+    bfx::require(ws->executed, "no executed batches");
+    if (batch >= ws->nb) throw std::out_of_range("batch index");
+    const bfx::DBatch& B = ws->batches[batch];
+    if (lane >= B.W) throw std::out_of_range("lane index");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    const size_t n = ws->graph->g.V;
+    bfx_device_run_status st;
+    BFX_CUDA(cudaMemcpyAsync(&st, ws->d_status + batch, sizeof(st), cudaMemcpyDeviceToHost, ws->stream));
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    std::uint32_t* d_out = nullptr;
+    BFX_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_out), n * 8, ws->stream));
+    bfx::expand_lane_kernel<<<ws->sm_count * 8, 256, 0, ws->stream>>>(ws->graph->g, B, st.final_distance_slot, lane,
+                                                                      d_out, d_out + n);
+    const cudaError_t le = cudaGetLastError();
+    if (le == cudaSuccess) {
+      if (distance_bits) cudaMemcpyAsync(distance_bits, d_out, n * 4, cudaMemcpyDeviceToHost, ws->stream);
+      if (predecessor_edges) cudaMemcpyAsync(predecessor_edges, d_out + n, n * 4, cudaMemcpyDeviceToHost, ws->stream);
+    }
+    cudaFreeAsync(d_out, ws->stream);
+    BFX_CUDA(le);
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+  });
+}
+
+int bfx_fetch_label_bounds(bfx_workspace* ws, uint32_t* max_finite_distance_bits) {
+  return bfx::guarded([&] {
+    bfx::require(ws && max_finite_distance_bits, "null argument");
+    bfx::require(ws->executed, "no executed batches");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    std::uint32_t* d_out = nullptr;
+    BFX_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_out), size_t{ws->nb} * 4, ws->stream));
+    cudaError_t e = cudaMemsetAsync(d_out, 0, size_t{ws->nb} * 4, ws->stream);
+    if (e == cudaSuccess) {
+      bfx::label_bound_kernel<<<ws->sm_count * 8, 256, 0, ws->stream>>>(ws->params, ws->d_status, d_out);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+      e = cudaMemcpyAsync(max_finite_distance_bits, d_out, size_t{ws->nb} * 4, cudaMemcpyDeviceToHost, ws->stream);
+    }
+    cudaFreeAsync(d_out, ws->stream);
+    BFX_CUDA(e);
     BFX_CUDA(cudaStreamSynchronize(ws->stream));
   });
 }

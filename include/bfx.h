@@ -208,6 +208,20 @@ int bfx_run_batches(bfx_workspace *ws, uint32_t count, const bfx_batch_descripti
 int bfx_download_labels(bfx_workspace *ws, uint32_t batch, uint32_t *distance_bits,
                         uint32_t *predecessor_edges);
 
+/* One lane of batch `batch` as a graph-sized V image, same encoding as
+ * bfx_download_labels (bfx extension: a width-32 batch over a 16.8M-vertex
+ * graph is 4.3 GB whole, so checkers fetch the lanes they compare).  Lanes
+ * at or above the batch's width fail with BFX_ERR_OUT_OF_RANGE. */
+int bfx_download_lane_labels(bfx_workspace *ws, uint32_t batch, uint32_t lane, uint32_t *distance_bits,
+                             uint32_t *predecessor_edges);
+
+/* Largest finite distance (float bits) among the final labels of every
+ * prepared batch, one word per batch; 0 when a batch reached nothing but
+ * its sources (bfx extension).  Integer costs stay exact in float sums only
+ * while every distance is below 2^24 (bits 0x4B800000): checkers of integer-
+ * cost workloads assert that bound with this. */
+int bfx_fetch_label_bounds(bfx_workspace *ws, uint32_t *max_finite_distance_bits);
+
 /* Device time of the most recent bfx_execute, measured by CUDA events the
  * library records on the workspace stream: out[0] = relaxation kernels
  * (the persistent launch, or all round/advance launches of a host-poll run),

@@ -118,6 +118,16 @@ class Oracle:
         return grad
 
 
+class RefTiles:
+    """Tile table of a reference case, shaped like a layout's `.tiles` for the
+    query samplers (bfx.workloads.box_queries / full_graph_queries)."""
+
+    def __init__(self, tiles: dict, vertex_count: int, tile_count: int):
+        self.tiles = tiles
+        self.vertex_count = vertex_count
+        self.tile_count = tile_count
+
+
 class Ref:
     """The reference's own CPU library (oracle/_ref), when built."""
 
@@ -144,6 +154,44 @@ class Ref:
             _p(g.resource_class, C.c_uint16), u64(g.edge_count), _p(g.edge_source), _p(g.edge_destination),
             _p(g.edge_weight, f32), _p(g.provenance_domain), _p(g.provenance_kind), _p(g.provenance_record, u64),
             C.c_int32(order.origin_x), C.c_int32(order.origin_y), u32(order.tile_width), u32(order.tile_height)))
+
+    def case_synth(self, spec: dict) -> int:
+        """A case from the synthetic graph generator restated in ref_driver.cpp
+        (same parameters as bfx.workloads.GRAPHS), partitioned by the reference."""
+        spans = np.zeros(8, np.uint32)
+        spans[:len(spec["spans"])] = spec["spans"]
+        base = np.zeros(8, np.float32)
+        base[:len(spec.get("span_base", ()))] = spec.get("span_base", ())
+        return self._chk(self.lib.ref_case_synth(
+            u32(spec["tiles_x"]), u32(spec["tiles_y"]), u32(spec["nodes_per_tile"]), u32(spec["intra"]),
+            u32(spec["inter"]), u32(len(spec["spans"])), _p(spans), u32(spec.get("cost_kind", 0)),
+            u32(spec.get("cost_lo", 1)), u32(spec.get("cost_hi", 64)), f32(spec.get("intra_base", 1.0)),
+            _p(base, f32), f32(spec.get("sigma", 0.5)), u64(spec["seed"])))
+
+    def tiles(self, h) -> "RefTiles":
+        """The case's tile table (coordinates, located flags, vertex offsets)."""
+        c = self.counts(h)
+        T = c["T"]
+        xy = np.zeros(2 * T, np.int64)
+        has = np.zeros(T, np.uint8)
+        tvo = np.zeros(T + 1, np.uint32)
+        nul = [None] * 16
+        self._chk(self.lib.ref_case_layout(C.c_int(h), *nul, _p(xy, C.c_int64), _p(has, C.c_uint8), _p(tvo)))
+        return RefTiles({"tile_xy": xy.reshape(T, 2), "has_location": has, "tile_vertex_offsets": tvo}, c["V"], T)
+
+    def time_dijkstra_steps(self, h, qidx, threads: int, warmup: int, steps: int, want_dist: bool = False):
+        """Induced graphs built once, then `warmup` + `steps` passes of
+        dijkstra_oracle over all listed queries (one query per thread)."""
+        q = np.ascontiguousarray(qidx, np.uint32)
+        walls = np.zeros(max(steps, 1), np.float64)
+        ind = C.c_double()
+        edges = u64()
+        dist = np.zeros((len(q), self.counts(h)["V"]), np.float32) if want_dist else None
+        self._chk(self.lib.ref_time_dijkstra_steps(C.c_int(h), u32(len(q)), _p(q), u32(threads), u32(warmup),
+                                                   u32(steps), _p(walls, C.c_double), C.byref(ind),
+                                                   C.byref(edges), _p(dist, f32)))
+        return {"step_s": walls[:steps].tolist(), "induced_wall_s": ind.value, "edges": int(edges.value),
+                "dist": dist}
 
     def fixture_count(self, suite: str) -> int:
         return self.lib.ref_fixture_count(suite.encode())

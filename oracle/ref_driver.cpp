@@ -43,7 +43,10 @@
 #include "jacobi_fixture_suite.hpp"
 
 #include <atomic>
+#include <algorithm>
 #include <bit>
+#include <cmath>
+#include <limits>
 #include <chrono>
 #include <cstdint>
 #include <cstring>
@@ -165,6 +168,182 @@ int ref_case_from_input(
     InputGraph input{std::move(vertices), std::move(edges)};
     const UniformGridPartitioner part{SpatialOrderConfig{ox, oy, tw, th}};
     return store(from_partitioned("input", part.partition(input)));
+  });
+}
+
+// Synthetic spatial graph straight into the reference's partitioner, so the
+// reference arm of the benchmark needs nothing from the product library.
+// The generator restates the product's seeded synthetic workload
+// (xoshiro256** seeded through splitmix64, multiply-shift uniform integers
+// from the top 32 bits, Box-Muller normals in double rounded once to float;
+// tiles of tile_width x tile_height local coordinates, row-major tile ids,
+// intra-tile edges to another uniform node of the tile, inter-tile edges to a
+// uniform 4-neighbour at a uniform span, redrawn up to 16 times off the grid
+// and then clamped to the border); tests/test_ref_synth.py checks that both
+// produce the same graph.
+namespace {
+
+struct SynthRng {
+  std::uint64_t s[4];
+  explicit SynthRng(std::uint64_t seed) {
+    std::uint64_t x = seed;
+    for (int i = 0; i < 4; ++i) {
+      x += 0x9E3779B97F4A7C15ULL;
+      std::uint64_t z = x;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+      s[i] = z ^ (z >> 31);
+    }
+  }
+  std::uint64_t next() {
+    auto rotl = [](std::uint64_t v, int k) { return (v << k) | (v >> (64 - k)); };
+    const std::uint64_t out = rotl(s[1] * 5U, 7) * 9U;
+    const std::uint64_t t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = rotl(s[3], 45);
+    return out;
+  }
+  std::uint32_t uniform(std::uint32_t n) { return static_cast<std::uint32_t>(((next() >> 32) * n) >> 32); }
+  double unit() { return static_cast<double>(next() >> 11) / 9007199254740992.0; }
+  double gauss() {
+    const double a = 1.0 - unit();
+    const double b = unit();
+    return std::sqrt(-2.0 * std::log(a)) * std::cos(6.283185307179586476925 * b);
+  }
+};
+
+}  // namespace
+
+int ref_case_synth(std::uint32_t tiles_x, std::uint32_t tiles_y, std::uint32_t nodes, std::uint32_t intra,
+                   std::uint32_t inter, std::uint32_t span_count, const std::uint32_t* spans,
+                   std::uint32_t cost_kind, std::uint32_t cost_lo, std::uint32_t cost_hi, float intra_base,
+                   const float* span_base, float sigma, std::uint64_t seed) {
+  return guarded([&] {
+    if (tiles_x == 0 || tiles_y == 0 || nodes < 2 || span_count == 0 || span_count > 8) {
+      throw std::invalid_argument{"bad synthetic graph parameters"};
+    }
+    std::uint32_t w = nodes, h = 1;
+    if (nodes == 128U) {
+      w = 16;
+      h = 8;
+    } else {
+      const auto r = static_cast<std::uint32_t>(std::lround(std::sqrt(static_cast<double>(nodes))));
+      if (r * r == nodes) w = h = r;
+    }
+    const std::uint64_t V = std::uint64_t{tiles_x} * tiles_y * nodes;
+    std::vector<VertexMetadata> vertices;
+    vertices.reserve(V);
+    std::vector<EdgeInputRecord> edges;
+    edges.reserve(V * (intra + inter));
+    SynthRng rng(seed);
+    auto draw_cost = [&](int span) -> float {
+      if (cost_kind == 0U) return static_cast<float>(cost_lo + rng.uniform(cost_hi - cost_lo + 1U));
+      const double base = span < 0 ? intra_base : span_base[span];
+      return static_cast<float>(base * std::exp(static_cast<double>(sigma) * rng.gauss()));
+    };
+    const int step_x[4] = {1, -1, 0, 0};
+    const int step_y[4] = {0, 0, 1, -1};
+    std::uint64_t record = 0;
+    for (std::uint32_t ty = 0; ty < tiles_y; ++ty) {
+      for (std::uint32_t tx = 0; tx < tiles_x; ++tx) {
+        const std::uint64_t tile = std::uint64_t{ty} * tiles_x + tx;
+        for (std::uint32_t i = 0; i < nodes; ++i) {
+          const std::uint64_t v = tile * nodes + i;
+          vertices.push_back(VertexMetadata::located(static_cast<std::int32_t>(tx * w + i % w),
+                                                     static_cast<std::int32_t>(ty * h + i / w), ResourceClassId{1U}));
+          for (std::uint32_t j = 0; j < intra; ++j) {
+            std::uint32_t other = rng.uniform(nodes - 1U);
+            other += other >= i ? 1U : 0U;
+            const float c = draw_cost(-1);
+            edges.push_back(EdgeInputRecord{VertexId{static_cast<std::uint32_t>(v)},
+                                            VertexId{static_cast<std::uint32_t>(tile * nodes + other)}, c,
+                                            PhysicalProvenance{1U, 1U, record++}});
+          }
+          for (std::uint32_t j = 0; j < inter; ++j) {
+            std::int64_t nx = 0, ny = 0;
+            std::uint32_t si = 0;
+            bool inside = false;
+            for (int attempt = 0; attempt < 16 && !inside; ++attempt) {
+              const std::uint32_t dir = rng.uniform(4U);
+              si = rng.uniform(span_count);
+              nx = static_cast<std::int64_t>(tx) + step_x[dir] * static_cast<std::int64_t>(spans[si]);
+              ny = static_cast<std::int64_t>(ty) + step_y[dir] * static_cast<std::int64_t>(spans[si]);
+              inside = nx >= 0 && ny >= 0 && nx < tiles_x && ny < tiles_y;
+            }
+            nx = std::clamp<std::int64_t>(nx, 0, tiles_x - 1);
+            ny = std::clamp<std::int64_t>(ny, 0, tiles_y - 1);
+            const std::uint64_t other_tile = static_cast<std::uint64_t>(ny) * tiles_x + static_cast<std::uint64_t>(nx);
+            const std::uint32_t node = rng.uniform(nodes);
+            const float c = draw_cost(static_cast<int>(si));
+            edges.push_back(EdgeInputRecord{VertexId{static_cast<std::uint32_t>(v)},
+                                            VertexId{static_cast<std::uint32_t>(other_tile * nodes + node)}, c,
+                                            PhysicalProvenance{1U, 1U, record++}});
+          }
+        }
+      }
+    }
+    InputGraph input{std::move(vertices), std::move(edges)};
+    const UniformGridPartitioner part{SpatialOrderConfig{0, 0, w, h}};
+    return store(from_partitioned("synthetic", part.partition(input)));
+  });
+}
+
+// CPU baseline over several timed steps: the induced graphs of the listed
+// queries are built once (in parallel; their wall time goes to
+// *induced_wall_seconds), then `warmup` untimed and `steps` timed passes run
+// dijkstra_oracle over all of them, one query at a time per host thread.
+// step_seconds[i] receives the wall time of timed pass i; *edges_out the
+// summed induced edge counts.  dist_out (optional, nq x V floats) receives
+// each query's distances of the last pass, mapped back to global ids (+inf
+// outside the selected tiles).
+int ref_time_dijkstra_steps(int h, std::uint32_t nq, const std::uint32_t* qidx, std::uint32_t threads,
+                            std::uint32_t warmup, std::uint32_t steps, double* step_seconds,
+                            double* induced_wall_seconds, std::uint64_t* edges_out, float* dist_out) {
+  return guarded([&]() -> int {
+    RefCase* c = get(h);
+    if (!c) throw std::invalid_argument{"bad handle"};
+    if (threads == 0) threads = 1;
+    const WeightedGraph& g = c->partitioned->graph;
+    std::vector<std::optional<InducedQueryGraph>> induced(nq);
+    auto run_pool = [&](auto&& body) {
+      std::atomic<std::uint32_t> next{0U};
+      std::vector<std::thread> pool;
+      for (std::uint32_t t = 0; t < threads; ++t) {
+        pool.emplace_back([&] {
+          for (std::uint32_t i; (i = next.fetch_add(1U)) < nq;) body(i);
+        });
+      }
+      for (auto& th : pool) th.join();
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    run_pool([&](std::uint32_t i) { induced[i].emplace(build_induced_query_graph(g, c->queries.at(qidx[i]))); });
+    if (induced_wall_seconds) {
+      *induced_wall_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    std::uint64_t edges = 0;
+    for (const auto& ig : induced) edges += ig->graph.edge_count();
+    if (edges_out) *edges_out = edges;
+    for (std::uint32_t pass = 0; pass < warmup + steps; ++pass) {
+      const bool last = pass + 1U == warmup + steps;
+      const auto a = std::chrono::steady_clock::now();
+      run_pool([&](std::uint32_t i) {
+        const SsspResult res = dijkstra_oracle(induced[i]->graph, induced[i]->sources);
+        if (last && dist_out) {
+          float* d = dist_out + std::uint64_t{i} * g.vertex_count();
+          std::fill(d, d + g.vertex_count(), std::numeric_limits<float>::infinity());
+          for (std::size_t l = 0; l < induced[i]->local_to_global.size(); ++l) {
+            d[induced[i]->local_to_global[l].value()] = res.distances[l];
+          }
+        }
+      });
+      const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
+      if (pass >= warmup && step_seconds) step_seconds[pass - warmup] = wall;
+    }
+    return 0;
   });
 }
 

@@ -16,24 +16,38 @@ def load_bench():
 
 def test_traffic_estimate_scales_the_committed_captures():
     """Traffic = the capture's bytes per relaxation x this launch's
-    relaxations (c2 from the c2 capture, c3/c5 from the c3-shaped one), and
-    the DRAM rate is reported against the random-sector ceiling."""
+    relaxations (c2 from the c2 capture, c3/c5 from the c3-shaped one), only
+    for a launch at the capture's near/far step; the DRAM rate is reported
+    against the random-sector ceiling."""
     bench = load_bench()
     rows = {}
     for line in (REPO / "profiles" / "frontier_push_traffic.txt").read_text().splitlines():
         parts = line.split()
-        if parts and not line.startswith("#") and len(parts) == 4:
-            rows[parts[0]] = (int(parts[1]), int(parts[2]))
+        if parts and not line.startswith("#") and len(parts) == 5:
+            rows[parts[0]] = (int(parts[1]), int(parts[2]), parts[3])
     for workload, key in (("c2", "c2"), ("c3", "c3small"), ("c5", "c3small")):
-        b, rl = rows[key]
-        t, src, ceil = bench.traffic_estimate(workload, 2 * rl, 10.0)
+        b, rl, step = rows[key]
+        t, src, ceil = bench.traffic_estimate(workload, 2 * rl, 10.0, step)
         assert t == pytest.approx(2 * b, rel=1e-9)
         assert src.endswith(f"{2 * rl:,} relaxations")
         assert ceil["dram_gbs"] == pytest.approx(2 * b / 0.010 / 1e9)
         assert 0 < ceil["frac"] and ceil["peak_gbs"] > 0
+        # another step: not scaled, and the source says why
+        t, src, ceil = bench.traffic_estimate(workload, 2 * rl, 10.0, "another")
+        assert t is None and ceil is None and "not scaled" in src
     assert bench.traffic_estimate("c2", 0, 10.0) == (None, None, None)
+
+
+def test_step_label():
+    bench = load_bench()
+    inf = float("inf")
+    assert bench.step_label([2, 2], [2.0, 2.0], 2.0) == "1"
+    assert bench.step_label([2, 2], [inf, inf], 2.0) == "plain"
+    assert bench.step_label([2, 0], [1.0, inf], 2.0) == "0.5"
+    assert bench.step_label([2, 2], [1.0, 4.0], 2.0) == "mixed"
+    assert bench.step_label([0, 1], [inf, inf], 2.0) == "none"
 
 
 def test_traffic_estimate_without_file(tmp_path):
     bench = load_bench()
-    assert bench.traffic_estimate("c2", 10, 1.0, tmp_path / "absent.txt") == (None, None, None)
+    assert bench.traffic_estimate("c2", 10, 1.0, path=tmp_path / "absent.txt") == (None, None, None)
