@@ -302,12 +302,17 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
 
     resident = bfx.ResidentDeviceGraph.upload_once(wl.layout, device)
     ws = bfx.Workspace(resident)
-    layout_ids = {"flat": bfx.FRONTIER_FLAT, "groups": bfx.FRONTIER_GROUPS, "chunked": bfx.FRONTIER_CHUNKED}
+    layout_ids = {"flat": bfx.FRONTIER_FLAT, "groups": bfx.FRONTIER_GROUPS, "chunked": bfx.FRONTIER_CHUNKED,
+                  "tiled": bfx.FRONTIER_TILED}
     ws.set_frontier_layout(layout_ids[args.frontier])
     ws.set_register_budget(args.regs)
     eff_regs = args.regs or (80 if args.frontier == "chunked" else 64)
     if args.frontier != "chunked" and eff_regs == 80:
         eff_regs = 64
+    if args.frontier == "tiled":
+        eff_regs = 128  # the tiled kernel's own bound: two 256-thread blocks per SM
+        if args.stage_min is not None:
+            ws.set_tile_stage_min(args.stage_min)
     ws.set_flat_items(args.items)
     ws.set_relax_atomic(args.amin)
     ws.set_flat_order(args.edge_major)
@@ -531,7 +536,7 @@ def main():
     ap.add_argument("--impl", default="bfx", choices=["bfx", "reference"])
     ap.add_argument("--engine", default="auto", choices=["auto", "frontier", "jacobi", "dense"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5", "c3small"])
-    ap.add_argument("--frontier", default="chunked", choices=["groups", "flat", "chunked"],
+    ap.add_argument("--frontier", default="chunked", choices=["groups", "flat", "chunked", "tiled"],
                     help="frontier-push work layout (sub-warp groups or flat work list)")
     ap.add_argument("--regs", type=int, default=0, choices=[0, 40, 64, 80],
                     help="register budget of the persistent kernel (0: 80 for the chunked layout, else 64)")
@@ -547,6 +552,8 @@ def main():
                     help="with --engine frontier: near/far threshold step in mean edge weights (0 = plain frontier)")
     ap.add_argument("--tune-policy", action="store_true",
                     help="choose the planner policy by timing each candidate's plan (bfx_autotune_policy)")
+    ap.add_argument("--stage-min", type=int, default=None,
+                    help="tiled layout: lane-edge work from which a tile visit stages its labels")
     ap.add_argument("--shard", action="store_true",
                     help="multi-GPU: split one query set's batches over the ranks (strong scaling)")
     ap.add_argument("--no-c3", action="store_true", help="skip the c3 object of the default c2 run")

@@ -34,7 +34,7 @@ P = C.POINTER
 ENGINE_JACOBI_PULL, ENGINE_DENSE_CHAOTIC_PUSH, ENGINE_FRONTIER_PUSH = 0, 1, 2
 ENGINE_AUTO = 0xFFFFFFFF
 CONTROL_PERSISTENT, CONTROL_CHUNKED, CONTROL_PER_ROUND = 0, 1, 2
-FRONTIER_GROUPS, FRONTIER_FLAT, FRONTIER_CHUNKED = 0, 1, 2
+FRONTIER_GROUPS, FRONTIER_FLAT, FRONTIER_CHUNKED, FRONTIER_TILED = 0, 1, 2, 3
 STOP_NONE, STOP_CONVERGED, STOP_MAXIMUM_ROUNDS, STOP_QUEUE_OVERFLOW, STOP_INVALID, STOP_FAILURE = range(6)
 INF_BITS = 0x7F800000
 NO_EDGE = 0xFFFFFFFF
@@ -602,8 +602,13 @@ class Workspace:
         _check(load().bfx_set_flat_items(self._h, u32(items)))
 
     def set_frontier_layout(self, layout: int):
-        """FRONTIER_GROUPS (sub-warp groups per entry) or FRONTIER_FLAT (flat work list)."""
+        """FRONTIER_GROUPS (sub-warp groups per entry), FRONTIER_FLAT (flat work list),
+        FRONTIER_CHUNKED (32-vertex chunks) or FRONTIER_TILED (tile visits in shared memory)."""
         _check(load().bfx_set_frontier_layout(self._h, u32(layout)))
+
+    def set_tile_stage_min(self, lane_edges: int):
+        """Tiled layout: visits with less lane-edge work relax in global memory (no staging)."""
+        _check(load().bfx_set_tile_stage_min(self._h, u32(lane_edges)))
 
     def set_batch_engines(self, engines: Sequence[int]):
         arr = (u32 * len(engines))(*engines)
@@ -723,7 +728,8 @@ class Workspace:
         w = [int(x) for x in out]
         return {"push": dict(zip(self.WORK_KEYS[:7], w[:7])), "rounds": w[7],
                 "jacobi": {"items": w[8], "records": w[9], "relaxations": w[10], "changes": w[11]},
-                "split": {"entries": w[12], "lanes": w[13]}}
+                "split": {"entries": w[12], "lanes": w[13]},
+                "tiled": {"local_relaxations": w[14], "staged_visits": w[15]}}
 
     def run_query(self, sources, targets, selected_tiles, options: GpuRunOptions) -> DeviceRunStatus:
         s = np.ascontiguousarray(np.unique(np.asarray(sources, np.uint32)))

@@ -155,8 +155,8 @@ __global__ void init_kernel(LaunchParams p) {
     B.mask[1][cv] = 0u;
     B.fmask[cv] = 0u;
     B.fbound[cv] = 0xFFFFFFFFu;
-    if (p.flat == 2u) {
-      if ((cv & 1023u) == 0u) {  // chunk bitmap words, one per 1,024 vertices
+    if (p.flat >= 2u) {
+      if ((cv & 1023u) == 0u) {  // chunk bitmap words, one per 1,024 vertices (enough for any shift >= 5)
         B.cmask[0][cv >> 10] = 0u;
         B.cmask[1][cv >> 10] = 0u;
       }
@@ -202,6 +202,7 @@ __global__ void init_kernel(LaunchParams p) {
     p.run->stop = 0u;
     p.run->abort = 0u;
     for (int i = 0; i < 16; ++i) p.run->work[i] = 0u;
+    for (int i = 0; i < 3; ++i) p.run->items[i] = 0u;
   }
 }
 
@@ -226,11 +227,11 @@ __global__ void seed_kernel(LaunchParams p, const u32* src_base) {
     B.dist[0][(static_cast<u64>(cv) << B.shift) + lane] = dev::kSourceWord;
     const u32 eng = engine_of(p, b);
     if (eng == BFX_ENGINE_JACOBI_PULL) B.dist[1][(static_cast<u64>(cv) << B.shift) + lane] = dev::kSourceWord;
-    if (eng == BFX_ENGINE_FRONTIER_PUSH && p.flat == 2u) {
-      // chunked frontier: pending lane, then the chunk's bit; the thread that
-      // sets the bit queues the chunk
+    if (eng == BFX_ENGINE_FRONTIER_PUSH && p.flat >= 2u) {
+      // chunked / tiled frontier: pending lane, then the claim unit's bit;
+      // the thread that sets the bit queues the unit
       atomicOr(&B.mask[0][cv], 1u << lane);
-      const u32 chunk = cv >> 5;
+      const u32 chunk = cv >> p.cshift;
       const u32 bit = 1u << (chunk & 31u);
       if ((atomicOr(&B.cmask[0][chunk >> 5], bit) & bit) == 0u) {
         const u32 slot = atomicAdd(&p.ctl[b].count[0], 1u);
@@ -375,14 +376,26 @@ __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
     if (engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH) {
       const DCtl& C = p.ctl[b];
       const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
+      if (p.flat == 3u) {  // tiled: block items (one claim unit, or 32 far entries per warp of the block)
+        if (n != 0u) return chunk_items(n, B.U, p.cshift);
+        const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
+        const u32 per = 32u * (blockDim.x >> 5);
+        return (f + per - 1u) / per;
+      }
       if (n != 0u) {  // warp items: one chunk (chunked), flat_entries_per_item(n) entries (flat), 4 or 1 entries
-        if (p.flat == 2u) return chunk_items(n, B.U);
+        if (p.flat == 2u) return chunk_items(n, B.U, 5u);
         return p.flat ? (n + flat_entries_per_item(n) - 1u) / flat_entries_per_item(n) : (B.W <= 8u ? (n + 3u) >> 2 : n);
       }
       const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
       return (f + 31u) >> 5;  // split round: 32 far entries per warp item
     }
-    return batch_exec(p, b, ridx) != 0u ? (((B.U << B.shift) + 31u) >> 5) : 0u;
+    if (batch_exec(p, b, ridx) == 0u) return 0u;
+    const u32 warp_items = ((B.U << B.shift) + 31u) >> 5;
+    if (p.flat == 3u) {  // tiled: each warp of a block item takes one warp item
+      const u32 nw = blockDim.x >> 5;
+      return (warp_items + nw - 1u) / nw;
+    }
+    return warp_items;
   });
   return prefix[p.nb];
 }
@@ -454,7 +467,7 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
       if (n != 0u) {
         if (kChunked) {
           u32 chunk = kNoChunk;  // sparse round: the item's queue word names the chunk
-          if (chunk_dense(n, V.U)) {
+          if (chunk_dense(n, V.U, 5u)) {
             // dense round: the item is chunk slot `item`; clear bit, no work
             // (every lane reads the same word, so the skip is warp-uniform)
             const u32 word = dev::ld_cg(V.cmask_r + (item >> 5));
@@ -514,6 +527,7 @@ __device__ void round_bookkeeping(const LaunchParams& p, u32 r) {
     C.count[zidx] = 0u;
     C.changed[zidx] = 0u;
   }
+  if (threadIdx.x == 0u) p.run->items[zidx] = 0u;  // tiled layout: the block-item counter of round r + 2
 }
 
 // Frontier batches whose round r is a near/far split round (round trace
@@ -644,6 +658,9 @@ __global__ void start_kernel(LaunchParams p) {
     p.run->done = (total == 0u || p.max_rounds == 0u) ? 1u : 0u;
   }
 }
+
+// Tiled frontier layout (see tiled.cuh).
+#include "tiled.cuh"
 
 // ---------------------------------------------------------------------------
 // Finalize: one block per batch.  Reached / miss lanes from target
@@ -960,6 +977,20 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
     G->g.csc = reinterpret_cast<const uint4*>(base + o_csc);
     G->g.eid_src = reinterpret_cast<const std::uint32_t*>(base + o_eid_src);
     G->bytes = total;
+    {
+      const std::uint32_t size0 = G->tile_vertex_offsets[1] - G->tile_vertex_offsets[0];
+      bool uniform = true;
+      for (std::uint32_t t = 0; t < T && uniform; ++t) {
+        uniform = G->tile_vertex_offsets[t + 1] - G->tile_vertex_offsets[t] == size0;
+      }
+      std::uint32_t shift = 8;
+      if (uniform && size0 >= 32u && size0 <= 256u && (size0 & (size0 - 1u)) == 0u) {
+        shift = static_cast<std::uint32_t>(__builtin_ctz(size0));
+      } else if (uniform && size0 < 32u) {
+        shift = 5;
+      }
+      G->tile_shift = shift;
+    }
     *out = G.release();
   });
 }
@@ -1334,6 +1365,18 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   p.engines = nullptr;
   p.deltas = nullptr;
   p.flat = ws->frontier_layout == BFX_FRONTIER_FLAT ? 1u : (ws->frontier_layout == BFX_FRONTIER_CHUNKED ? 2u : 0u);
+  p.cshift = 5u;
+  p.tile_stage_min = ws->tile_stage_min;
+  p.tile_wmax = 1u;
+  if (ws->frontier_layout == BFX_FRONTIER_TILED) {
+    // the tiled layout runs in persistent mode; host-poll modes use the
+    // chunked layout's round kernels
+    p.flat = o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE ? 3u : 2u;
+    if (p.flat == 3u) {
+      p.cshift = ws->graph->tile_shift;
+      for (const DBatch& b : ws->batches) p.tile_wmax = std::max(p.tile_wmax, b.W);
+    }
+  }
   p.round_trace = nullptr;
   p.trace_cap = 0u;
   p.amin = ws->relax_atomic;
@@ -1382,7 +1425,17 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   ++launches;
   BFX_CUDA(cudaGetLastError());
   BFX_CUDA(cudaEventRecord(ws->ev[1], ws->stream));
-  if (o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
+  if (o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE && p.flat == 3u) {
+    require(block == 256, "the tiled frontier layout runs blocks of 256 threads");
+    const void* kfn = o.instrumentation != 0u ? reinterpret_cast<const void*>(persistent_tiled_kernel<true>)
+                                              : reinterpret_cast<const void*>(persistent_tiled_kernel<false>);
+    const size_t tsmem = tile_smem_bytes(ws->nb, p.cshift, p.tile_wmax);
+    BFX_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(tsmem)));
+    const int grid = grid_blocks(ws, kfn, block, tsmem, o);
+    void* args[] = {&p};
+    BFX_CUDA(cudaLaunchCooperativeKernel(kfn, grid, block, args, tsmem, ws->stream));
+    ++launches;
+  } else if (o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE) {
     // register budget 0 (default): 80 for the chunked layout with blocks of
     // at most 256 threads, 64 otherwise
     const std::uint32_t regs =
@@ -1525,9 +1578,17 @@ int bfx_set_flat_items(bfx_workspace* ws, uint32_t items) {
 int bfx_set_frontier_layout(bfx_workspace* ws, uint32_t layout) {
   return bfx::guarded([&] {
     bfx::require(ws != nullptr, "null argument");
-    bfx::require(layout == BFX_FRONTIER_GROUPS || layout == BFX_FRONTIER_FLAT || layout == BFX_FRONTIER_CHUNKED,
+    bfx::require(layout == BFX_FRONTIER_GROUPS || layout == BFX_FRONTIER_FLAT || layout == BFX_FRONTIER_CHUNKED ||
+                     layout == BFX_FRONTIER_TILED,
                  "invalid frontier layout");
     ws->frontier_layout = layout;
+  });
+}
+
+int bfx_set_tile_stage_min(bfx_workspace* ws, uint32_t lane_edges) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null argument");
+    ws->tile_stage_min = lane_edges;
   });
 }
 

@@ -100,7 +100,10 @@ struct DRun {
   u32 abort;       // device failure seen
   u64 max_rounds;
   u64 launches;
-  u64 work[16];    // launch-wide work counters: [0..6] push engines, [7] rounds, [8..11] Jacobi, [12..13] splits
+  u64 work[16];    // launch-wide work counters: [0..6] push engines, [7] rounds, [8..11] Jacobi, [12..13] splits,
+                   // [14..15] tiled visits (lane-edge relaxations inside shared memory, staged visits)
+  u32 items[3];    // tiled layout: block items drawn in round r from items[r % 3] (cleared two rounds ahead)
+  u32 reserved[5];
 };
 
 // Work counters of an instrumented run (instrumentation >= 1):
@@ -111,8 +114,10 @@ struct DRun {
 // dense push (entries / vertex items, edge records, source reads, lane-edge
 // relaxations, queue claims, decreases, min-reductions), c[7..10] Jacobi
 // pull (vertex-lane items, in-edge records, relaxations, changes), c[11..12]
-// near/far split rounds (far pile entries scanned, parked lanes re-read).
-constexpr int kWorkCounters = 13;
+// near/far split rounds (far pile entries scanned, parked lanes re-read),
+// c[13..14] tiled visits (lane-edge relaxations in shared memory, visits
+// that staged their labels).
+constexpr int kWorkCounters = 15;
 struct Work {
   u64 c[kWorkCounters];
   __device__ void zero() {
@@ -133,7 +138,8 @@ struct LaunchParams {
   u32 nb;
   u32 engine;            // engine of every batch when `engines` is null
   u32 per_lane;
-  u32 flat;              // frontier layout: 0 sub-warp groups, 1 flat work list, 2 chunked flat work list
+  u32 flat;              // frontier layout: 0 sub-warp groups, 1 flat work list, 2 chunked flat work list,
+                         // 3 tiled (a block visits 2^cshift compact vertices with their labels in shared memory)
   u64 max_rounds;
   u64 budget_ns;         // wall-clock budget of one relaxation launch; past it the launch stops (device_failure)
   const u32* engines;    // [nb] per-batch engine (autotuned launches) or null
@@ -143,7 +149,10 @@ struct LaunchParams {
   u32 trace_cap;         // rounds the trace holds
   u32 amin;              // flat frontier: 1 = returning min per relaxation, 0 = pre-read + min on success
   u32 edge_major;        // flat frontier work order: 1 = entry, edge, lane; 0 = entry, lane, edge
-  u32 reserved3;
+  u32 cshift;            // chunked / tiled layouts: a claim unit is 2^cshift consecutive compact vertices
+                         // (5 for the chunked layout; the tile size for the tiled one)
+  u32 tile_stage_min;    // tiled layout: lane-edge work below which a block visit relaxes in place (no staging)
+  u32 tile_wmax;         // tiled layout: widest batch of the launch (sizes the staged label rows)
 };
 
 constexpr u32 kRoundTraceCap = 65536;
@@ -214,6 +223,10 @@ struct bfx_resident_graph {
   std::vector<std::uint32_t> tile_vertex_offsets;  // host copy, [T+1]
   std::uint64_t bytes{0};
   double mean_weight{0.0};
+  // Tiled frontier claim unit: log2 of the tile size when every tile holds
+  // the same power-of-two count of vertices in [32, 256], else 8 (units then
+  // straddle tiles, which costs locality but not correctness); at least 5.
+  std::uint32_t tile_shift{8};
 };
 
 struct bfx_workspace {
@@ -266,6 +279,7 @@ struct bfx_workspace {
   std::uint32_t chunk_pairs = 0;             // chunked frontier pair mode (see bfx_set_chunk_pairs)
   std::uint32_t flat_items = 2;              // flat layout: work items per thread per iteration (2..4)
   std::uint32_t register_budget = 0;         // persistent kernel registers per thread: 0 automatic, 40, 64, 80
+  std::uint32_t tile_stage_min = 1024;       // tiled layout: lane-edge work from which a visit stages its labels
   bfx::DeviceBuffer deltas_dev;
   bfx::PinnedBuffer deltas_host;
   bfx::DeviceBuffer engines_dev;

@@ -361,7 +361,7 @@ __device__ __forceinline__ void split_group(const LaunchParams& p, const Frontie
   if (near != 0u) {
     if (kChunked) {
       dev::red_or(B.mask_w + cv, near);
-      const u32 chunk = cv >> 5;
+      const u32 chunk = cv >> p.cshift;
       const u32 bit = 1u << (chunk & 31u);
       claim = (atomicOr(B.cmask_w + (chunk >> 5), bit) & bit) == 0u;
       qword = chunk;
@@ -459,8 +459,13 @@ constexpr u32 kNoChunk = 0xFFFFFFFFu;
 // pending, the items are all chunk slots in index order and a warp skips the
 // slots whose bit is clear.  Concurrent warps then relax neighbouring
 // chunks, whose target labels (intra-tile edges) are shared in the L2.
-__device__ __forceinline__ bool chunk_dense(u32 n, u32 U) { return 2u * n >= ((U + 31u) >> 5); }
-__device__ __forceinline__ u32 chunk_items(u32 n, u32 U) { return chunk_dense(n, U) ? (U + 31u) >> 5 : n; }
+// cshift: the claim unit is 2^cshift compact vertices (5: the chunked layout's
+// 32-vertex chunks; the tile size in the tiled layout).
+__device__ __forceinline__ u32 chunk_count(u32 U, u32 cshift) { return (U + (1u << cshift) - 1u) >> cshift; }
+__device__ __forceinline__ bool chunk_dense(u32 n, u32 U, u32 cshift) { return 2u * n >= chunk_count(U, cshift); }
+__device__ __forceinline__ u32 chunk_items(u32 n, u32 U, u32 cshift) {
+  return chunk_dense(n, U, cshift) ? chunk_count(U, cshift) : n;
+}
 
 template <bool kCount, u32 kItems, bool kChunked, bool kPairs = false>
 __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,

@@ -314,9 +314,19 @@ int bfx_set_batch_deltas(bfx_workspace *ws, uint32_t count, const float *deltas)
  * threads (batches of <= 8 lanes) or a whole warp; BFX_FRONTIER_CHUNKED
  * (default) queues 32-vertex chunks instead of vertices (a chunk bitmap per round
  * slot, pending lanes set with non-returning ORs) and runs the flat work list
- * over each chunk's vertices in index (spatial) order. */
-enum { BFX_FRONTIER_GROUPS = 0, BFX_FRONTIER_FLAT = 1, BFX_FRONTIER_CHUNKED = 2 };
+ * over each chunk's vertices in index (spatial) order; BFX_FRONTIER_TILED
+ * queues whole tiles (blocks of the graph's tile size, 32..256 vertices) and
+ * lets a thread block visit one at a time: it stages the tile's label rows in
+ * shared memory, relaxes intra-tile edges there until no lane of the tile is
+ * pending, pushes inter-tile edges through global memory and writes the
+ * changed labels back (persistent control mode, blocks of 256 threads; the
+ * host-poll modes run the chunked layout instead). */
+enum { BFX_FRONTIER_GROUPS = 0, BFX_FRONTIER_FLAT = 1, BFX_FRONTIER_CHUNKED = 2, BFX_FRONTIER_TILED = 3 };
 int bfx_set_frontier_layout(bfx_workspace *ws, uint32_t layout);
+/* Tiled layout: a tile visit whose pending lane-edge work is below
+ * `lane_edges` relaxes in global memory without staging its labels (bfx
+ * extension; results unchanged; default 1024). */
+int bfx_set_tile_stage_min(bfx_workspace *ws, uint32_t lane_edges);
 /* Register budget of the persistent relaxation kernel (a bfx tuning option,
  * results unchanged): 40 registers per thread (three 512-thread blocks per
  * SM), 64 (two 512-thread blocks per SM: no spills in the group layout, few

@@ -13,9 +13,9 @@ min-eid tight predecessors, bit for bit:
   c5  64 seeded regional lanes and two full-graph lanes of the 4,096 + 16
       query set in one launch.
 
-The integer-cost configurations (c3, c5) also assert that every finite
-distance is below 2^24, the range in which float sums of integer costs are
-exact.
+Each runs with the chunked and the tiled frontier layouts.  The
+integer-cost configurations (c3, c5) also assert that every finite distance
+is below 2^24, the range in which float sums of integer costs are exact.
 """
 from __future__ import annotations
 
@@ -34,12 +34,16 @@ TWO_POW_24_BITS = 0x4B800000  # float bits of 2^24
 THREADS = max(1, min(32, os.cpu_count() or 1))
 
 
-def tuned_launch(resident, wl):
+LAYOUTS = {"chunked": bfx.FRONTIER_CHUNKED, "tiled": bfx.FRONTIER_TILED}
+
+
+def tuned_launch(resident, wl, layout="chunked"):
     """Plan, autotune (engines and near/far steps per batch) and run the set
     in one launch, as the benchmark does."""
     plan = bfx.make_overlapping_batch_plan(wl.layout, wl.queries, wl.policy)
     descs = plan.descriptions()
     ws = bfx.Workspace(resident)
+    ws.set_frontier_layout(LAYOUTS[layout])
     engines, _ = ws.autotune(descs)
     ws.execute(bfx.GpuRunOptions(engine=bfx.ENGINE_AUTO))
     statuses = ws.fetch_statuses()
@@ -83,24 +87,32 @@ def c3_graph(gpu):
     resident.close()
 
 
-def test_c2_every_lane_bit_exact(gpu):
+@pytest.fixture(scope="module")
+def c2_graph(gpu):
     wl = workloads.bench_workload("c2")
     resident = bfx.ResidentDeviceGraph.upload_once(wl.layout)
-    ws, descs, engines, statuses = tuned_launch(resident, wl)
+    yield wl, resident, Oracle.from_layout(wl.layout)
+    resident.close()
+
+
+@pytest.mark.parametrize("layout", ["chunked", "tiled"])
+def test_c2_every_lane_bit_exact(c2_graph, layout):
+    wl, resident, orc = c2_graph
+    ws, descs, engines, statuses = tuned_launch(resident, wl, layout)
     assert_statuses(statuses)
     picks = [(b, l) for b, d in enumerate(descs) for l in valid_lanes(d)]
     assert len(picks) == len(wl.queries) == 256
-    checked, dist_bad, pred_bad, reached = compare_lanes(ws, Oracle.from_layout(wl.layout), wl, descs, picks)
+    checked, dist_bad, pred_bad, reached = compare_lanes(ws, orc, wl, descs, picks)
     assert (checked, dist_bad, pred_bad) == (256, 0, 0)
     # every query's target is inside its own box, so every lane reaches it
     assert sum(bin(s.reached_target_mask).count("1") for s in statuses) == reached
     ws.close()
-    resident.close()
 
 
-def test_c3_sampled_full_graph_lanes_bit_exact(c3_graph):
+@pytest.mark.parametrize("layout", ["chunked", "tiled"])
+def test_c3_sampled_full_graph_lanes_bit_exact(c3_graph, layout):
     wl, resident, orc = c3_graph
-    ws, descs, engines, statuses = tuned_launch(resident, wl)
+    ws, descs, engines, statuses = tuned_launch(resident, wl, layout)
     assert_statuses(statuses)
     assert len(descs) == 2 and all(d.lane_width == 32 for d in descs)
     rng = np.random.default_rng(3030)
@@ -112,12 +124,13 @@ def test_c3_sampled_full_graph_lanes_bit_exact(c3_graph):
     ws.close()
 
 
-def test_c5_sampled_regional_and_full_lanes_bit_exact(c3_graph):
+@pytest.mark.parametrize("layout", ["chunked", "tiled"])
+def test_c5_sampled_regional_and_full_lanes_bit_exact(c3_graph, layout):
     wl3, resident, orc = c3_graph
     queries, _ = workloads.bench_queries("c5", wl3.layout, wl3.grid)
     wl = workloads.BenchWorkload("c5", None, None, wl3.layout, wl3.grid, queries, [],
                                  bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True), "", True)
-    ws, descs, engines, statuses = tuned_launch(resident, wl)
+    ws, descs, engines, statuses = tuned_launch(resident, wl, layout)
     assert_statuses(statuses)
     n_regional = 4096
     lanes = [(b, l) for b, d in enumerate(descs) for l in valid_lanes(d)]
