@@ -606,6 +606,10 @@ class Workspace:
         FRONTIER_CHUNKED (32-vertex chunks) or FRONTIER_TILED (tile visits in shared memory)."""
         _check(load().bfx_set_frontier_layout(self._h, u32(layout)))
 
+    def set_tile_passes(self, passes: int):
+        """Tiled layout: local relaxation passes per staged visit."""
+        _check(load().bfx_set_tile_passes(self._h, u32(passes)))
+
     def set_tile_stage_min(self, lane_edges: int):
         """Tiled layout: visits with less lane-edge work relax in global memory (no staging)."""
         _check(load().bfx_set_tile_stage_min(self._h, u32(lane_edges)))

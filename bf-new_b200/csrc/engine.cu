@@ -163,6 +163,7 @@ __global__ void init_kernel(LaunchParams p) {
       const u32 v = r.y + (cv - B.range_off[lo]);
       const u32 rb = p.g.csr_off[v];
       B.crow[cv] = make_uint2(rb, p.g.csr_off[v + 1u] - rb);
+      if (p.flat == 3u) B.clrun[cv] = p.g.lrun[v];
     }
     for (u32 l = 0; l < B.W; ++l) {
       B.dist[0][(static_cast<u64>(cv) << B.shift) + l] = dev::kUnreached;
@@ -376,26 +377,14 @@ __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
     if (engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH) {
       const DCtl& C = p.ctl[b];
       const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
-      if (p.flat == 3u) {  // tiled: block items (one claim unit, or 32 far entries per warp of the block)
-        if (n != 0u) return chunk_items(n, B.U, p.cshift);
-        const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
-        const u32 per = 32u * (blockDim.x >> 5);
-        return (f + per - 1u) / per;
-      }
       if (n != 0u) {  // warp items: one chunk (chunked), flat_entries_per_item(n) entries (flat), 4 or 1 entries
-        if (p.flat == 2u) return chunk_items(n, B.U, 5u);
+        if (p.flat >= 2u) return chunk_items(n, B.U, 5u);
         return p.flat ? (n + flat_entries_per_item(n) - 1u) / flat_entries_per_item(n) : (B.W <= 8u ? (n + 3u) >> 2 : n);
       }
       const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
       return (f + 31u) >> 5;  // split round: 32 far entries per warp item
     }
-    if (batch_exec(p, b, ridx) == 0u) return 0u;
-    const u32 warp_items = ((B.U << B.shift) + 31u) >> 5;
-    if (p.flat == 3u) {  // tiled: each warp of a block item takes one warp item
-      const u32 nw = blockDim.x >> 5;
-      return (warp_items + nw - 1u) / nw;
-    }
-    return warp_items;
+    return batch_exec(p, b, ridx) != 0u ? (((B.U << B.shift) + 31u) >> 5) : 0u;
   });
   return prefix[p.nb];
 }
@@ -931,8 +920,19 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
 
     std::vector<uint4> csr(E), csc(E);
     std::vector<std::uint32_t> eid_src(E, 0U);
+    std::vector<uint2> lrun(V);
     bfx::parallel_for(V, 0, [&](std::uint64_t b, std::uint64_t e) {
       for (std::uint64_t v = b; v < e; ++v) {
+        // own-tile run: rows are ordered by destination tile, so the edges
+        // into v's own tile are contiguous
+        std::uint32_t lb = L.csr_row_offsets[v], lc = 0;
+        for (std::uint32_t p = L.csr_row_offsets[v]; p < L.csr_row_offsets[v + 1]; ++p) {
+          if (L.owner_tiles[L.csr_destinations[p]] == L.owner_tiles[v]) {
+            if (lc == 0) lb = p;
+            ++lc;
+          }
+        }
+        lrun[v] = make_uint2(lb, lc);
         for (std::uint32_t p = L.csr_row_offsets[v]; p < L.csr_row_offsets[v + 1]; ++p) {
           const std::uint32_t d = L.csr_destinations[p];
           std::uint32_t wb;
@@ -955,7 +955,8 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
     const size_t o_csr = bfx::align256(o_csc_off + (size_t{V} + 1) * 4);
     const size_t o_csc = bfx::align256(o_csr + size_t{E} * 16);
     const size_t o_eid_src = bfx::align256(o_csc + size_t{E} * 16);
-    const size_t total = bfx::align256(o_eid_src + size_t{E} * 4);
+    const size_t o_lrun = bfx::align256(o_eid_src + size_t{E} * 4);
+    const size_t total = bfx::align256(o_lrun + size_t{V} * 8);
     G->mem.reserve(total, device);
     char* base = static_cast<char*>(G->mem.ptr);
     BFX_CUDA(cudaMemcpy(base + o_owner, L.owner_tiles, size_t{V} * 4, cudaMemcpyHostToDevice));
@@ -964,6 +965,7 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
     BFX_CUDA(cudaMemcpy(base + o_csr, csr.data(), size_t{E} * 16, cudaMemcpyHostToDevice));
     BFX_CUDA(cudaMemcpy(base + o_csc, csc.data(), size_t{E} * 16, cudaMemcpyHostToDevice));
     BFX_CUDA(cudaMemcpy(base + o_eid_src, eid_src.data(), size_t{E} * 4, cudaMemcpyHostToDevice));
+    BFX_CUDA(cudaMemcpy(base + o_lrun, lrun.data(), size_t{V} * 8, cudaMemcpyHostToDevice));
     double wsum = 0.0;
     for (std::uint32_t e = 0; e < E; ++e) wsum += L.csr_weights[e];
     G->mean_weight = E ? wsum / E : 0.0;
@@ -976,6 +978,7 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
     G->g.csr = reinterpret_cast<const uint4*>(base + o_csr);
     G->g.csc = reinterpret_cast<const uint4*>(base + o_csc);
     G->g.eid_src = reinterpret_cast<const std::uint32_t*>(base + o_eid_src);
+    G->g.lrun = reinterpret_cast<const uint2*>(base + o_lrun);
     G->bytes = total;
     {
       const std::uint32_t size0 = G->tile_vertex_offsets[1] - G->tile_vertex_offsets[0];
@@ -1160,7 +1163,7 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
     for (std::uint32_t b = 0; b < count; ++b) {
       arena_off[b] = arena_total;
       const size_t U = sz[b].U;
-      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 5 + bfx::align256(U * 8) * 6 +
+      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 5 + bfx::align256(U * 8) * 7 +
                      bfx::align256((U + 1023) / 1024 * 4) * 2;
     }
     const size_t tiles_off = arena_total;
@@ -1246,6 +1249,8 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
         a += bfx::align256((U + 1023) / 1024 * 4);
       }
       B.crow = reinterpret_cast<uint2*>(a);
+      a += bfx::align256(U * 8);
+      B.clrun = reinterpret_cast<uint2*>(a);
       a += bfx::align256(U * 8);
       B.tiles = reinterpret_cast<uint2*>(ab + tiles_off + tile_table_bytes * b);
       ubase[b] = static_cast<std::uint32_t>(usum);
@@ -1367,13 +1372,14 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   p.flat = ws->frontier_layout == BFX_FRONTIER_FLAT ? 1u : (ws->frontier_layout == BFX_FRONTIER_CHUNKED ? 2u : 0u);
   p.cshift = 5u;
   p.tile_stage_min = ws->tile_stage_min;
+  p.tile_iters = ws->tile_iters;
   p.tile_wmax = 1u;
   if (ws->frontier_layout == BFX_FRONTIER_TILED) {
     // the tiled layout runs in persistent mode; host-poll modes use the
     // chunked layout's round kernels
     p.flat = o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE ? 3u : 2u;
     if (p.flat == 3u) {
-      p.cshift = ws->graph->tile_shift;
+      p.tshift = ws->graph->tile_shift;
       for (const DBatch& b : ws->batches) p.tile_wmax = std::max(p.tile_wmax, b.W);
     }
   }
@@ -1426,10 +1432,13 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   BFX_CUDA(cudaGetLastError());
   BFX_CUDA(cudaEventRecord(ws->ev[1], ws->stream));
   if (o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE && p.flat == 3u) {
-    require(block == 256, "the tiled frontier layout runs blocks of 256 threads");
-    const void* kfn = o.instrumentation != 0u ? reinterpret_cast<const void*>(persistent_tiled_kernel<true>)
-                                              : reinterpret_cast<const void*>(persistent_tiled_kernel<false>);
-    const size_t tsmem = tile_smem_bytes(ws->nb, p.cshift, p.tile_wmax);
+    require(block == 256 || block == 384, "the tiled frontier layout runs blocks of 256 or 384 threads");
+    const void* kfn =
+        block == 256 ? (o.instrumentation != 0u ? reinterpret_cast<const void*>(persistent_tiled_kernel<true, 256>)
+                                                : reinterpret_cast<const void*>(persistent_tiled_kernel<false, 256>))
+                     : (o.instrumentation != 0u ? reinterpret_cast<const void*>(persistent_tiled_kernel<true, 384>)
+                                                : reinterpret_cast<const void*>(persistent_tiled_kernel<false, 384>));
+    const size_t tsmem = tile_smem_bytes(ws->nb, p.tshift, p.tile_wmax);
     BFX_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(tsmem)));
     const int grid = grid_blocks(ws, kfn, block, tsmem, o);
     void* args[] = {&p};
@@ -1589,6 +1598,14 @@ int bfx_set_tile_stage_min(bfx_workspace* ws, uint32_t lane_edges) {
   return bfx::guarded([&] {
     bfx::require(ws != nullptr, "null argument");
     ws->tile_stage_min = lane_edges;
+  });
+}
+
+int bfx_set_tile_passes(bfx_workspace* ws, uint32_t passes) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null argument");
+    bfx::require(passes >= 1u && passes <= 1024u, "tile passes must be 1..1024");
+    ws->tile_iters = passes;
   });
 }
 

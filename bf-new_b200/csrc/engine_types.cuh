@@ -40,6 +40,8 @@ struct DGraph {
   const u32* csc_off;  // [V+1]
   const uint4* csc;    // [E] {src, weight bits, eid+1, src tile}
   const u32* eid_src;  // [E] source vertex of each stable edge id
+  const uint2* lrun;   // [V] own-tile run of each CSR row {first CSR index, count} (rows are sorted by
+                       // destination tile, so a vertex's edges into its own tile are contiguous)
 };
 
 struct DBatch {
@@ -63,6 +65,7 @@ struct DBatch {
                           // (chunked layout: the vertex field holds the compact index)
   u32* cmask[2];          // [ceil(U/1024)] chunk bitmaps (chunked frontier): bit c = chunk c pending
   uint2* crow;            // [U] {CSR row begin, out-degree} per compact vertex (chunked frontier)
+  uint2* clrun;           // [U] own-tile run {first CSR index, count} per compact vertex (tiled frontier)
 };
 
 struct DCtl {
@@ -153,6 +156,8 @@ struct LaunchParams {
                          // (5 for the chunked layout; the tile size for the tiled one)
   u32 tile_stage_min;    // tiled layout: lane-edge work below which a block visit relaxes in place (no staging)
   u32 tile_wmax;         // tiled layout: widest batch of the launch (sizes the staged label rows)
+  u32 tile_iters;        // tiled layout: local relaxation passes per visit before the rest waits a round
+  u32 tshift;            // tiled layout: a dense round visits units of 2^tshift compact vertices (the tile size)
 };
 
 constexpr u32 kRoundTraceCap = 65536;
@@ -280,6 +285,7 @@ struct bfx_workspace {
   std::uint32_t flat_items = 2;              // flat layout: work items per thread per iteration (2..4)
   std::uint32_t register_budget = 0;         // persistent kernel registers per thread: 0 automatic, 40, 64, 80
   std::uint32_t tile_stage_min = 1024;       // tiled layout: lane-edge work from which a visit stages its labels
+  std::uint32_t tile_iters = 32;             // tiled layout: local passes per visit
   bfx::DeviceBuffer deltas_dev;
   bfx::PinnedBuffer deltas_host;
   bfx::DeviceBuffer engines_dev;

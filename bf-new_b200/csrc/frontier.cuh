@@ -37,6 +37,7 @@ struct FrontierView {
   u64* pile;      // near round: far pile being filled; split round: pile read
   u64* pile_out;  // split round: pile written
   const uint2* crow;  // compact index -> {CSR row begin, out-degree} (chunked layout)
+  const uint2* clrun; // compact index -> own-tile run {first CSR index, count} (tiled layout)
   u32* cmask_r;       // chunk bitmaps (chunked layout): read and write slots
   u32* cmask_w;
   u32 shift, valid, U, full;
@@ -55,6 +56,7 @@ __device__ __forceinline__ FrontierView frontier_view(const DBatch& b, u32 rd, u
   v.pile = b.fpile[pile];
   v.pile_out = b.fpile[pile_out];
   v.crow = b.crow;
+  v.clrun = b.clrun;
   v.cmask_r = b.cmask[rd];
   v.cmask_w = b.cmask[rd ^ 1u];
   v.shift = b.shift;

@@ -1,29 +1,36 @@
 // Tiled frontier push (BFX_FRONTIER_TILED; included by engine.cu after the
 // Jacobi and dense items).
 //
-// The claim unit is a block of 2^cshift consecutive compact vertices -- one
-// spatial tile when every tile holds 2^cshift vertices, as vertices are
-// ordered by tile and a batch's union tiles are concatenated in compact
-// order.  A block item of the persistent grid is one such unit of one
-// batch ("visit"):
-//   1. the block reads the unit's pending lanes (and clears them) and its
-//      compact row table, and sums the lane-edge work;
-//   2. with enough work it stages the unit's label rows (2^cshift x W packed
+// Claims and queues are the chunked layout's (32-vertex chunks, chunk
+// bitmaps, staged appends).  Sparse rounds run exactly as there, as warp
+// items each warp draws on its own (the chunked round body).  Dense rounds --
+// at least half of a batch's chunk slots pending -- visit whole tiles
+// instead: a block item is one unit of 2^tshift consecutive compact vertices,
+// which is one spatial tile when every tile holds 2^tshift vertices
+// (vertices are ordered by tile, and a batch's union tiles are concatenated
+// in compact order).  A visit:
+//   1. reads and clears the unit's chunk bits and its vertices' pending
+//      lanes, and their row tables: CSR row, and the own-tile run (a row is
+//      sorted by destination tile, so the edges into the vertex's own tile
+//      are contiguous; the resident graph keeps them per vertex);
+//   2. with enough work, stages the unit's label rows (2^tshift x W packed
 //      words, contiguous in the vertex-major layout) in shared memory and
-//      relaxes in local iterations: every pending (vertex, lane) pushes all
-//      its admitted out-edges; a target inside the unit is relaxed with a
-//      64-bit atomicMin in shared memory and, on a decrease below the
-//      threshold, marked pending for the next local iteration; a target
-//      outside goes through the global path (pre-read, red.min, pending
-//      lane OR, unit claim through the chunk bitmap, staged queue append).
-//      Iterations repeat until no local lane is pending (or a cap, whose
-//      leftovers are handed to the next round);
-//   3. changed labels are written back with red.min -- another block may
-//      have lowered the same word meanwhile through an inter-tile edge, and
-//      that improvement is also queued for the next round, so the min keeps
-//      both;
-//   4. a unit with little work skips the staging and relaxes every target in
-//      global memory, like the chunked layout.
+//      runs local passes: every pending (vertex, lane) relaxes its own-tile
+//      run against the staged labels with a 64-bit atomicMin in shared
+//      memory; a decrease below the threshold makes the target pending for
+//      the next pass and marks it for the global push.  Passes repeat until
+//      no lane of the unit is pending (or a cap; the rest is handed to the
+//      next round);
+//   3. pushes the other edges of every marked (vertex, lane) once, with its
+//      final label, through the global path (pre-read, red.min, pending lane
+//      OR, chunk claim, staged append) -- a loop in which every item is a
+//      global relaxation, so no warp waits on one slow item among fast ones;
+//   4. writes the changed labels back with red.min (another block may have
+//      lowered the same word through an inter-tile edge meanwhile; that
+//      improvement is queued for the next round as well, and the min keeps
+//      both);
+//   5. a unit with little pending work skips the staging and relaxes all its
+//      edges in global memory in one pass.
 // Near/far thresholds apply unchanged: a decrease at or above tau parks the
 // lane on the far pile (global far mask, bound and pile), local or not.
 // Within a pass the work list is flat over the block: (vertex, lane, edge)
@@ -32,40 +39,48 @@
 #pragma once
 
 // Shared-memory layout of a tiled visit, after the round prefix:
-// labels S[n][W] then six u32 arrays of n = 2^cshift entries.
+// labels S[n][W] then nine u32 arrays of n = 2^tshift entries.
 struct TileSmem {
   u64* S;
-  u32* P;    // pending lanes for the next local iteration
-  u32* M;    // lanes processed in this pass
+  u32* P;    // lanes pending for the next local pass
+  u32* G;    // lanes whose other edges are pushed by the global pass
+  u32* M;    // lanes of the current pass
   u32* CH;   // lanes whose staged label changed (written back)
-  u32* WI;   // inclusive lane-edge work scan
+  u32* WI;   // inclusive lane-edge work scan of the current pass
   u32* RB;   // CSR row begin
   u32* DG;   // out-degree
+  u32* LB;   // own-tile run: first CSR index
+  u32* LC;   // own-tile run: edge count
 };
 
-constexpr u32 kTileLocalIterations = 32;
+constexpr u32 kTileArrays = 9;
 
-__device__ __forceinline__ TileSmem tile_smem(u32* prefix, u32 nb, u32 cshift, u32 wmax) {
-  const size_t off = ((static_cast<size_t>(nb) + 1u) * 4u + 15u) & ~static_cast<size_t>(15);
+// Dynamic shared memory: the round's two prefixes (block items, warp items;
+// nb + 1 words each), then the visit arrays.
+__device__ __forceinline__ TileSmem tile_smem(u32* prefix, u32 nb, u32 tshift, u32 wmax) {
+  const size_t off = ((static_cast<size_t>(nb) + 1u) * 8u + 15u) & ~static_cast<size_t>(15);
   char* base = reinterpret_cast<char*>(prefix) + off;
-  const u32 n = 1u << cshift;
+  const u32 n = 1u << tshift;
   TileSmem t;
   t.S = reinterpret_cast<u64*>(base);
   u32* a = reinterpret_cast<u32*>(base + static_cast<size_t>(n) * wmax * 8u);
   t.P = a;
-  t.M = a + n;
-  t.CH = a + 2u * n;
-  t.WI = a + 3u * n;
-  t.RB = a + 4u * n;
-  t.DG = a + 5u * n;
+  t.G = a + n;
+  t.M = a + 2u * n;
+  t.CH = a + 3u * n;
+  t.WI = a + 4u * n;
+  t.RB = a + 5u * n;
+  t.DG = a + 6u * n;
+  t.LB = a + 7u * n;
+  t.LC = a + 8u * n;
   return t;
 }
 
 // Dynamic shared memory of the tiled kernel (host and device agree).
-__host__ __device__ inline size_t tile_smem_bytes(u32 nb, u32 cshift, u32 wmax) {
-  const size_t off = ((static_cast<size_t>(nb) + 1u) * 4u + 15u) & ~static_cast<size_t>(15);
-  const size_t n = size_t{1} << cshift;
-  return off + n * wmax * 8u + 6u * n * 4u;
+__host__ __device__ inline size_t tile_smem_bytes(u32 nb, u32 tshift, u32 wmax) {
+  const size_t off = ((static_cast<size_t>(nb) + 1u) * 8u + 15u) & ~static_cast<size_t>(15);
+  const size_t n = size_t{1} << tshift;
+  return off + n * wmax * 8u + kTileArrays * n * 4u;
 }
 
 // Block-wide inclusive scan of one value per thread (blockDim.x <= 1024).
@@ -92,26 +107,39 @@ __device__ __forceinline__ u32 block_inclusive_scan(u32 x, u32* warp_sums, u32& 
   return x + before;
 }
 
-// A decrease at or above the threshold: the lane is parked (far mask, bound,
-// pile).  Returns true when this OR parked the vertex on the pile.
-__device__ __forceinline__ bool tile_park(const FrontierView& B, Stages& st, u32 cdst, u32 bit, u32 dist_bits) {
-  st.fd = min(st.fd, dist_bits);
-  dev::red_min_u32(B.fbound + cdst, dist_bits);
-  return atomicOr(B.fmask + cdst, bit) == 0u;
+// Pass kinds: kLocal relaxes the own-tile runs against the staged labels;
+// kGlobal pushes the other edges of the marked lanes (sources staged);
+// kInPlace relaxes every edge in global memory (unstaged visit).
+enum TilePass : u32 { kLocal = 0, kGlobal = 1, kInPlace = 2 };
+
+// Snapshot for a pass: M = src (src cleared), per-vertex lane-edge work of
+// the pass kind, inclusive scan into WI.  Returns the block's work.
+template <u32 kKind>
+__device__ __forceinline__ u32 tile_snapshot(const TileSmem& sm, u32* src, u32 n, u32* warp_sums) {
+  u32 work = 0u;
+  const u32 i = threadIdx.x;
+  if (i < n) {
+    const u32 m = src[i];
+    sm.M[i] = m;
+    src[i] = 0u;
+    const u32 edges = kKind == kLocal ? sm.LC[i] : (kKind == kGlobal ? sm.DG[i] - sm.LC[i] : sm.DG[i]);
+    work = static_cast<u32>(__popc(m)) * edges;
+  }
+  u32 total = 0u;
+  const u32 incl = block_inclusive_scan(work, warp_sums, total);
+  if (i < n) sm.WI[i] = incl;
+  __syncthreads();
+  return total;
 }
 
-// One pass over the snapshot M[0..n) of a visit: every (vertex, lane) in M
-// pushes its admitted out-edges.  kStaged: source labels and in-unit
-// targets live in S (shared memory); otherwise everything is global.
-// Executed by the whole block; `total` is the block's lane-edge work.
-template <bool kCount, bool kStaged>
+// One pass over the snapshot M[0..n) (see TilePass).  Executed by the whole
+// block; `total` is the pass's lane-edge work.
+template <bool kCount, u32 kKind>
 __device__ __forceinline__ void tile_pass(const LaunchParams& p, const FrontierView& B, const TileSmem& sm, u32 c0,
                                           u32 n, u32 total, u32 tau_bits, Stages& st, Work& wk) {
-  const u32 cs = p.cshift;
   const u32 shift = B.shift;
   u32 known_chunk = 0xFFFFFFFFu;
   for (u32 base = 0; base < total; base += 2u * blockDim.x) {
-    // decode two items per thread
     u32 ii[2], ll[2], ee[2];
     bool live[2];
 #pragma unroll
@@ -126,12 +154,21 @@ __device__ __forceinline__ void tile_pass(const LaunchParams& p, const FrontierV
           if (sm.WI[mid] > w) hi = mid; else lo = mid + 1u;
         }
         const u32 i = lo;
-        const u32 excl = i == 0u ? 0u : sm.WI[i - 1u];
-        const u32 r = w - excl;
-        const u32 deg = sm.DG[i];
+        const u32 r = w - (i == 0u ? 0u : sm.WI[i - 1u]);
+        const u32 lc = sm.LC[i];
+        const u32 deg = kKind == kLocal ? lc : (kKind == kGlobal ? sm.DG[i] - lc : sm.DG[i]);
         const u32 j = r / deg;
+        const u32 k = r - j * deg;
         ii[u] = i;
-        ee[u] = sm.RB[i] + (r - j * deg);
+        if (kKind == kLocal) {
+          ee[u] = sm.LB[i] + k;
+        } else if (kKind == kGlobal) {
+          // the row without its own-tile run [LB, LB + LC)
+          const u32 before = sm.LB[i] - sm.RB[i];
+          ee[u] = k < before ? sm.RB[i] + k : sm.LB[i] + lc + (k - before);
+        } else {
+          ee[u] = sm.RB[i] + k;
+        }
         ll[u] = __fns(sm.M[i], 0u, static_cast<int>(j) + 1);
       }
     }
@@ -142,11 +179,10 @@ __device__ __forceinline__ void tile_pass(const LaunchParams& p, const FrontierV
       if (live[u]) {
         rec[u] = __ldg(p.g.csr + ee[u]);
         const u64 si = (static_cast<u64>(ii[u]) << shift) + ll[u];
-        src[u] = kStaged ? dev::hi(*reinterpret_cast<volatile u64*>(sm.S + si))
-                         : dev::hi(dev::ld_cg(B.dist + (static_cast<u64>(c0) << shift) + si));
+        src[u] = kKind != kInPlace ? dev::hi(*reinterpret_cast<volatile u64*>(sm.S + si))
+                                   : dev::hi(dev::ld_cg(B.dist + (static_cast<u64>(c0) << shift) + si));
       }
     }
-    // admission and compact target
     u32 cdst[2], bitv[2];
     bool relax[2], local[2];
     u64 cand[2], cur[2];
@@ -161,7 +197,9 @@ __device__ __forceinline__ void tile_pass(const LaunchParams& p, const FrontierV
         cdst[u] = rec[u].x - dt.y;
         relax[u] = (dt.x >> ll[u]) & 1u;
         cand[u] = dev::candidate(src[u], rec[u].y, rec[u].z);
-        local[u] = kStaged && (cdst[u] - c0) < n;
+        // own-tile edges whose target lies in the staged unit (all of them
+        // when tiles and units coincide)
+        local[u] = kKind == kLocal && (cdst[u] - c0) < n;
       }
     }
 #pragma unroll
@@ -202,9 +240,10 @@ __device__ __forceinline__ void tile_pass(const LaunchParams& p, const FrontierV
       if (dev::hi(cand[u]) < tau_bits) {
         if (local[u]) {
           atomicOr(sm.P + (cdst[u] - c0), bitv[u]);
+          atomicOr(sm.G + (cdst[u] - c0), bitv[u]);
         } else {
           dev::red_or(B.mask_w + cdst[u], bitv[u]);
-          const u32 chunk = cdst[u] >> cs;
+          const u32 chunk = cdst[u] >> 5;
           if (chunk != known_chunk) {
             const u32 cb = 1u << (chunk & 31u);
             near_claim[u] = (atomicOr(B.cmask_w + (chunk >> 5), cb) & cb) == 0u;
@@ -212,78 +251,53 @@ __device__ __forceinline__ void tile_pass(const LaunchParams& p, const FrontierV
           }
         }
       } else {
-        far_claim[u] = tile_park(B, st, cdst[u], bitv[u], dev::hi(cand[u]));
+        st.fd = min(st.fd, dev::hi(cand[u]));
+        dev::red_min_u32(B.fbound + cdst[u], dev::hi(cand[u]));
+        far_claim[u] = atomicOr(B.fmask + cdst[u], bitv[u]) == 0u;
       }
     }
 #pragma unroll
     for (u32 u = 0; u < 2u; ++u) {
       if (kCount && near_claim[u]) wk.c[4] += 1;
-      stage_push(st, kNear, near_claim[u], cdst[u] >> cs);
+      stage_push(st, kNear, near_claim[u], cdst[u] >> 5);
       stage_push(st, kFar, far_claim[u], queue_word(cdst[u], cdst[u]));
     }
   }
 }
 
-// Snapshot of the pending lanes for a pass: M = P, P = 0, inclusive work
-// scan into WI; returns the block's lane-edge work (block-uniform).
-__device__ __forceinline__ u32 tile_snapshot(const TileSmem& sm, u32 n, u32* warp_sums) {
-  u32 work = 0u;
-  const u32 i = threadIdx.x;
-  if (i < n) {
-    const u32 m = sm.P[i];
-    sm.M[i] = m;
-    sm.P[i] = 0u;
-    work = static_cast<u32>(__popc(m)) * sm.DG[i];
-  }
-  u32 total = 0u;
-  const u32 incl = block_inclusive_scan(work, warp_sums, total);
-  if (i < n) sm.WI[i] = incl;
-  __syncthreads();
-  return total;
-}
-
-// One visit: block item `item` of a near round of a frontier batch (n_queued
-// queued units; dense rounds enumerate every unit).  Executed by the whole
-// block; every branch is block-uniform.
+// One visit of a dense round: tile unit `unit` of a frontier batch.
+// Executed by the whole block; every branch is block-uniform.
 template <bool kCount>
-__device__ void tile_visit(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 n_queued,
-                           u32 tau_bits, const TileSmem& sm, Stages& st, Work& wk) {
+__device__ void tile_visit(const LaunchParams& p, const FrontierView& B, u32 unit, u32 tau_bits, const TileSmem& sm,
+                           Stages& st, Work& wk) {
   __shared__ u32 s_warp[32];
-  __shared__ u32 s_unit;
-  const u32 cs = p.cshift;
-  const u32 units = chunk_count(B.U, cs);
+  __shared__ u32 s_live;
+  const u32 ts = p.tshift;
+  const u32 c0 = unit << ts;
+  const u32 n = min(1u << ts, B.U - c0);
+  // the unit's chunk bits (2^(ts-5) bits of one word): read and clear
   if (threadIdx.x == 0u) {
-    u32 unit;
-    if (chunk_dense(n_queued, B.U, cs)) {
-      // dense round: the item is unit slot `item`; a clear bit means no work
-      const u32 word = dev::ld_cg(B.cmask_r + (item >> 5));
-      unit = ((word >> (item & 31u)) & 1u) ? item : 0xFFFFFFFEu;
-    } else {
-      unit = static_cast<u32>(dev::ld_cg(B.queue_r + item));
-      if (unit >= units) {
-        atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
-        unit = 0xFFFFFFFEu;
-      }
-    }
-    if (unit < units) atomicAnd(B.cmask_r + (unit >> 5), ~(1u << (unit & 31u)));
-    s_unit = unit;
+    const u32 first = c0 >> 5, count = (n + 31u) >> 5;
+    const u32 bits = (count >= 32u ? 0xFFFFFFFFu : ((1u << count) - 1u)) << (first & 31u);
+    s_live = (atomicAnd(B.cmask_r + (first >> 5), ~bits) & bits) != 0u;
   }
   __syncthreads();
-  const u32 unit = s_unit;
-  if (unit >= units) return;
-  const u32 c0 = unit << cs;
-  const u32 n = min(1u << cs, B.U - c0);
-  // 1. pending lanes (cleared) and rows
+  if (!s_live) return;
+  // 1. pending lanes (cleared) and row tables
   const u32 i = threadIdx.x;
   u32 work = 0u;
   if (i < n) {
     const u32 m = dev::ld_cg(B.mask_r + c0 + i) & B.valid;
     const uint2 row = __ldg(B.crow + c0 + i);
+    const uint2 lr = __ldg(B.clrun + c0 + i);
     if (m != 0u) B.mask_r[c0 + i] = 0u;
     sm.P[i] = m;
+    sm.G[i] = m;
     sm.CH[i] = 0u;
     sm.RB[i] = row.x;
     sm.DG[i] = row.y;
+    sm.LB[i] = lr.x;
+    sm.LC[i] = lr.y;
     work = static_cast<u32>(__popc(m)) * row.y;
     if (kCount && m != 0u) {
       wk.c[0] += 1;
@@ -292,16 +306,16 @@ __device__ void tile_visit(const LaunchParams& p, const FrontierView& B, DCtl& C
     }
   }
   u32 total = 0u;
-  (void)block_inclusive_scan(work, s_warp, total);  // block total (the pass rescans)
+  (void)block_inclusive_scan(work, s_warp, total);
   if (total == 0u) return;
   if (total < p.tile_stage_min) {
-    // 4. little work: relax in place
-    const u32 t = tile_snapshot(sm, n, s_warp);
-    tile_pass<kCount, false>(p, B, sm, c0, n, t, tau_bits, st, wk);
+    // 5. little work: every edge in global memory, one pass
+    const u32 t = tile_snapshot<kInPlace>(sm, sm.P, n, s_warp);
+    tile_pass<kCount, kInPlace>(p, B, sm, c0, n, t, tau_bits, st, wk);
     __syncthreads();
     return;
   }
-  // 2. stage the label rows (n x W words, 256-byte aligned: c0 is a multiple of 32)
+  // 2. stage the label rows (n x W words; 256-byte aligned as c0 is a multiple of 32)
   {
     const u32 words = n << B.shift;
     const u64* g = B.dist + (static_cast<u64>(c0) << B.shift);
@@ -312,28 +326,34 @@ __device__ void tile_visit(const LaunchParams& p, const FrontierView& B, DCtl& C
   }
   if (kCount && threadIdx.x == 0u) wk.c[14] += 1;
   __syncthreads();
-  for (u32 it = 0; it < kTileLocalIterations; ++it) {
-    const u32 t = tile_snapshot(sm, n, s_warp);
+  for (u32 it = 0; it < p.tile_iters; ++it) {
+    const u32 t = tile_snapshot<kLocal>(sm, sm.P, n, s_warp);
     if (t == 0u) break;
-    if (kCount && i < n && sm.M[i] != 0u) {
-      if (it > 0u) {
-        wk.c[0] += 1;
-        wk.c[1] += sm.DG[i];
-        wk.c[2] += __popc(sm.M[i]);
-      }
+    if (kCount && it > 0u && i < n && sm.M[i] != 0u) {
+      wk.c[0] += 1;
+      wk.c[1] += sm.LC[i];
+      wk.c[2] += __popc(sm.M[i]);
     }
-    tile_pass<kCount, true>(p, B, sm, c0, n, t, tau_bits, st, wk);
+    tile_pass<kCount, kLocal>(p, B, sm, c0, n, t, tau_bits, st, wk);
     __syncthreads();
   }
-  // leftovers after the cap: the next round picks them up
+  // leftovers after the cap: the next round relaxes all their edges
   bool claim = false;
   if (i < n && sm.P[i] != 0u) {
     dev::red_or(B.mask_w + c0 + i, sm.P[i]);
-    const u32 cb = 1u << (unit & 31u);
-    claim = (atomicOr(B.cmask_w + (unit >> 5), cb) & cb) == 0u;
+    sm.G[i] &= ~sm.P[i];
+    const u32 chunk = (c0 + i) >> 5;
+    const u32 cb = 1u << (chunk & 31u);
+    claim = (atomicOr(B.cmask_w + (chunk >> 5), cb) & cb) == 0u;
   }
-  stage_push(st, kNear, claim, unit);
-  // 3. write back the changed labels
+  stage_push(st, kNear, claim, (c0 + i) >> 5);
+  __syncthreads();
+  // 3. the other edges of every marked lane, once, with its final label
+  {
+    const u32 t = tile_snapshot<kGlobal>(sm, sm.G, n, s_warp);
+    tile_pass<kCount, kGlobal>(p, B, sm, c0, n, t, tau_bits, st, wk);
+  }
+  // 4. write back the changed labels
   {
     const u32 words = n << B.shift;
     u64* g = B.dist + (static_cast<u64>(c0) << B.shift);
@@ -344,76 +364,85 @@ __device__ void tile_visit(const LaunchParams& p, const FrontierView& B, DCtl& C
   __syncthreads();
 }
 
-// One round of the tiled layout: block items drawn from a per-round counter.
-// Frontier near rounds: one unit visit per item; split rounds: 32 far
-// entries per warp of the block; Jacobi / dense batches: one warp item per
-// warp of the block.  Every branch is block-uniform (the item, its batch and
-// the batch's round values are broadcast through shared memory).
+// Work of round r in two prefixes: block items (one tile visit per unit of a
+// frontier batch in a dense near round) and warp items (everything else, as
+// the chunked layout counts them: one queued chunk per sparse near item, 32
+// far entries per split item, Jacobi / dense warp items).
+__device__ u32 round_work_tiled(const LaunchParams& p, u32 r, u32* prefix_block, u32* prefix_warp) {
+  const u32 ridx = r % 3u;
+  block_prefix(prefix_block, p.nb, [&](u32 b) -> u32 {
+    if (engine_of(p, b) != BFX_ENGINE_FRONTIER_PUSH) return 0u;
+    const DBatch& B = p.batches[b];
+    const u32 n = min(dev::ld_cg(&p.ctl[b].count[ridx]), B.U);
+    return n != 0u && chunk_dense(n, B.U, 5u) ? chunk_count(B.U, p.tshift) : 0u;
+  });
+  block_prefix(prefix_warp, p.nb, [&](u32 b) -> u32 {
+    const DBatch& B = p.batches[b];
+    if (engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH) {
+      const DCtl& C = p.ctl[b];
+      const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
+      if (n != 0u) return chunk_dense(n, B.U, 5u) ? 0u : n;
+      const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
+      return (f + 31u) >> 5;
+    }
+    return batch_exec(p, b, ridx) != 0u ? (((B.U << B.shift) + 31u) >> 5) : 0u;
+  });
+  return prefix_block[p.nb] + prefix_warp[p.nb];
+}
+
+// One round of the tiled layout.  Phase 1: block items drawn from a
+// per-round counter, one tile visit each (block-uniform branches only,
+// their values broadcast through shared memory).  Phase 2: the warp items,
+// run by the chunked layout's round body (each warp draws its own items).
 template <bool kCount>
-__device__ void round_body_tiled(const LaunchParams& p, u32 r, u32* prefix, Work& wk) {
+__device__ void round_body_tiled(const LaunchParams& p, u32 r, u32* prefix_block, u32* prefix_warp, Work& wk) {
   __shared__ u32 s_item;
-  __shared__ u32 s_vals[5];
+  __shared__ u32 s_vals[3];
   const u32 ridx = r % 3u, widx = (r + 1u) % 3u;
-  const u32 total = prefix[p.nb];
-  const u32 nw = blockDim.x >> 5, wib = threadIdx.x >> 5;
-  const TileSmem sm = tile_smem(prefix, p.nb, p.cshift, p.tile_wmax);
+  const u32 total = prefix_block[p.nb];
+  const u32 wib = threadIdx.x >> 5;
+  const TileSmem sm = tile_smem(prefix_block, p.nb, p.tshift, p.tile_wmax);
   Stages st{{0u, 0u}, 0xFFFFFFFFu};
   u32 staged_batch = 0xFFFFFFFFu;
-  for (;;) {
+  while (total != 0u) {
     if (threadIdx.x == 0u) s_item = atomicAdd(&p.run->items[ridx], 1u);
     __syncthreads();
     const u32 w = s_item;
     __syncthreads();
     if (w >= total) break;
-    const u32 b = find_batch(prefix, p.nb, w);
+    const u32 b = find_batch(prefix_block, p.nb, w);
     const DBatch& B = p.batches[b];
     DCtl& C = p.ctl[b];
-    const u32 item = w - prefix[b];
-    const u32 eng = engine_of(p, b);
-    if (eng == BFX_ENGINE_FRONTIER_PUSH) {
-      if (threadIdx.x == 0u) {
-        const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
-        const u32 g = dev::ld_cg(&C.gen[r & 1u]);
-        const u32 tau = dev::ld_cg(&C.tau[r & 1u]);
-        s_vals[0] = n;
-        s_vals[1] = g;
-        s_vals[2] = tau;
-        s_vals[3] = n == 0u ? min(dev::ld_cg(&C.fcount[g % 3u]), B.U) : 0u;
-        s_vals[4] = n == 0u ? split_threshold(C, tau, g % 3u) : 0u;
-      }
-      __syncthreads();
-      const u32 n = s_vals[0], g = s_vals[1], tau = s_vals[2], f = s_vals[3], tau_next = s_vals[4];
-      __syncthreads();
-      const FrontierView V = frontier_view(B, r & 1u, g % 3u, (g + 1u) % 3u);
-      if (b != staged_batch) {
-        stages_flush(st);
-        staged_batch = b;
-        const u32 po = n != 0u ? g % 3u : (g + 1u) % 3u;
-        if (lane_id() == 0u) {
-          s_stage_queue[kNear][wib] = StageQueue{V.queue_w, &C.count[widx], &C.error_bits, V.U};
-          s_stage_queue[kFar][wib] = StageQueue{n != 0u ? V.pile : V.pile_out, &C.fcount[po], &C.error_bits, V.U};
-          s_fmin_target[wib] = &C.fmin[po];
-        }
-        __syncwarp();
-      }
-      if (n != 0u) {
-        tile_visit<kCount>(p, V, C, item, n, tau, sm, st, wk);
-      } else {
-        split_group<kCount, true>(p, V, C, item * nw + wib, f, tau_next, st, wk);
-      }
-    } else if (eng == BFX_ENGINE_JACOBI_PULL) {
-      jacobi_item<kCount>(p, B, C, item * nw + wib, r, widx, wk);
-    } else {
-      dense_item<kCount>(p, B, C, item * nw + wib, batch_exec(p, b, ridx), widx, wk);
+    if (threadIdx.x == 0u) {
+      s_vals[0] = dev::ld_cg(&C.gen[r & 1u]);
+      s_vals[1] = dev::ld_cg(&C.tau[r & 1u]);
     }
+    __syncthreads();
+    const u32 g = s_vals[0], tau = s_vals[1];
+    __syncthreads();
+    const FrontierView V = frontier_view(B, r & 1u, g % 3u, (g + 1u) % 3u);
+    if (b != staged_batch) {
+      stages_flush(st);
+      staged_batch = b;
+      if (lane_id() == 0u) {
+        s_stage_queue[kNear][wib] = StageQueue{V.queue_w, &C.count[widx], &C.error_bits, V.U};
+        s_stage_queue[kFar][wib] = StageQueue{V.pile, &C.fcount[g % 3u], &C.error_bits, V.U};
+        s_fmin_target[wib] = &C.fmin[g % 3u];
+      }
+      __syncwarp();
+    }
+    tile_visit<kCount>(p, V, w - prefix_block[b], tau, sm, st, wk);
   }
   stages_flush(st);
+  __syncthreads();
+  round_body<kCount, 2, true>(p, r, prefix_warp, wk);
 }
 
-// Persistent cooperative kernel of the tiled layout: 256-thread blocks, two
-// per SM by launch bounds (the staged labels take up to 64 KB per block).
-template <bool kCount>
-__global__ void __launch_bounds__(256, 2) persistent_tiled_kernel(LaunchParams p) {
+// Persistent cooperative kernel of the tiled layout: blocks of kThreads
+// (256: up to 128 registers; 384: 80), two per SM by launch bounds (the
+// staged labels take up to 64 KB per block).
+template <bool kCount, int kThreads>
+__global__ void __launch_bounds__(kThreads, 2) persistent_tiled_kernel(LaunchParams p) {
   extern __shared__ u32 prefix[];
   const u32 nblocks = gridDim.x;
   Work wk;
@@ -421,8 +450,9 @@ __global__ void __launch_bounds__(256, 2) persistent_tiled_kernel(LaunchParams p
   u64 traced[2] = {0u, 0u};
   const u64 t0 = dev::global_ns();
   u32 r = 0;
+  u32* const prefix_warp = prefix + (p.nb + 1u);
   for (;; ++r) {
-    const u32 total = round_work(p, r, prefix);
+    const u32 total = round_work_tiled(p, r, prefix, prefix_warp);
     if (total == 0u || r >= p.max_rounds) break;
     if (blockIdx.x == 0) round_bookkeeping(p, r);
     if (p.round_trace != nullptr && blockIdx.x == 0 && threadIdx.x < 32u && r < p.trace_cap) {
@@ -433,7 +463,7 @@ __global__ void __launch_bounds__(256, 2) persistent_tiled_kernel(LaunchParams p
         p.round_trace[4u * r + 1u] = total | (static_cast<u64>(splits) << 32);
       }
     }
-    round_body_tiled<kCount>(p, r, prefix, wk);
+    round_body_tiled<kCount>(p, r, prefix, prefix_warp, wk);
     if (kCount && p.round_trace != nullptr && r < p.trace_cap) trace_round_work(p, r, wk, traced);
     if (blockIdx.x == 0 && threadIdx.x == 0 && dev::global_ns() - t0 > p.budget_ns) {
       atomicExch(&p.run->sync.abort, 1u);

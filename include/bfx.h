@@ -327,6 +327,10 @@ int bfx_set_frontier_layout(bfx_workspace *ws, uint32_t layout);
  * `lane_edges` relaxes in global memory without staging its labels (bfx
  * extension; results unchanged; default 1024). */
 int bfx_set_tile_stage_min(bfx_workspace *ws, uint32_t lane_edges);
+/* Tiled layout: local relaxation passes per staged tile visit (1..1024,
+ * default 32); lanes still pending after them are relaxed in the next round
+ * (bfx extension; results unchanged). */
+int bfx_set_tile_passes(bfx_workspace *ws, uint32_t passes);
 /* Register budget of the persistent relaxation kernel (a bfx tuning option,
  * results unchanged): 40 registers per thread (three 512-thread blocks per
  * SM), 64 (two 512-thread blocks per SM: no spills in the group layout, few

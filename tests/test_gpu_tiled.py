@@ -21,7 +21,7 @@ STAGE = {"staged": 0, "default": 1024, "unstaged": 1 << 30}
 
 
 def run_tiled(layout, descs, stage_min=1024, deltas=None, engines=None, instr=0, max_rounds=1 << 30,
-              control=bfx.CONTROL_PERSISTENT):
+              control=bfx.CONTROL_PERSISTENT, block=256):
     res = bfx.ResidentDeviceGraph.upload_once(layout)
     ws = bfx.Workspace(res)
     ws.set_frontier_layout(bfx.FRONTIER_TILED)
@@ -34,7 +34,7 @@ def run_tiled(layout, descs, stage_min=1024, deltas=None, engines=None, instr=0,
         ws.set_batch_engines(engines)
         engine = bfx.ENGINE_AUTO
     ws.execute(bfx.GpuRunOptions(engine=engine, instrumentation=instr, maximum_rounds=max_rounds,
-                                 control_mode=control))
+                                 control_mode=control, block_size=block))
     st = ws.fetch_statuses()
     labels = [ws.download_labels(b, d.lane_width) for b, d in enumerate(descs)]
     work = ws.engine_work() if instr else None
@@ -74,6 +74,7 @@ def test_c1_full_graph_tiled(gpu, c1, stage, step, instr):
             assert work["tiled"]["local_relaxations"] > 0 and work["tiled"]["staged_visits"] > 0
         if stage == "unstaged":
             assert work["tiled"]["local_relaxations"] == 0 and work["tiled"]["staged_visits"] == 0
+        assert work["tiled"]["local_relaxations"] <= relax
 
 
 @pytest.fixture(scope="module")
@@ -88,11 +89,13 @@ def c2_regional():
 
 @pytest.mark.parametrize("stage", ["staged", "default", "unstaged"])
 @pytest.mark.parametrize("step", [None, 3.0])
-def test_regional_batches_tiled(gpu, c2_regional, stage, step):
+@pytest.mark.parametrize("block", [256, 384])
+def test_regional_batches_tiled(gpu, c2_regional, stage, step, block):
     """128-vertex tiles (2^7), regional batches of widths 1..32 in one launch."""
     layout, descs, lanes = c2_regional
     assert len({d.lane_width for d in descs}) >= 2
-    st, labels, _ = run_tiled(layout, descs, STAGE[stage], None if step is None else [step] * len(descs))
+    st, labels, _ = run_tiled(layout, descs, STAGE[stage], None if step is None else [step] * len(descs),
+                              block=block)
     check_batches(layout, descs, lanes, st, labels, Oracle.from_layout(layout))
 
 
@@ -105,14 +108,15 @@ def test_regional_batches_tiled_mixed_engines(gpu, c2_regional):
 
 
 @pytest.mark.parametrize("step", [None, 2.0])
-def test_c3_shaped_full_graph_w32_tiled(gpu, step):
+@pytest.mark.parametrize("block", [256, 384])
+def test_c3_shaped_full_graph_w32_tiled(gpu, step, block):
     """256-vertex tiles (2^8, 64 KB of staged labels at W=32): the c3
     generator on 16x16 tiles, one full-graph batch of 32 sources."""
     layout, grid = workloads.build_graph("c3", scale_tiles=(16, 16))
     qs = workloads.full_graph_queries(layout, grid, 32, seed=77)
     d = bfx.make_description(layout, qs, 32)
     wbar = float(np.mean(layout.arrays["csr_weights"]))
-    st, labels, _ = run_tiled(layout, [d], 1024, None if step is None else [step * wbar])
+    st, labels, _ = run_tiled(layout, [d], 1024, None if step is None else [step * wbar], block=block)
     check_batches(layout, [d], [qs], st, labels, Oracle.from_layout(layout))
 
 
