@@ -71,3 +71,72 @@ def test_replica_shards_gather_and_max_timing():
             assert [x[0] - 1 for x in recs[r]] == shards0[r]
             assert all(x[1] == r and x[2] == bfx.STOP_CONVERGED for x in recs[r])
         assert out[rank][3] == 2.0  # max over ranks
+
+
+def _shard_worker(rank, world, port, queue):
+    """One rank of a sharded run: the whole query set is planned on every
+    rank, this rank takes its shard of batches (balanced lane-edges), runs
+    each valid lane through the oracle as the runner, and the per-query
+    results are all-gathered."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle.oracle import Oracle
+        layout, grid = workloads.build_graph("c2", scale_tiles=(16, 16))
+        qs = workloads.box_queries(layout, grid, 40, 2, 8, seed=5, targets=(1, 3))
+        plan = bfx.make_overlapping_batch_plan(layout, qs, bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True))
+        descs = plan.descriptions()
+        mine = workloads.shard_batches([e[3] for e in plan.estimates], world)[rank]
+        orc = Oracle.from_layout(layout)
+        results = {}
+        for b in mine:
+            d = descs[b]
+            for lane in range(d.lane_width):
+                if not (d.valid_lane_mask >> lane) & 1:
+                    continue
+                qi = int(d.query_index_by_lane[lane])
+                q = qs[qi]
+                od, op = orc.region_sssp(q.sources, q.targets, q.selected_tiles)
+                tg = np.asarray(q.targets, np.int64)
+                results[qi] = (od[tg].tolist(), op[tg].tolist(), int(od.astype(np.uint64).sum()), rank)
+        gathered = [None] * world
+        dist.all_gather_object(gathered, results)
+        queue.put((rank, gathered, len(descs)))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def test_sharded_query_set_equals_one_rank_run():
+    """bench.py --shard's split (not measured on GPUs here): two gloo ranks
+    share one planned query set by shard_batches; the union of their gathered
+    per-query results covers every query exactly once and equals the one-rank
+    run of the whole set."""
+    from oracle.oracle import Oracle
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    port = 30500 + (os.getpid() % 1000)
+    procs = [ctx.Process(target=_shard_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get() for _ in range(world)]
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    out.sort(key=lambda x: x[0])
+    assert out[0][1] == out[1][1]  # every rank holds the same gathered set
+    merged = {}
+    for part in out[0][1]:
+        assert not set(part) & set(merged)  # no query on two ranks
+        merged.update(part)
+    assert {r for v in merged.values() for r in [v[3]]} == {0, 1}  # both ranks did work
+    layout, grid = workloads.build_graph("c2", scale_tiles=(16, 16))
+    qs = workloads.box_queries(layout, grid, 40, 2, 8, seed=5, targets=(1, 3))
+    assert sorted(merged) == list(range(len(qs)))
+    orc = Oracle.from_layout(layout)
+    for qi, qq in enumerate(qs):
+        od, op = orc.region_sssp(qq.sources, qq.targets, qq.selected_tiles)
+        tg = np.asarray(qq.targets, np.int64)
+        assert merged[qi][:3] == (od[tg].tolist(), op[tg].tolist(), int(od.astype(np.uint64).sum()))
