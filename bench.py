@@ -9,8 +9,9 @@ queries with box sides U[4,64] tiles, one source and one target each; the
 planner groups overlapping queries into batches (narrowed to 1/8/16/32
 lanes) and one persistent cooperative launch relaxes all of them.  On one GPU
 the default run also times c3 (64 full-graph sources on 256x256 tiles x 256
-nodes, 16.8M V / 168M E, uint costs) and reports it in the line's `c3`
-object with its own roofline.
+nodes, 16.8M V / 168M E, uint costs) and c5 (4,096 regional + 16 full-graph
+queries on the same graph) and reports them in the line's `c3` and `c5`
+objects, each with its own roofline and plain per-query comparison.
 
 A step is one pass of the hot path over the whole query set: labels reset,
 seeded, relaxed to convergence, targets classified.  `value` times the steps
@@ -528,6 +529,12 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
     return line, lane_images
 
 
+def bfx_policy_regional():
+    """The planner policy of the regional workloads (c2, c5)."""
+    import bfx
+    return bfx.BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -556,7 +563,7 @@ def main():
                     help="tiled layout: lane-edge work from which a tile visit stages its labels")
     ap.add_argument("--shard", action="store_true",
                     help="multi-GPU: split one query set's batches over the ranks (strong scaling)")
-    ap.add_argument("--no-c3", action="store_true", help="skip the c3 object of the default c2 run")
+    ap.add_argument("--no-c3", action="store_true", help="skip the c3 and c5 objects of the default c2 run")
     ap.add_argument("--c3-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=None)
@@ -601,16 +608,23 @@ def main():
         line["cpu_baseline"] = cb
         line["parity"] = parity
     if args.workload == "c2" and world == 1 and not args.no_c3 and args.queries is None:
-        # the c3 full-graph configuration, timed in the same run (its own roofline)
+        # the c3 full-graph configuration and the c5 mixed set on the same
+        # graph, timed in the same run (each with its own roofline)
         del wl
         t0 = time.time()
         wl3 = workloads.bench_workload("c3")
         log(f"[bench] c3 graph+layout {time.time() - t0:.1f}s")
+        keep = ("metric", "value", "unit", "steps", "warmup", "ms_per_step", "gteps", "e2e", "host", "roofline",
+                "clocks", "config", "plain_per_query", "max_finite_distance", "gpu_launches")
         c3, _ = measure(wl3, args, rank=rank, world=world, dist=dist, device=device, steps=args.c3_steps,
                         warmup=3, shard=False)
-        line["c3"] = {k: c3[k] for k in ("metric", "value", "unit", "steps", "warmup", "ms_per_step", "gteps",
-                                          "e2e", "host", "roofline", "clocks", "config", "plain_per_query",
-                                          "max_finite_distance", "gpu_launches")}
+        line["c3"] = {k: c3[k] for k in keep}
+        q5, classes5 = workloads.bench_queries("c5", wl3.layout, wl3.grid)
+        wl5 = workloads.BenchWorkload("c5", wl3.graph_input, wl3.order, wl3.layout, wl3.grid, q5, classes5,
+                                      bfx_policy_regional(), workloads.BENCH_DESCRIPTIONS["c5"], True)
+        c5, _ = measure(wl5, args, rank=rank, world=world, dist=dist, device=device, steps=args.c3_steps,
+                        warmup=3, shard=False)
+        line["c5"] = {k: c5[k] for k in keep}
     if rank == 0:
         print(json.dumps(line))
     if dist:

@@ -11,8 +11,10 @@
 // never revisits a vertex; a revisit needs an equal-distance (zero-weight)
 // step, so the walk tracks runs of equal distances and hands a target to the
 // exact backtracking search (reconstruct_target, src/compact_paths.cpp:131-211)
-// when a run revisits a vertex or grows long.  That search runs serially per
-// flagged target with scratch sized by the largest union.
+// when a run revisits a vertex or grows long.  Flagged targets are gathered
+// into a list and searched in parallel, one thread per target over a bounded
+// number of search slots (each with its own stacks and on-path marks sized by
+// the largest union).
 //
 // Two passes as in the reference: summaries (status, source, distance,
 // length), then, after a host prefix over the lengths, the payload (path
@@ -46,12 +48,18 @@ struct PathArgs {
   u32* out_vertices;
   float* out_labels;
   u32* out_edges;
-  // search scratch
+  // search scratch: `slots` search slots, each with its own stacks
+  // (slot_stride words apart) and on-path bitmap (mark_stride words apart)
   u32* stack_v;
   u32* stack_c;
   u32* stack_e;
   u32* on_path;  // bitmap over compact vertices
   u32 max_union;
+  u32 slots;
+  u64 slot_stride;
+  u64 mark_stride;
+  u32* flagged;        // [targets] indices of the targets the walk handed over
+  u32* flagged_count;  // [1]
 };
 
 __device__ __forceinline__ u32 lane_of(const u32* offsets, u32 W, u32 pos) {
@@ -163,23 +171,36 @@ __global__ void summaries_kernel(PathArgs a) {
 // candidates in stable-edge-id order, predecessors on the current path
 // skipped, dead ends popped.  Returns the edge count (or ~0u if no path) and
 // leaves the path on the stacks (stack_v[0] = target).
-__device__ u32 search_target(const PathArgs& a, const DBatch& B, const u64* d, u32 t, u32 lane) {
+struct SearchSlot {
+  u32* stack_v;
+  u32* stack_c;
+  u32* stack_e;
+  u32* on_path;
+};
+
+__device__ __forceinline__ SearchSlot search_slot(const PathArgs& a, u32 slot) {
+  return SearchSlot{a.stack_v + slot * a.slot_stride, a.stack_c + slot * a.slot_stride,
+                    a.stack_e + slot * a.slot_stride, a.on_path + slot * a.mark_stride};
+}
+
+__device__ u32 search_target(const PathArgs& a, const SearchSlot& sl, const DBatch& B, const u64* d, u32 t,
+                             u32 lane) {
   auto cv = [&](u32 v) { return v - B.tiles[a.g.owner[v]].y; };
   auto mark = [&](u32 v, bool on) {
     const u32 c = cv(v);
-    if (on) a.on_path[c >> 5] |= 1u << (c & 31u); else a.on_path[c >> 5] &= ~(1u << (c & 31u));
+    if (on) sl.on_path[c >> 5] |= 1u << (c & 31u); else sl.on_path[c >> 5] &= ~(1u << (c & 31u));
   };
   auto marked = [&](u32 v) {
     const u32 c = cv(v);
-    return (a.on_path[c >> 5] >> (c & 31u)) & 1u;
+    return (sl.on_path[c >> 5] >> (c & 31u)) & 1u;
   };
   int depth = 0;
-  a.stack_v[0] = t;
-  a.stack_c[0] = 0u;
+  sl.stack_v[0] = t;
+  sl.stack_c[0] = 0u;
   mark(t, true);
   u32 found = 0xFFFFFFFFu;
   while (depth >= 0) {
-    const u32 v = a.stack_v[depth];
+    const u32 v = sl.stack_v[depth];
     const u64 wv = label(a.g, B, d, v, lane);
     if (static_cast<u32>(wv) == 0u) {  // a source of this lane
       found = static_cast<u32>(depth);
@@ -189,7 +210,7 @@ __device__ u32 search_target(const PathArgs& a, const DBatch& B, const u64* d, u
     u32 best = 0xFFFFFFFFu, bu = 0u;
     for (u32 q = a.g.csc_off[v]; q < a.g.csc_off[v + 1]; ++q) {
       const uint4 rec = a.g.csc[q];
-      if (rec.z <= a.stack_c[depth] || rec.z >= best) continue;
+      if (rec.z <= sl.stack_c[depth] || rec.z >= best) continue;
       const uint2 su = B.tiles[rec.w];
       if (((su.x >> lane) & 1u) == 0u) continue;
       const u32 du = dev::hi(d[(static_cast<u64>(rec.x - su.y) << B.shift) + lane]);
@@ -203,35 +224,47 @@ __device__ u32 search_target(const PathArgs& a, const DBatch& B, const u64* d, u
       --depth;
       continue;
     }
-    a.stack_c[depth] = best;
+    sl.stack_c[depth] = best;
     if (marked(bu)) continue;
     ++depth;
-    a.stack_v[depth] = bu;
-    a.stack_c[depth] = 0u;
-    a.stack_e[depth] = best - 1u;
+    sl.stack_v[depth] = bu;
+    sl.stack_c[depth] = 0u;
+    sl.stack_e[depth] = best - 1u;
     mark(bu, true);
   }
   // clear the marks of the path that remained (popped vertices are clear)
   if (found != 0xFFFFFFFFu) {
-    for (u32 k = 0; k <= found; ++k) mark(a.stack_v[k], false);
+    for (u32 k = 0; k <= found; ++k) mark(sl.stack_v[k], false);
   }
   return found;
 }
 
-// Serial pass over flagged targets (rare: zero-weight ties that revisit).
-// payload == false: fill summaries; true: write the payload.
-__global__ void search_kernel(PathArgs a, bool payload) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+// Gathers the indices of the targets the walk handed to the search.
+__global__ void flag_list_kernel(PathArgs a) {
   const u32 total = a.target_base[a.batch_count];
-  for (u32 i = 0; i < total; ++i) {
-    if ((a.lengths[i] & kFallback) == 0u) continue;
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    if ((a.lengths[i] & kFallback) != 0u) a.flagged[atomicAdd(a.flagged_count, 1u)] = i;
+  }
+}
+
+// The flagged targets (rare: zero-weight ties that revisit), one thread per
+// target over `slots` search slots; each target's result depends only on
+// the labels, so the order is free.  payload == false: fill summaries;
+// true: write the payload.
+__global__ void search_kernel(PathArgs a, bool payload) {
+  const u32 slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= a.slots) return;
+  const SearchSlot sl = search_slot(a, slot);
+  const u32 count = *a.flagged_count;
+  for (u32 k = slot; k < count; k += a.slots) {
+    const u32 i = a.flagged[k];
     const u32 bi = find_b(a.target_base, a.batch_count, i);
     const u32 b = a.first_batch + bi;
     const DBatch& B = a.batches[b];
     const u32 pos = i - a.target_base[bi];
     const u32 lane = lane_of(B.tgt_off, B.W, pos);
     const u64* d = B.dist[a.status[b].final_distance_slot];
-    const u32 n = search_target(a, B, d, B.tgt[pos], lane);
+    const u32 n = search_target(a, sl, B, d, B.tgt[pos], lane);
     if (!payload) {
       bfx_compact_target_summary& s = a.summaries[i];
       if (n == 0xFFFFFFFFu) {
@@ -239,16 +272,16 @@ __global__ void search_kernel(PathArgs a, bool payload) {
       } else {
         s.reconstruction = 0u;
         s.path_length = n;
-        s.selected_source = a.stack_v[n];
+        s.selected_source = sl.stack_v[n];
         s.has_selected_source = 1u;
       }
     } else if (n != 0xFFFFFFFFu) {
       const u64 vo = a.vertex_offsets[i], eo = a.edge_offsets[i];
-      for (u32 k = 0; k <= n; ++k) {
-        const u32 v = a.stack_v[n - k];
-        a.out_vertices[vo + k] = v;
-        a.out_labels[vo + k] = __uint_as_float(dev::hi(label(a.g, B, d, v, lane)));
-        if (k < n) a.out_edges[eo + k] = a.stack_e[n - k];
+      for (u32 j = 0; j <= n; ++j) {
+        const u32 v = sl.stack_v[n - j];
+        a.out_vertices[vo + j] = v;
+        a.out_labels[vo + j] = __uint_as_float(dev::hi(label(a.g, B, d, v, lane)));
+        if (j < n) a.out_edges[eo + j] = sl.stack_e[n - j];
       }
     }
   }
@@ -385,19 +418,24 @@ __global__ void adjoint_walk_kernel(PathArgs a, const float* grads, unsigned lon
   }
 }
 
+// The flagged targets' paths by search, one thread per target over the
+// search slots (the exact accumulation makes the order free).
 __global__ void adjoint_search_kernel(PathArgs a, const float* grads, unsigned long long* acc) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  const u32 total = a.target_base[a.batch_count];
-  for (u32 i = 0; i < total; ++i) {
-    if ((a.lengths[i] & kFallback) == 0u || a.summaries[i].reconstruction != 0u || grads[i] == 0.0f) continue;
+  const u32 slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= a.slots) return;
+  const SearchSlot sl = search_slot(a, slot);
+  const u32 count = *a.flagged_count;
+  for (u32 k = slot; k < count; k += a.slots) {
+    const u32 i = a.flagged[k];
+    if (a.summaries[i].reconstruction != 0u || grads[i] == 0.0f) continue;
     const u32 bi = find_b(a.target_base, a.batch_count, i);
     const u32 b = a.first_batch + bi;
     const DBatch& B = a.batches[b];
     const u32 pos = i - a.target_base[bi];
     const u32 lane = lane_of(B.tgt_off, B.W, pos);
     const u64* d = B.dist[a.status[b].final_distance_slot];
-    const u32 n = search_target(a, B, d, B.tgt[pos], lane);
-    for (u32 k = 1; k <= n && n != 0xFFFFFFFFu; ++k) exact_add(acc + 4ull * a.stack_e[k], grads[i]);
+    const u32 n = search_target(a, sl, B, d, B.tgt[pos], lane);
+    for (u32 j = 1; j <= n && n != 0xFFFFFFFFu; ++j) exact_add(acc + 4ull * sl.stack_e[j], grads[i]);
   }
 }
 
@@ -412,40 +450,77 @@ void check_ready(bfx_workspace* ws) {
   require(ws->executed, "no executed batches");
 }
 
-// PathArgs over the workspace's path buffer for the batches of the last
-// summaries pass (same layout the summaries pass wrote).
-PathArgs path_args(bfx_workspace* ws) {
-  const std::uint64_t T = ws->path_targets;
-  const std::uint32_t batch_count = ws->path_batch_count;
-  std::uint32_t max_union = 0;
-  for (std::uint32_t i = 0; i < batch_count; ++i) max_union = std::max(max_union, ws->batches[ws->path_first_batch + i].U);
+// Layout of the workspace's path buffer for `targets` targets of
+// `batch_count` batches whose largest union has `max_union` vertices:
+// target prefix, summaries, walk lengths, payload offsets, the flagged list,
+// then the search slots (stacks and on-path bitmaps).  The number of slots is
+// what fits a 256 MB scratch budget (at least 1, at most 256).
+struct PathLayout {
+  size_t o_tb, o_sum, o_len, o_vo, o_eo, o_fl, o_fc, o_sv, o_sc, o_se, o_op, total;
+  u32 slots;
+  u64 slot_stride, mark_stride;
+};
+
+PathLayout path_layout(std::uint64_t T, std::uint32_t batch_count, std::uint32_t max_union) {
+  PathLayout L{};
+  L.slot_stride = align256((size_t{max_union} + 1) * 4) / 4;
+  L.mark_stride = align256((size_t{max_union} / 32 + 1) * 4) / 4;
+  const size_t per_slot = 3 * L.slot_stride * 4 + L.mark_stride * 4;
+  L.slots = static_cast<u32>(std::max<size_t>(1, std::min<size_t>(256, (size_t{256} << 20) / per_slot)));
+  L.o_tb = 0;
+  L.o_sum = align256(L.o_tb + (batch_count + 1) * 4);
+  L.o_len = align256(L.o_sum + T * sizeof(bfx_compact_target_summary));
+  L.o_vo = align256(L.o_len + T * 4);
+  L.o_eo = align256(L.o_vo + T * 8);
+  L.o_fl = align256(L.o_eo + T * 8);
+  L.o_fc = align256(L.o_fl + T * 4);
+  L.o_sv = align256(L.o_fc + 4);
+  L.o_sc = L.o_sv + size_t{L.slots} * L.slot_stride * 4;
+  L.o_se = L.o_sc + size_t{L.slots} * L.slot_stride * 4;
+  L.o_op = L.o_se + size_t{L.slots} * L.slot_stride * 4;
+  L.total = align256(L.o_op + size_t{L.slots} * L.mark_stride * 4);
+  return L;
+}
+
+PathArgs path_args_at(bfx_workspace* ws, const PathLayout& L, std::uint32_t first_batch, std::uint32_t batch_count,
+                      std::uint32_t max_union) {
   char* base = static_cast<char*>(ws->paths.ptr);
-  const size_t o_tb = 0;
-  const size_t o_sum = align256(o_tb + (batch_count + 1) * 4);
-  const size_t o_len = align256(o_sum + T * sizeof(bfx_compact_target_summary));
-  const size_t o_vo = align256(o_len + T * 4);
-  const size_t o_eo = align256(o_vo + T * 8);
-  const size_t o_sv = align256(o_eo + T * 8);
-  const size_t o_sc = align256(o_sv + (size_t{max_union} + 1) * 4);
-  const size_t o_se = align256(o_sc + (size_t{max_union} + 1) * 4);
-  const size_t o_op = align256(o_se + (size_t{max_union} + 1) * 4);
   PathArgs a{};
   a.g = ws->graph->g;
   a.batches = ws->params.batches;
   a.status = ws->d_status;
-  a.first_batch = ws->path_first_batch;
+  a.first_batch = first_batch;
   a.batch_count = batch_count;
-  a.target_base = reinterpret_cast<const std::uint32_t*>(base + o_tb);
-  a.summaries = reinterpret_cast<bfx_compact_target_summary*>(base + o_sum);
-  a.lengths = reinterpret_cast<std::uint32_t*>(base + o_len);
-  a.vertex_offsets = reinterpret_cast<const std::uint64_t*>(base + o_vo);
-  a.edge_offsets = reinterpret_cast<const std::uint64_t*>(base + o_eo);
-  a.stack_v = reinterpret_cast<std::uint32_t*>(base + o_sv);
-  a.stack_c = reinterpret_cast<std::uint32_t*>(base + o_sc);
-  a.stack_e = reinterpret_cast<std::uint32_t*>(base + o_se);
-  a.on_path = reinterpret_cast<std::uint32_t*>(base + o_op);
+  a.target_base = reinterpret_cast<const std::uint32_t*>(base + L.o_tb);
+  a.summaries = reinterpret_cast<bfx_compact_target_summary*>(base + L.o_sum);
+  a.lengths = reinterpret_cast<std::uint32_t*>(base + L.o_len);
+  a.vertex_offsets = reinterpret_cast<const std::uint64_t*>(base + L.o_vo);
+  a.edge_offsets = reinterpret_cast<const std::uint64_t*>(base + L.o_eo);
+  a.flagged = reinterpret_cast<std::uint32_t*>(base + L.o_fl);
+  a.flagged_count = reinterpret_cast<std::uint32_t*>(base + L.o_fc);
+  a.stack_v = reinterpret_cast<std::uint32_t*>(base + L.o_sv);
+  a.stack_c = reinterpret_cast<std::uint32_t*>(base + L.o_sc);
+  a.stack_e = reinterpret_cast<std::uint32_t*>(base + L.o_se);
+  a.on_path = reinterpret_cast<std::uint32_t*>(base + L.o_op);
   a.max_union = max_union;
+  a.slots = L.slots;
+  a.slot_stride = L.slot_stride;
+  a.mark_stride = L.mark_stride;
   return a;
+}
+
+std::uint32_t largest_union(bfx_workspace* ws, std::uint32_t first_batch, std::uint32_t batch_count) {
+  std::uint32_t m = 0;
+  for (std::uint32_t i = 0; i < batch_count; ++i) m = std::max(m, ws->batches[first_batch + i].U);
+  return m;
+}
+
+// PathArgs over the workspace's path buffer for the batches of the last
+// summaries pass (same layout the summaries pass wrote).
+PathArgs path_args(bfx_workspace* ws) {
+  const std::uint32_t mu = largest_union(ws, ws->path_first_batch, ws->path_batch_count);
+  return path_args_at(ws, path_layout(ws->path_targets, ws->path_batch_count, mu), ws->path_first_batch,
+                      ws->path_batch_count, mu);
 }
 
 }  // namespace
@@ -462,48 +537,24 @@ int bfx_compact_path_summaries(bfx_workspace* ws, uint32_t first_batch, uint32_t
       throw std::out_of_range("batch range");
     BFX_CUDA(cudaSetDevice(ws->graph->device));
     std::vector<std::uint32_t> tbase(batch_count + 1, 0U);
-    std::uint32_t max_union = 0;
-    for (std::uint32_t i = 0; i < batch_count; ++i) {
-      const bfx::DBatch& B = ws->batches[first_batch + i];
-      tbase[i + 1] = tbase[i] + B.tgt_count;
-      max_union = std::max(max_union, B.U);
-    }
+    for (std::uint32_t i = 0; i < batch_count; ++i) tbase[i + 1] = tbase[i] + ws->batches[first_batch + i].tgt_count;
+    const std::uint32_t max_union = bfx::largest_union(ws, first_batch, batch_count);
     const std::uint64_t T = tbase[batch_count];
-    const size_t o_tb = 0;
-    const size_t o_sum = bfx::align256(o_tb + (batch_count + 1) * 4);
-    const size_t o_len = bfx::align256(o_sum + T * sizeof(bfx_compact_target_summary));
-    const size_t o_vo = bfx::align256(o_len + T * 4);
-    const size_t o_eo = bfx::align256(o_vo + T * 8);
-    const size_t o_sv = bfx::align256(o_eo + T * 8);
-    const size_t o_sc = bfx::align256(o_sv + (size_t{max_union} + 1) * 4);
-    const size_t o_se = bfx::align256(o_sc + (size_t{max_union} + 1) * 4);
-    const size_t o_op = bfx::align256(o_se + (size_t{max_union} + 1) * 4);
-    const size_t total = bfx::align256(o_op + (size_t{max_union} / 32 + 1) * 4);
-    ws->paths.reserve(total, ws->graph->device);
+    const bfx::PathLayout L = bfx::path_layout(T, batch_count, max_union);
+    ws->paths.reserve(L.total, ws->graph->device);
     char* base = static_cast<char*>(ws->paths.ptr);
-    BFX_CUDA(cudaMemcpyAsync(base + o_tb, tbase.data(), (batch_count + 1) * 4, cudaMemcpyHostToDevice, ws->stream));
-    BFX_CUDA(cudaMemsetAsync(base + o_op, 0, (size_t{max_union} / 32 + 1) * 4, ws->stream));
-    bfx::PathArgs a{};
-    a.g = ws->graph->g;
-    a.batches = ws->params.batches;
-    a.status = ws->d_status;
-    a.first_batch = first_batch;
-    a.batch_count = batch_count;
-    a.target_base = reinterpret_cast<const std::uint32_t*>(base + o_tb);
-    a.summaries = reinterpret_cast<bfx_compact_target_summary*>(base + o_sum);
-    a.lengths = reinterpret_cast<std::uint32_t*>(base + o_len);
-    a.vertex_offsets = reinterpret_cast<const std::uint64_t*>(base + o_vo);
-    a.edge_offsets = reinterpret_cast<const std::uint64_t*>(base + o_eo);
-    a.stack_v = reinterpret_cast<std::uint32_t*>(base + o_sv);
-    a.stack_c = reinterpret_cast<std::uint32_t*>(base + o_sc);
-    a.stack_e = reinterpret_cast<std::uint32_t*>(base + o_se);
-    a.on_path = reinterpret_cast<std::uint32_t*>(base + o_op);
-    a.max_union = max_union;
+    BFX_CUDA(cudaMemcpyAsync(base + L.o_tb, tbase.data(), (batch_count + 1) * 4, cudaMemcpyHostToDevice, ws->stream));
+    // every slot's on-path bitmap starts clear (a search leaves it clear)
+    BFX_CUDA(cudaMemsetAsync(base + L.o_op, 0, size_t{L.slots} * L.mark_stride * 4, ws->stream));
+    BFX_CUDA(cudaMemsetAsync(base + L.o_fc, 0, 4, ws->stream));
+    const bfx::PathArgs a = bfx::path_args_at(ws, L, first_batch, batch_count, max_union);
     if (T > 0) {
       const int blocks = static_cast<int>(std::min<std::uint64_t>((T + 255) / 256, 4096));
       bfx::summaries_kernel<<<blocks, 256, 0, ws->stream>>>(a);
       BFX_CUDA(cudaGetLastError());
-      bfx::search_kernel<<<1, 1, 0, ws->stream>>>(a, false);
+      bfx::flag_list_kernel<<<blocks, 256, 0, ws->stream>>>(a);
+      BFX_CUDA(cudaGetLastError());
+      bfx::search_kernel<<<(a.slots + 31) / 32, 32, 0, ws->stream>>>(a, false);
       BFX_CUDA(cudaGetLastError());
     }
     ws->paths_host.reserve(T * sizeof(bfx_compact_target_summary) + 256);
@@ -522,8 +573,8 @@ int bfx_compact_path_summaries(bfx_workspace* ws, uint32_t first_batch, uint32_t
         ne += summaries[i].path_length;
       }
     }
-    BFX_CUDA(cudaMemcpyAsync(base + o_vo, vo.data(), T * 8, cudaMemcpyHostToDevice, ws->stream));
-    BFX_CUDA(cudaMemcpyAsync(base + o_eo, eo.data(), T * 8, cudaMemcpyHostToDevice, ws->stream));
+    BFX_CUDA(cudaMemcpyAsync(base + L.o_vo, vo.data(), T * 8, cudaMemcpyHostToDevice, ws->stream));
+    BFX_CUDA(cudaMemcpyAsync(base + L.o_eo, eo.data(), T * 8, cudaMemcpyHostToDevice, ws->stream));
     BFX_CUDA(cudaStreamSynchronize(ws->stream));
     ws->path_first_batch = first_batch;
     ws->path_batch_count = batch_count;
@@ -546,49 +597,21 @@ int bfx_compact_path_payload(bfx_workspace* ws, uint32_t* vertices, float* dista
     bfx::require(vertices && distance_labels && (edge_ids || ws->path_edges == 0), "null output");
     BFX_CUDA(cudaSetDevice(ws->graph->device));
     const std::uint64_t T = ws->path_targets, nv = ws->path_vertices, ne = ws->path_edges;
-    const std::uint32_t batch_count = ws->path_batch_count;
-    std::uint32_t max_union = 0;
-    for (std::uint32_t i = 0; i < batch_count; ++i) max_union = std::max(max_union, ws->batches[ws->path_first_batch + i].U);
-    char* base = static_cast<char*>(ws->paths.ptr);
-    const size_t o_tb = 0;
-    const size_t o_sum = bfx::align256(o_tb + (batch_count + 1) * 4);
-    const size_t o_len = bfx::align256(o_sum + T * sizeof(bfx_compact_target_summary));
-    const size_t o_vo = bfx::align256(o_len + T * 4);
-    const size_t o_eo = bfx::align256(o_vo + T * 8);
-    const size_t o_sv = bfx::align256(o_eo + T * 8);
-    const size_t o_sc = bfx::align256(o_sv + (size_t{max_union} + 1) * 4);
-    const size_t o_se = bfx::align256(o_sc + (size_t{max_union} + 1) * 4);
-    const size_t o_op = bfx::align256(o_se + (size_t{max_union} + 1) * 4);
     // Output arena: vertices, labels, edges in one device allocation.
     const size_t out_bytes = bfx::align256(nv * 4) * 2 + bfx::align256(ne * 4 + 4);
     char* dout = nullptr;
     BFX_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&dout), out_bytes, ws->stream));
-    bfx::PathArgs a{};
-    a.g = ws->graph->g;
-    a.batches = ws->params.batches;
-    a.status = ws->d_status;
-    a.first_batch = ws->path_first_batch;
-    a.batch_count = batch_count;
-    a.target_base = reinterpret_cast<const std::uint32_t*>(base + o_tb);
-    a.summaries = reinterpret_cast<bfx_compact_target_summary*>(base + o_sum);
-    a.lengths = reinterpret_cast<std::uint32_t*>(base + o_len);
-    a.vertex_offsets = reinterpret_cast<const std::uint64_t*>(base + o_vo);
-    a.edge_offsets = reinterpret_cast<const std::uint64_t*>(base + o_eo);
+    bfx::PathArgs a = bfx::path_args(ws);
     a.out_vertices = reinterpret_cast<std::uint32_t*>(dout);
     a.out_labels = reinterpret_cast<float*>(dout + bfx::align256(nv * 4));
     a.out_edges = reinterpret_cast<std::uint32_t*>(dout + 2 * bfx::align256(nv * 4));
-    a.stack_v = reinterpret_cast<std::uint32_t*>(base + o_sv);
-    a.stack_c = reinterpret_cast<std::uint32_t*>(base + o_sc);
-    a.stack_e = reinterpret_cast<std::uint32_t*>(base + o_se);
-    a.on_path = reinterpret_cast<std::uint32_t*>(base + o_op);
-    a.max_union = max_union;
     cudaError_t err = cudaSuccess;
     if (T > 0) {
       const int blocks = static_cast<int>(std::min<std::uint64_t>((T + 255) / 256, 4096));
       bfx::payload_kernel<<<blocks, 256, 0, ws->stream>>>(a);
       err = cudaGetLastError();
       if (err == cudaSuccess) {
-        bfx::search_kernel<<<1, 1, 0, ws->stream>>>(a, true);
+        bfx::search_kernel<<<(a.slots + 31) / 32, 32, 0, ws->stream>>>(a, true);
         err = cudaGetLastError();
       }
     }
@@ -635,7 +658,7 @@ extern "C" int bfx_edge_usage_adjoint(bfx_workspace* ws, const float* target_gra
       const int blocks = static_cast<int>(std::min<std::uint64_t>((T + 255) / 256, 4096));
       bfx::adjoint_walk_kernel<<<blocks, 256, 0, ws->stream>>>(a, g, acc);
       BFX_CUDA(cudaGetLastError());
-      bfx::adjoint_search_kernel<<<1, 1, 0, ws->stream>>>(a, g, acc);
+      bfx::adjoint_search_kernel<<<(a.slots + 31) / 32, 32, 0, ws->stream>>>(a, g, acc);
       BFX_CUDA(cudaGetLastError());
     }
     bfx::adjoint_round_kernel<<<std::max(1, std::min<int>((E + 255) / 256, 8192)), 256, 0, ws->stream>>>(E, acc, out);

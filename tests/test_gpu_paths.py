@@ -101,3 +101,22 @@ def test_round_limited_lanes_report_terminal_failure(gpu):
     assert all(p["reconstruction"] == 2 and p["reached"] == 0 for p in paths)
     ws.close()
     res.close()
+
+
+def test_many_backtracking_targets_searched_in_parallel(gpu):
+    """Forty copies of the zero-weight-cycle query (lanes of five width-8
+    batches) hand forty targets to the backtracking search at once; the
+    searches run one per thread over the search slots, each with its own
+    stacks and marks, and every path equals the reference's."""
+    case = load_case(GOLDEN / "compact_paths.npz")
+    gq = case.queries[0]
+    descs = [bfx.make_description(case.layout, [gq.query] * 8, 8) for _ in range(5)]
+    _, paths = run_paths(case.layout, descs)
+    st, verts, edges = gq.paths()[0]
+    per_query = len(gq.query.targets)
+    assert len(paths) == 40 * per_query
+    for k in range(40):
+        p = paths[k * per_query]
+        assert p["reconstruction"] == st == 0
+        np.testing.assert_array_equal(p["vertices"], verts)
+        np.testing.assert_array_equal(p["edges"], edges)
