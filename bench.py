@@ -407,9 +407,22 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
         all_statuses = replicas.gather_statuses(dist, statuses)
         assert all(s.stop_reason == bfx.STOP_CONVERGED for part in all_statuses for s in part)
 
-    # ---- end-to-end timing through the C ABI from host buffers (e2e)
+    # ---- end-to-end timing through the C ABI from host buffers (e2e): each
+    # step prepares the set (host descriptions, or on the device from the
+    # lane -> query assignment), relaxes it and fetches the statuses
+    lanes = [(d.lane_width, [int(x) for x in d.query_index_by_lane[:bin(d.valid_lane_mask).count("1")]])
+             for d in descs]
+
+    def prepare():
+        if args.prepare == "device":
+            ws.prepare_from_queries(lanes, wl.queries)
+        else:
+            ws.prepare(descs)
+        if engines_chosen is None and args.step is not None:
+            ws.set_batch_deltas(deltas)
+
     for _ in range(warmup):
-        ws.prepare(descs)
+        prepare()
         ws.execute(opts)
         ws.fetch_statuses()
     barrier()
@@ -417,7 +430,7 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
     e2 = torch.cuda.Event(enable_timing=True)
     s2.record(stream)
     for _ in range(steps):
-        ws.prepare(descs)
+        prepare()
         ws.execute(opts)
         ws.fetch_statuses()
     e2.record(stream)
@@ -502,7 +515,8 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
         "gteps": lane_edges * (1 if shard else world) / (ms_per_step / 1000) / 1e9,
         "reached_lanes": reached,
         "max_finite_distance": max_distance,
-        "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "prepare": args.prepare},
         "host": {"plan_s": plan_s, "tune_s": tune_s,
                  "note": "host planner (batch grouping + descriptions) and autotuner run once per query set, "
                          "before both timed regions"},
@@ -559,6 +573,9 @@ def main():
                     help="with --engine frontier: near/far threshold step in mean edge weights (0 = plain frontier)")
     ap.add_argument("--tune-policy", action="store_true",
                     help="choose the planner policy by timing each candidate's plan (bfx_autotune_policy)")
+    ap.add_argument("--prepare", default="device", choices=["host", "device"],
+                    help="e2e steps prepare the batch set from host descriptions or on the device from the "
+                         "lane -> query assignment")
     ap.add_argument("--stage-min", type=int, default=None,
                     help="tiled layout: lane-edge work from which a tile visit stages its labels")
     ap.add_argument("--shard", action="store_true",

@@ -127,6 +127,10 @@ class RouteQueryC(C.Structure):
                 ("selected_tiles", P(u32))]
 
 
+class BatchLanesC(C.Structure):
+    _fields_ = [("lane_width", u32), ("lane_count", u32), ("query_index_by_lane", P(u32))]
+
+
 class PlannerPolicyC(C.Structure):
     _fields_ = [("lane_width", u32), ("minimum_jaccard_numerator", u32), ("minimum_jaccard_denominator", u32),
                 ("maximum_union_inflation_numerator", u32), ("maximum_union_inflation_denominator", u32),
@@ -535,6 +539,32 @@ class Workspace:
         self._keep = batches
         _check(load().bfx_prepare_batches(self._h, u32(len(batches)), arr))
         self.batch_count = len(batches)
+
+    def prepare_from_queries(self, lanes: Sequence[tuple[int, Sequence[int]]], queries: Sequence["RouteQuery"]):
+        """bfx_prepare_batches_from_queries: batches given as (lane width, query
+        indices of the valid lanes); descriptions are built on the device."""
+        qc = (RouteQueryC * len(queries))(*[q.c() for q in queries])
+        idx = [np.ascontiguousarray(np.asarray(ix, np.uint32)) for _, ix in lanes]
+        bc = (BatchLanesC * len(lanes))(*[BatchLanesC(w, len(ix), _ptr(a)) for (w, ix), a in zip(lanes, idx)])
+        self._keep = (qc, idx, list(queries))
+        _check(load().bfx_prepare_batches_from_queries(self._h, u32(len(lanes)), bc, u32(len(queries)), qc))
+        self.batch_count = len(lanes)
+
+    def prepared_description(self, batch: int) -> "BatchDescription":
+        """The prepared description of a batch, read back from the device."""
+        lib = load()
+        counts = (u32 * 5)()
+        _check(lib.bfx_fetch_prepared_description(self._h, u32(batch), counts, None, None, None, None, None, None,
+                                                  None))
+        W, valid, S, Tg, R = (int(x) for x in counts)
+        T = self.graph.layout.tile_count
+        so, to = np.zeros(W + 1, np.uint32), np.zeros(W + 1, np.uint32)
+        sv, tv = np.zeros(max(S, 1), np.uint32), np.zeros(max(Tg, 1), np.uint32)
+        ut, tm = np.zeros(max(R, 1), np.uint32), np.zeros(T, np.uint32)
+        rg = np.zeros(3 * max(R, 1), np.uint32)
+        _check(lib.bfx_fetch_prepared_description(self._h, u32(batch), counts, _ptr(so), _ptr(sv), _ptr(to), _ptr(tv),
+                                                  _ptr(ut), _ptr(tm), C.cast(_ptr(rg), P(BatchVertexRange))))
+        return BatchDescription(W, valid, so, sv[:S], to, tv[:Tg], ut[:R], tm, rg[:3 * R])
 
     def execute(self, options: GpuRunOptions):
         _check(load().bfx_execute(self._h, C.byref(options)))

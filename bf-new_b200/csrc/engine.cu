@@ -30,6 +30,7 @@
 //     launch with a grid barrier whose waits time out; host-poll modes run
 //     CUDA-graph-captured chunks of rounds.
 #include "bfx.h"
+#include "bfx_host.h"
 #include "bfx_internal.hpp"
 #include "device_common.cuh"
 #include "engine_types.cuh"
@@ -814,6 +815,181 @@ __global__ void label_bound_kernel(LaunchParams p, const bfx_device_run_status* 
 }
 
 // ---------------------------------------------------------------------------
+// Device-side batch description preparation (bfx_prepare_batches_from_queries):
+// the per-batch image prepare_batch_device_description builds on the host
+// (src/batch_layout.cpp:1056-1296) -- dense tile lane masks, one vertex range
+// per union tile with its compact offset, lane terminal slices -- built from
+// the batches' lane -> query assignment and the queries' selected tiles and
+// terminals.
+// ---------------------------------------------------------------------------
+
+// The uploaded query and lane image.  Per query q: tiles [tile_off[q],
+// tile_off[q+1]), sources and targets likewise; per batch b: lanes
+// [lane_base[b], lane_base[b+1]) with their query indices; per lane its
+// first entry in the flattened (lane, tile) list.
+struct QueryImage {
+  const u32* tile_off;
+  const u32* tiles;
+  const u32* src_off;
+  const u32* srcs;
+  const u32* tgt_off;
+  const u32* tgts;
+  const u32* lane_base;      // [nb+1]
+  const u32* lane_query;     // [lanes]
+  const u32* lane_tile_base; // [lanes+1]
+  u32 nb, lanes;
+};
+
+// Scatter: every (lane, selected tile) ORs the lane's bit into its batch's
+// dense tile mask.
+__global__ void desc_mask_kernel(QueryImage q, uint2* tiles, u64 tstride) {
+  const u32 total = q.lane_tile_base[q.lanes];
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const u32 lane_g = find_batch(q.lane_tile_base, q.lanes, i);
+    const u32 b = find_batch(q.lane_base, q.nb, lane_g);
+    const u32 lane = lane_g - q.lane_base[b];
+    const u32 qi = q.lane_query[lane_g];
+    const u32 t = q.tiles[q.tile_off[qi] + (i - q.lane_tile_base[lane_g])];
+    atomicOr(&tiles[b * tstride + t].x, 1u << lane);
+  }
+}
+
+// One block per batch: union tile count, union vertex count, and the count
+// of union tiles whose mask is not every valid lane (0 with R == T: a
+// full-graph batch).  out[4b..4b+3] = {R, U, partial tiles, 0}.
+__global__ void desc_count_kernel(const u32* tile_off, u32 T, const uint2* tiles, u64 tstride, const u32* valid,
+                                  u32* out) {
+  __shared__ u32 s_acc[3];
+  const u32 b = blockIdx.x;
+  if (threadIdx.x == 0u) s_acc[0] = s_acc[1] = s_acc[2] = 0u;
+  __syncthreads();
+  u32 r = 0u, u = 0u, partial = 0u;
+  for (u32 t = threadIdx.x; t < T; t += blockDim.x) {
+    const u32 m = tiles[b * tstride + t].x;
+    if (m != 0u) {
+      ++r;
+      u += tile_off[t + 1] - tile_off[t];
+      partial += m != valid[b];
+    }
+  }
+  r = __reduce_add_sync(0xFFFFFFFFu, r);
+  u = __reduce_add_sync(0xFFFFFFFFu, u);
+  partial = __reduce_add_sync(0xFFFFFFFFu, partial);
+  if (lane_id() == 0u) {
+    atomicAdd(&s_acc[0], r);
+    atomicAdd(&s_acc[1], u);
+    atomicAdd(&s_acc[2], partial);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0u) {
+    out[4u * b] = s_acc[0];
+    out[4u * b + 1u] = s_acc[1];
+    out[4u * b + 2u] = s_acc[2];
+    out[4u * b + 3u] = 0u;
+  }
+}
+
+// One block per batch: union tiles in increasing order with their vertex
+// ranges, compact offsets and the tile table's compact biases (block scans
+// over the tile ids), then the lane terminal slices; a terminal whose owner
+// tile is not selected for its lane sets *error.
+__global__ void desc_fill_kernel(QueryImage q, const u32* owner, const u32* tile_off, u32 T, uint2* tiles,
+                                 u64 tstride, const DBatch* batches, u32* error) {
+  __shared__ u32 s_f[32], s_v[32], s_tot[2];
+  __shared__ u32 s_carry[2];
+  const u32 b = blockIdx.x;
+  const DBatch& B = batches[b];
+  uint4* ranges = const_cast<uint4*>(B.ranges);
+  u32* roff = const_cast<u32*>(B.range_off);
+  uint2* tb = tiles + b * tstride;
+  if (threadIdx.x == 0u) s_carry[0] = s_carry[1] = 0u;
+  __syncthreads();
+  const u32 nw = blockDim.x >> 5, wib = threadIdx.x >> 5, lane = lane_id();
+  for (u32 base = 0; base < T; base += blockDim.x) {
+    const u32 t = base + threadIdx.x;
+    const u32 m = t < T ? tb[t].x : 0u;
+    const u32 size = m != 0u ? tile_off[t + 1] - tile_off[t] : 0u;
+    // block exclusive scans of (union flag, union vertices)
+    u32 f = m != 0u ? 1u : 0u, v = size;
+    for (u32 o = 1; o < 32u; o <<= 1) {
+      const u32 yf = __shfl_up_sync(0xFFFFFFFFu, f, o);
+      const u32 yv = __shfl_up_sync(0xFFFFFFFFu, v, o);
+      if (lane >= o) {
+        f += yf;
+        v += yv;
+      }
+    }
+    if (lane == 31u) {
+      s_f[wib] = f;
+      s_v[wib] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0u) {
+      u32 af = 0u, av = 0u;
+      for (u32 w = 0; w < nw; ++w) {
+        const u32 xf = s_f[w], xv = s_v[w];
+        s_f[w] = af;
+        s_v[w] = av;
+        af += xf;
+        av += xv;
+      }
+      s_tot[0] = af;  // this chunk's union tiles and vertices
+      s_tot[1] = av;
+    }
+    __syncthreads();
+    const u32 idx = s_carry[0] + s_f[wib] + f - (m != 0u ? 1u : 0u);
+    const u32 off = s_carry[1] + s_v[wib] + v - size;
+    if (m != 0u) {
+      ranges[idx] = make_uint4(t, tile_off[t], tile_off[t + 1], m);
+      roff[idx] = off;
+      tb[t].y = tile_off[t] - off;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0u) {
+      s_carry[0] += s_tot[0];
+      s_carry[1] += s_tot[1];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0u) roff[B.range_count] = s_carry[1];
+  // terminal slices: lanes in order, invalid lanes empty
+  u32* so = const_cast<u32*>(B.src_off);
+  u32* src = const_cast<u32*>(B.src);
+  u32* to = const_cast<u32*>(B.tgt_off);
+  u32* tgt = const_cast<u32*>(B.tgt);
+  const u32 lanes = q.lane_base[b + 1] - q.lane_base[b];
+  if (threadIdx.x == 0u) {
+    u32 ns = 0u, nt = 0u;
+    so[0] = to[0] = 0u;
+    for (u32 l = 0; l < B.W; ++l) {
+      if (l < lanes) {
+        const u32 qi = q.lane_query[q.lane_base[b] + l];
+        ns += q.src_off[qi + 1] - q.src_off[qi];
+        nt += q.tgt_off[qi + 1] - q.tgt_off[qi];
+      }
+      so[l + 1] = ns;
+      to[l + 1] = nt;
+    }
+  }
+  __syncthreads();
+  for (u32 l = wib; l < lanes; l += nw) {
+    const u32 qi = q.lane_query[q.lane_base[b] + l];
+    const u32 s0 = q.src_off[qi], s1 = q.src_off[qi + 1], t0 = q.tgt_off[qi], t1 = q.tgt_off[qi + 1];
+    const u32 sb = so[l], tb0 = to[l];
+    for (u32 k = lane; k < s1 - s0; k += 32u) {
+      const u32 v = q.srcs[s0 + k];
+      src[sb + k] = v;
+      if (((tb[owner[v]].x >> l) & 1u) == 0u) atomicOr(error, 1u);
+    }
+    for (u32 k = lane; k < t1 - t0; k += 32u) {
+      const u32 v = q.tgts[t0 + k];
+      tgt[tb0 + k] = v;
+      if (((tb[owner[v]].x >> l) & 1u) == 0u) atomicOr(error, 1u);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 }  // namespace bfx
 
 namespace bfx {
@@ -956,7 +1132,8 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
     const size_t o_csc = bfx::align256(o_csr + size_t{E} * 16);
     const size_t o_eid_src = bfx::align256(o_csc + size_t{E} * 16);
     const size_t o_lrun = bfx::align256(o_eid_src + size_t{E} * 4);
-    const size_t total = bfx::align256(o_lrun + size_t{V} * 8);
+    const size_t o_toff = bfx::align256(o_lrun + size_t{V} * 8);
+    const size_t total = bfx::align256(o_toff + (size_t{T} + 1) * 4);
     G->mem.reserve(total, device);
     char* base = static_cast<char*>(G->mem.ptr);
     BFX_CUDA(cudaMemcpy(base + o_owner, L.owner_tiles, size_t{V} * 4, cudaMemcpyHostToDevice));
@@ -966,6 +1143,7 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
     BFX_CUDA(cudaMemcpy(base + o_csc, csc.data(), size_t{E} * 16, cudaMemcpyHostToDevice));
     BFX_CUDA(cudaMemcpy(base + o_eid_src, eid_src.data(), size_t{E} * 4, cudaMemcpyHostToDevice));
     BFX_CUDA(cudaMemcpy(base + o_lrun, lrun.data(), size_t{V} * 8, cudaMemcpyHostToDevice));
+    BFX_CUDA(cudaMemcpy(base + o_toff, G->tile_vertex_offsets.data(), (size_t{T} + 1) * 4, cudaMemcpyHostToDevice));
     double wsum = 0.0;
     for (std::uint32_t e = 0; e < E; ++e) wsum += L.csr_weights[e];
     G->mean_weight = E ? wsum / E : 0.0;
@@ -979,6 +1157,7 @@ int bfx_resident_graph_upload(const bfx_device_graph_layout32* layout, int devic
     G->g.csc = reinterpret_cast<const uint4*>(base + o_csc);
     G->g.eid_src = reinterpret_cast<const std::uint32_t*>(base + o_eid_src);
     G->g.lrun = reinterpret_cast<const uint2*>(base + o_lrun);
+    G->g.tile_off = reinterpret_cast<const std::uint32_t*>(base + o_toff);
     G->bytes = total;
     {
       const std::uint32_t size0 = G->tile_vertex_offsets[1] - G->tile_vertex_offsets[0];
@@ -1058,9 +1237,173 @@ int bfx_workspace_stream(bfx_workspace* ws, void** stream) {
 int bfx_workspace_bytes(bfx_workspace* ws, uint64_t* bytes) {
   return bfx::guarded([&] {
     bfx::require(ws && bytes, "null argument");
-    *bytes = ws->meta.bytes + ws->arena.bytes;
+    *bytes = ws->meta.bytes + ws->arena.bytes + ws->tile_tables.bytes + ws->qimage.bytes;
   });
 }
+
+}  // extern "C"
+
+namespace bfx {
+namespace {
+
+// Per-batch sizes of a prepared set.
+struct BatchSizes {
+  u32 U, R, S, Tg, W, shift, valid, full;
+};
+
+// Where a batch's description arrays sit in the metadata block.
+struct DescArrays {
+  size_t src_off, src, tgt_off, tgt, ranges, range_off;
+};
+
+// Lays out a prepared set: the metadata block (batch records, controllers,
+// launch state, unit and source prefixes, statuses, controllers, then each
+// batch's description arrays), the arena (per-batch labels -- two slots, so
+// one prepare serves every engine -- pending masks, queues, compact map, far
+// pile state, chunk bitmaps, row tables) and the tile tables (one dense
+// {lane mask, compact bias} table per batch).  Fills ws->batches with device
+// pointers, the staging header (records, prefixes) and the launch
+// parameters; the caller writes the description arrays and uploads.
+struct Layout {
+  size_t o_up, meta_total;
+  std::vector<DescArrays> arrays;
+};
+
+Layout lay_out_batches(bfx_workspace* ws, std::uint32_t count, const std::vector<BatchSizes>& sz) {
+  const DGraph& g = ws->graph->g;
+  const size_t o_batch = 0;
+  const size_t o_ctl = align256(o_batch + count * sizeof(DBatch));
+  const size_t o_run = align256(o_ctl + count * sizeof(DCtl));
+  const size_t o_ubase = align256(o_run + sizeof(DRun));
+  const size_t o_sbase = align256(o_ubase + (count + 1) * 4);
+  const size_t o_status = align256(o_sbase + (count + 1) * 4);
+  const size_t o_ctrl = align256(o_status + count * sizeof(bfx_device_run_status));
+  Layout L;
+  L.o_up = align256(o_ctrl + count * sizeof(bfx_device_controller));
+  L.arrays.resize(count);
+  size_t up = L.o_up;
+  for (std::uint32_t b = 0; b < count; ++b) {
+    const BatchSizes& s = sz[b];
+    DescArrays& a = L.arrays[b];
+    a.src_off = up;
+    up += align256((s.W + 1) * 4);
+    a.src = up;
+    up += align256(size_t{s.S} * 4);
+    a.tgt_off = up;
+    up += align256((s.W + 1) * 4);
+    a.tgt = up;
+    up += align256(size_t{s.Tg} * 4);
+    a.ranges = up;
+    up += align256(size_t{s.R} * 16);
+    a.range_off = up;
+    up += align256((size_t{s.R} + 1) * 4);
+  }
+  L.meta_total = up;
+  std::vector<size_t> arena_off(count);
+  size_t arena_total = 0;
+  for (std::uint32_t b = 0; b < count; ++b) {
+    arena_off[b] = arena_total;
+    const size_t U = sz[b].U;
+    arena_total += align256(U * sz[b].W * 8) * 2 + align256(U * 4) * 5 + align256(U * 8) * 7 +
+                   align256((U + 1023) / 1024 * 4) * 2;
+  }
+  const size_t tile_table_bytes = align256(size_t{g.T} * 8);
+  const bool grew = L.meta_total > ws->meta.bytes || arena_total > ws->arena.bytes ||
+                    tile_table_bytes * count > ws->tile_tables.bytes;
+  ws->meta.reserve(L.meta_total, ws->graph->device);
+  ws->arena.reserve(arena_total, ws->graph->device);
+  ws->tile_tables.reserve(tile_table_bytes * count, ws->graph->device);
+  if (grew) ++ws->generation;
+  ws->staging.reserve(L.meta_total);
+  char* hb = static_cast<char*>(ws->staging.ptr);
+  char* db = static_cast<char*>(ws->meta.ptr);
+  char* ab = static_cast<char*>(ws->arena.ptr);
+  char* tb = static_cast<char*>(ws->tile_tables.ptr);
+  std::memset(hb, 0, L.o_up);
+  ws->batches.assign(count, DBatch{});
+  std::uint32_t* ubase = reinterpret_cast<std::uint32_t*>(hb + o_ubase);
+  std::uint32_t* sbase = reinterpret_cast<std::uint32_t*>(hb + o_sbase);
+  std::uint64_t usum = 0, ssum = 0;
+  for (std::uint32_t b = 0; b < count; ++b) {
+    const BatchSizes& s = sz[b];
+    const DescArrays& da = L.arrays[b];
+    DBatch& B = ws->batches[b];
+    B.W = s.W;
+    B.shift = s.shift;
+    B.valid = s.valid;
+    B.U = s.U;
+    B.src_count = s.S;
+    B.tgt_count = s.Tg;
+    B.range_count = s.R;
+    B.full = s.full;
+    B.src_off = reinterpret_cast<const std::uint32_t*>(db + da.src_off);
+    B.src = reinterpret_cast<const std::uint32_t*>(db + da.src);
+    B.tgt_off = reinterpret_cast<const std::uint32_t*>(db + da.tgt_off);
+    B.tgt = reinterpret_cast<const std::uint32_t*>(db + da.tgt);
+    B.ranges = reinterpret_cast<const uint4*>(db + da.ranges);
+    B.range_off = reinterpret_cast<const std::uint32_t*>(db + da.range_off);
+    char* a = ab + arena_off[b];
+    const size_t U = s.U;
+    B.dist[0] = reinterpret_cast<u64*>(a);
+    a += align256(U * s.W * 8);
+    B.dist[1] = reinterpret_cast<u64*>(a);
+    a += align256(U * s.W * 8);
+    B.mask[0] = reinterpret_cast<std::uint32_t*>(a);
+    a += align256(U * 4);
+    B.mask[1] = reinterpret_cast<std::uint32_t*>(a);
+    a += align256(U * 4);
+    B.queue[0] = reinterpret_cast<u64*>(a);
+    a += align256(U * 8);
+    B.queue[1] = reinterpret_cast<u64*>(a);
+    a += align256(U * 8);
+    B.c2g = reinterpret_cast<std::uint32_t*>(a);
+    a += align256(U * 4);
+    B.fmask = reinterpret_cast<std::uint32_t*>(a);
+    a += align256(U * 4);
+    B.fbound = reinterpret_cast<std::uint32_t*>(a);
+    a += align256(U * 4);
+    for (int k = 0; k < 3; ++k) {
+      B.fpile[k] = reinterpret_cast<u64*>(a);
+      a += align256(U * 8);
+    }
+    for (int k = 0; k < 2; ++k) {
+      B.cmask[k] = reinterpret_cast<std::uint32_t*>(a);
+      a += align256((U + 1023) / 1024 * 4);
+    }
+    B.crow = reinterpret_cast<uint2*>(a);
+    a += align256(U * 8);
+    B.clrun = reinterpret_cast<uint2*>(a);
+    a += align256(U * 8);
+    B.tiles = reinterpret_cast<uint2*>(tb + tile_table_bytes * b);
+    ubase[b] = static_cast<std::uint32_t>(usum);
+    sbase[b] = static_cast<std::uint32_t>(ssum);
+    usum += U;
+    ssum += s.S;
+    if (usum > 0xFFFFFFFFull) throw std::overflow_error("total union vertices exceed 32 bits");
+  }
+  ubase[count] = static_cast<std::uint32_t>(usum);
+  sbase[count] = static_cast<std::uint32_t>(ssum);
+  std::memcpy(hb + o_batch, ws->batches.data(), count * sizeof(DBatch));
+  ws->nb = count;
+  ws->src_total = ssum;
+  ws->params = LaunchParams{};
+  ws->params.g = g;
+  ws->params.batches = reinterpret_cast<const DBatch*>(db + o_batch);
+  ws->params.ctl = reinterpret_cast<DCtl*>(db + o_ctl);
+  ws->params.run = reinterpret_cast<DRun*>(db + o_run);
+  ws->params.unit_base = reinterpret_cast<const std::uint32_t*>(db + o_ubase);
+  ws->params.nb = count;
+  ws->src_base = reinterpret_cast<u32*>(db + o_sbase);
+  ws->d_status = reinterpret_cast<bfx_device_run_status*>(db + o_status);
+  ws->d_ctrl = reinterpret_cast<bfx_device_controller*>(db + o_ctrl);
+  ws->executed = false;
+  return L;
+}
+
+}  // namespace
+}  // namespace bfx
+
+extern "C" {
 
 int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_description* batches) {
   return bfx::guarded([&] {
@@ -1072,11 +1415,7 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
     const auto& tvo = ws->graph->tile_vertex_offsets;
     // Validate descriptions (validate_batch_device_description,
     // include/bfnew/batch_layout.hpp:176-199) and size everything.
-    struct Sizes {
-      std::uint32_t U, R, S, Tg, W, shift;
-    };
-    std::vector<Sizes> sz(count);
-    size_t up_bytes = 0;
+    std::vector<bfx::BatchSizes> sz(count);
     for (std::uint32_t b = 0; b < count; ++b) {
       const bfx_batch_description& d = batches[b];
       const std::uint32_t W = d.lane_width;
@@ -1122,9 +1461,14 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
           if (d.targets[i] >= g.V) throw std::out_of_range("target out of range");
         }
       }
-      sz[b] = Sizes{static_cast<std::uint32_t>(U), d.range_count, S, Tg, W, static_cast<std::uint32_t>(__builtin_ctz(W))};
-      up_bytes += bfx::align256((W + 1) * 4) * 2 + bfx::align256(size_t{S} * 4) + bfx::align256(size_t{Tg} * 4) +
-                  bfx::align256(size_t{d.range_count} * 16) + bfx::align256((size_t{d.range_count} + 1) * 4);
+      // Full-graph batch: every tile in order, each selected by every valid
+      // lane -- the frontier then needs no tile-table lookup per edge.
+      bool full = d.range_count == g.T;
+      for (std::uint32_t i = 0; full && i < d.range_count; ++i) {
+        full = d.union_tiles[i] == i && d.selected_vertex_ranges[i].lane_mask == d.valid_lane_mask;
+      }
+      sz[b] = bfx::BatchSizes{static_cast<std::uint32_t>(U), d.range_count, S, Tg, W,
+                              static_cast<std::uint32_t>(__builtin_ctz(W)), d.valid_lane_mask, full ? 1u : 0u};
     }
     // Terminal ownership: a terminal's owner tile must be selected for its
     // lane (terminal_owner_tile_not_selected, src/query.cpp:221-236).
@@ -1144,144 +1488,225 @@ int bfx_prepare_batches(bfx_workspace* ws, uint32_t count, const bfx_batch_descr
         }
       }
     }
-    // Metadata block: DBatch[nb], DCtl[nb], DRun, unit_base[nb+1], src_base[nb+1],
-    // statuses, controllers, then uploaded description arrays.
-    const size_t o_batch = 0;
-    const size_t o_ctl = bfx::align256(o_batch + count * sizeof(bfx::DBatch));
-    const size_t o_run = bfx::align256(o_ctl + count * sizeof(bfx::DCtl));
-    const size_t o_ubase = bfx::align256(o_run + sizeof(bfx::DRun));
-    const size_t o_sbase = bfx::align256(o_ubase + (count + 1) * 4);
-    const size_t o_status = bfx::align256(o_sbase + (count + 1) * 4);
-    const size_t o_ctrl = bfx::align256(o_status + count * sizeof(bfx_device_run_status));
-    const size_t o_up = bfx::align256(o_ctrl + count * sizeof(bfx_device_controller));
-    const size_t meta_total = o_up + up_bytes;
-    // Arena: per batch labels (2 slots reserved so one prepare serves every
-    // engine), masks, queues, c2g; then the tile tables of all batches in one
-    // contiguous block, cleared by a single memset.
-    std::vector<size_t> arena_off(count);
-    size_t arena_total = 0;
-    for (std::uint32_t b = 0; b < count; ++b) {
-      arena_off[b] = arena_total;
-      const size_t U = sz[b].U;
-      arena_total += bfx::align256(U * sz[b].W * 8) * 2 + bfx::align256(U * 4) * 5 + bfx::align256(U * 8) * 7 +
-                     bfx::align256((U + 1023) / 1024 * 4) * 2;
-    }
-    const size_t tiles_off = arena_total;
-    const size_t tile_table_bytes = bfx::align256(size_t{g.T} * 8);
-    arena_total += tile_table_bytes * count;
-    const bool grew = meta_total > ws->meta.bytes || arena_total > ws->arena.bytes;
-    ws->meta.reserve(meta_total, ws->graph->device);
-    ws->arena.reserve(arena_total, ws->graph->device);
-    if (grew) ++ws->generation;
-    ws->staging.reserve(meta_total);
+    const bfx::Layout L = bfx::lay_out_batches(ws, count, sz);
     char* hb = static_cast<char*>(ws->staging.ptr);
-    char* db = static_cast<char*>(ws->meta.ptr);
-    char* ab = static_cast<char*>(ws->arena.ptr);
-    std::memset(hb, 0, o_up);
-    ws->batches.assign(count, bfx::DBatch{});
-    std::uint32_t* ubase = reinterpret_cast<std::uint32_t*>(hb + o_ubase);
-    std::uint32_t* sbase = reinterpret_cast<std::uint32_t*>(hb + o_sbase);
-    size_t up = o_up;
-    std::uint64_t usum = 0, ssum = 0;
     for (std::uint32_t b = 0; b < count; ++b) {
       const bfx_batch_description& d = batches[b];
-      const Sizes& s = sz[b];
-      bfx::DBatch& B = ws->batches[b];
-      B.W = s.W;
-      B.shift = s.shift;
-      B.valid = d.valid_lane_mask;
-      B.U = s.U;
-      B.src_count = s.S;
-      B.tgt_count = s.Tg;
-      B.range_count = s.R;
-      auto put = [&](const void* src, size_t bytes) -> const void* {
-        std::memcpy(hb + up, src, bytes);
-        const void* dptr = db + up;
-        up += bfx::align256(bytes);
-        return dptr;
-      };
-      B.src_off = static_cast<const std::uint32_t*>(put(d.source_offsets, (s.W + 1) * 4));
-      B.src = static_cast<const std::uint32_t*>(put(d.sources, size_t{s.S} * 4));
-      B.tgt_off = static_cast<const std::uint32_t*>(put(d.target_offsets, (s.W + 1) * 4));
-      B.tgt = static_cast<const std::uint32_t*>(put(d.targets, size_t{s.Tg} * 4));
-      std::vector<uint4> ranges(s.R);
-      std::vector<std::uint32_t> roff(s.R + 1, 0U);
+      const bfx::BatchSizes& s = sz[b];
+      const bfx::DescArrays& a = L.arrays[b];
+      std::memcpy(hb + a.src_off, d.source_offsets, (s.W + 1) * 4);
+      if (s.S) std::memcpy(hb + a.src, d.sources, size_t{s.S} * 4);
+      std::memcpy(hb + a.tgt_off, d.target_offsets, (s.W + 1) * 4);
+      if (s.Tg) std::memcpy(hb + a.tgt, d.targets, size_t{s.Tg} * 4);
+      uint4* ranges = reinterpret_cast<uint4*>(hb + a.ranges);
+      std::uint32_t* roff = reinterpret_cast<std::uint32_t*>(hb + a.range_off);
+      roff[0] = 0;
       for (std::uint32_t i = 0; i < s.R; ++i) {
         const bfx_batch_vertex_range& r = d.selected_vertex_ranges[i];
         ranges[i] = make_uint4(d.union_tiles[i], r.begin, r.end, r.lane_mask);
         roff[i + 1] = roff[i] + (r.end - r.begin);
       }
-      // Full-graph batch: every tile in order, each selected by every valid
-      // lane -- the frontier then needs no tile-table lookup per edge.
-      bool full = s.R == g.T;
-      for (std::uint32_t i = 0; full && i < s.R; ++i) {
-        full = ranges[i].x == i && ranges[i].y == roff[i] && ranges[i].w == d.valid_lane_mask;
-      }
-      B.full = full ? 1u : 0u;
-      B.ranges = static_cast<const uint4*>(put(ranges.data(), size_t{s.R} * 16));
-      B.range_off = static_cast<const std::uint32_t*>(put(roff.data(), (size_t{s.R} + 1) * 4));
-      char* a = ab + arena_off[b];
-      const size_t U = s.U;
-      B.dist[0] = reinterpret_cast<bfx::u64*>(a);
-      a += bfx::align256(U * s.W * 8);
-      B.dist[1] = reinterpret_cast<bfx::u64*>(a);
-      a += bfx::align256(U * s.W * 8);
-      B.mask[0] = reinterpret_cast<std::uint32_t*>(a);
-      a += bfx::align256(U * 4);
-      B.mask[1] = reinterpret_cast<std::uint32_t*>(a);
-      a += bfx::align256(U * 4);
-      B.queue[0] = reinterpret_cast<bfx::u64*>(a);
-      a += bfx::align256(U * 8);
-      B.queue[1] = reinterpret_cast<bfx::u64*>(a);
-      a += bfx::align256(U * 8);
-      B.c2g = reinterpret_cast<std::uint32_t*>(a);
-      a += bfx::align256(U * 4);
-      B.fmask = reinterpret_cast<std::uint32_t*>(a);
-      a += bfx::align256(U * 4);
-      B.fbound = reinterpret_cast<std::uint32_t*>(a);
-      a += bfx::align256(U * 4);
-      for (int k = 0; k < 3; ++k) {
-        B.fpile[k] = reinterpret_cast<bfx::u64*>(a);
-        a += bfx::align256(U * 8);
-      }
-      for (int k = 0; k < 2; ++k) {
-        B.cmask[k] = reinterpret_cast<std::uint32_t*>(a);
-        a += bfx::align256((U + 1023) / 1024 * 4);
-      }
-      B.crow = reinterpret_cast<uint2*>(a);
-      a += bfx::align256(U * 8);
-      B.clrun = reinterpret_cast<uint2*>(a);
-      a += bfx::align256(U * 8);
-      B.tiles = reinterpret_cast<uint2*>(ab + tiles_off + tile_table_bytes * b);
-      ubase[b] = static_cast<std::uint32_t>(usum);
-      sbase[b] = static_cast<std::uint32_t>(ssum);
-      usum += U;
-      ssum += s.S;
-      if (usum > 0xFFFFFFFFull) throw std::overflow_error("total union vertices exceed 32 bits");
     }
-    ubase[count] = static_cast<std::uint32_t>(usum);
-    sbase[count] = static_cast<std::uint32_t>(ssum);
-    std::memcpy(hb + o_batch, ws->batches.data(), count * sizeof(bfx::DBatch));
-    bfx::upload(db, hb, meta_total, ws->stream);
-    ws->last_h2d = meta_total;
-    // Tile tables must read 0 outside the union.
-    BFX_CUDA(cudaMemsetAsync(ab + tiles_off, 0, tile_table_bytes * count, ws->stream));
-    ws->nb = count;
-    ws->src_total = ssum;
-    ws->params = bfx::LaunchParams{};
-    ws->params.g = g;
-    ws->params.batches = reinterpret_cast<const bfx::DBatch*>(db + o_batch);
-    ws->params.ctl = reinterpret_cast<bfx::DCtl*>(db + o_ctl);
-    ws->params.run = reinterpret_cast<bfx::DRun*>(db + o_run);
-    ws->params.unit_base = reinterpret_cast<const std::uint32_t*>(db + o_ubase);
-    ws->params.nb = count;
-    ws->src_base = reinterpret_cast<bfx::u32*>(db + o_sbase);
-    ws->d_status = reinterpret_cast<bfx_device_run_status*>(db + o_status);
-    ws->d_ctrl = reinterpret_cast<bfx_device_controller*>(db + o_ctrl);
-    ws->executed = false;
+    bfx::upload(ws->meta.ptr, hb, L.meta_total, ws->stream);
+    ws->last_h2d = L.meta_total;
+    // Tile tables must read 0 outside the union (init_kernel writes the union).
+    BFX_CUDA(cudaMemsetAsync(ws->tile_tables.ptr, 0, bfx::align256(size_t{g.T} * 8) * count, ws->stream));
     // Staging must outlive the async copy: synchronise before the host may
     // reuse it (the next prepare overwrites it).
     BFX_CUDA(cudaStreamSynchronize(ws->stream));
+  });
+}
+
+int bfx_prepare_batches_from_queries(bfx_workspace* ws, uint32_t batch_count, const bfx_batch_lanes* batches,
+                                     uint32_t query_count, const bfx_route_query* queries) {
+  return bfx::guarded([&] {
+    using bfx::u32;
+    bfx::require(ws != nullptr, "null workspace");
+    bfx::require(batch_count > 0 && batches && queries, "at least one batch is required");
+    if (batch_count > bfx::kMaxBatchesPerLaunch) throw std::length_error("too many batches for one launch");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    const bfx::DGraph& g = ws->graph->g;
+    // Host checks of the image (validate_batch_device_description's terms,
+    // include/bfnew/batch_layout.hpp:176-199): lane widths and counts, query
+    // indices, strictly increasing tiles and terminals in range.  Terminal
+    // ownership is checked on the device.
+    std::vector<std::uint8_t> used(query_count, 0);
+    std::vector<u32> lane_base(batch_count + 1, 0U), lane_query, lane_tile_base(1, 0U);
+    std::vector<bfx::BatchSizes> sz(batch_count);
+    for (u32 b = 0; b < batch_count; ++b) {
+      const bfx_batch_lanes& d = batches[b];
+      const u32 W = d.lane_width;
+      bfx::require(W == 1 || W == 8 || W == 16 || W == 32, "unsupported lane width");
+      bfx::require(d.lane_count >= 1 && d.lane_count <= W, "lane count must be 1..lane width");
+      bfx::require(d.query_index_by_lane != nullptr, "null lane query indices");
+      u32 S = 0, Tg = 0;
+      for (u32 l = 0; l < d.lane_count; ++l) {
+        const u32 qi = d.query_index_by_lane[l];
+        if (qi >= query_count) throw std::out_of_range("lane query index out of range");
+        const bfx_route_query& r = queries[qi];
+        if (!used[qi]) {
+          bfx::require(r.source_count > 0 && r.target_count > 0, "route queries require sources and targets");
+          bfx::require(r.selected_tile_count > 0 && r.selected_tiles && r.sources && r.targets, "null query array");
+          for (u32 i = 0; i < r.selected_tile_count; ++i) {
+            if (r.selected_tiles[i] >= g.T) throw std::out_of_range("selected tile out of range");
+            bfx::require(i == 0 || r.selected_tiles[i] > r.selected_tiles[i - 1],
+                         "selected tiles must be strictly increasing");
+          }
+          for (u32 i = 0; i < r.source_count; ++i) {
+            if (r.sources[i] >= g.V) throw std::out_of_range("source out of range");
+            bfx::require(i == 0 || r.sources[i] > r.sources[i - 1], "noncanonical sources");
+          }
+          for (u32 i = 0; i < r.target_count; ++i) {
+            if (r.targets[i] >= g.V) throw std::out_of_range("target out of range");
+            bfx::require(i == 0 || r.targets[i] > r.targets[i - 1], "noncanonical targets");
+          }
+          used[qi] = 1;
+        }
+        S += r.source_count;
+        Tg += r.target_count;
+        lane_query.push_back(qi);
+        lane_tile_base.push_back(lane_tile_base.back() + r.selected_tile_count);
+      }
+      lane_base[b + 1] = static_cast<u32>(lane_query.size());
+      const u32 valid = d.lane_count == 32 ? 0xFFFFFFFFu : ((1u << d.lane_count) - 1u);
+      sz[b] = bfx::BatchSizes{0, 0, S, Tg, W, static_cast<u32>(__builtin_ctz(W)), valid, 0};
+    }
+    // The query image: per-query tiles and terminals (concatenated), lane
+    // tables, batch valid masks; one upload.
+    std::vector<u32> qt_off(query_count + 1, 0U), qs_off(query_count + 1, 0U), qg_off(query_count + 1, 0U);
+    for (u32 qi = 0; qi < query_count; ++qi) {
+      const bfx_route_query& r = queries[qi];
+      qt_off[qi + 1] = qt_off[qi] + (used[qi] ? r.selected_tile_count : 0U);
+      qs_off[qi + 1] = qs_off[qi] + (used[qi] ? r.source_count : 0U);
+      qg_off[qi + 1] = qg_off[qi] + (used[qi] ? r.target_count : 0U);
+    }
+    const u32 lanes = static_cast<u32>(lane_query.size());
+    size_t o = 0;
+    auto slot = [&](size_t words) {
+      const size_t at = o;
+      o = bfx::align256(o + words * 4);
+      return at;
+    };
+    const size_t o_qt_off = slot(query_count + 1), o_qt = slot(qt_off[query_count]);
+    const size_t o_qs_off = slot(query_count + 1), o_qs = slot(qs_off[query_count]);
+    const size_t o_qg_off = slot(query_count + 1), o_qg = slot(qg_off[query_count]);
+    const size_t o_lb = slot(batch_count + 1), o_lq = slot(lanes), o_ltb = slot(lanes + 1);
+    const size_t o_valid = slot(batch_count), o_count = slot(4 * size_t{batch_count}), o_err = slot(1);
+    const size_t image_bytes = o;
+    ws->qimage.reserve(image_bytes, ws->graph->device);
+    ws->staging.reserve(image_bytes);
+    char* hb = static_cast<char*>(ws->staging.ptr);
+    char* qb = static_cast<char*>(ws->qimage.ptr);
+    auto put = [&](size_t at, const u32* src, size_t words) {
+      if (words) std::memcpy(hb + at, src, words * 4);
+    };
+    put(o_qt_off, qt_off.data(), query_count + 1);
+    put(o_qs_off, qs_off.data(), query_count + 1);
+    put(o_qg_off, qg_off.data(), query_count + 1);
+    for (u32 qi = 0; qi < query_count; ++qi) {
+      if (!used[qi]) continue;
+      const bfx_route_query& r = queries[qi];
+      put(o_qt + size_t{qt_off[qi]} * 4, r.selected_tiles, r.selected_tile_count);
+      put(o_qs + size_t{qs_off[qi]} * 4, r.sources, r.source_count);
+      put(o_qg + size_t{qg_off[qi]} * 4, r.targets, r.target_count);
+    }
+    put(o_lb, lane_base.data(), batch_count + 1);
+    put(o_lq, lane_query.data(), lanes);
+    put(o_ltb, lane_tile_base.data(), lanes + 1);
+    for (u32 b = 0; b < batch_count; ++b) reinterpret_cast<u32*>(hb + o_valid)[b] = sz[b].valid;
+    reinterpret_cast<u32*>(hb + o_err)[0] = 0U;
+    bfx::upload(qb, hb, image_bytes, ws->stream);
+    bfx::QueryImage q{};
+    q.tile_off = reinterpret_cast<const u32*>(qb + o_qt_off);
+    q.tiles = reinterpret_cast<const u32*>(qb + o_qt);
+    q.src_off = reinterpret_cast<const u32*>(qb + o_qs_off);
+    q.srcs = reinterpret_cast<const u32*>(qb + o_qs);
+    q.tgt_off = reinterpret_cast<const u32*>(qb + o_qg_off);
+    q.tgts = reinterpret_cast<const u32*>(qb + o_qg);
+    q.lane_base = reinterpret_cast<const u32*>(qb + o_lb);
+    q.lane_query = reinterpret_cast<const u32*>(qb + o_lq);
+    q.lane_tile_base = reinterpret_cast<const u32*>(qb + o_ltb);
+    q.nb = batch_count;
+    q.lanes = lanes;
+    // Tile masks on the device, then the union sizes (one small readback
+    // sizes the arena).
+    const size_t tile_table_bytes = bfx::align256(size_t{g.T} * 8);
+    const std::uint64_t tstride = tile_table_bytes / 8;
+    ws->tile_tables.reserve(tile_table_bytes * batch_count, ws->graph->device);
+    uint2* tiles = static_cast<uint2*>(ws->tile_tables.ptr);
+    BFX_CUDA(cudaMemsetAsync(tiles, 0, tile_table_bytes * batch_count, ws->stream));
+    const int wide = ws->sm_count * 8;
+    bfx::desc_mask_kernel<<<wide, 256, 0, ws->stream>>>(q, tiles, tstride);
+    BFX_CUDA(cudaGetLastError());
+    u32* d_count = reinterpret_cast<u32*>(qb + o_count);
+    bfx::desc_count_kernel<<<batch_count, 512, 0, ws->stream>>>(g.tile_off, g.T, tiles, tstride,
+                                                                reinterpret_cast<const u32*>(qb + o_valid), d_count);
+    BFX_CUDA(cudaGetLastError());
+    std::vector<u32> counts(4 * size_t{batch_count});
+    BFX_CUDA(cudaMemcpyAsync(counts.data(), d_count, counts.size() * 4, cudaMemcpyDeviceToHost, ws->stream));
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    for (u32 b = 0; b < batch_count; ++b) {
+      sz[b].R = counts[4 * b];
+      sz[b].U = counts[4 * b + 1];
+      sz[b].full = (sz[b].R == g.T && counts[4 * b + 2] == 0U) ? 1U : 0U;
+      bfx::require(sz[b].U > 0, "batch has no selected vertices");
+    }
+    // Layout, records, then the description arrays written on the device.
+    const bfx::Layout L = bfx::lay_out_batches(ws, batch_count, sz);
+    bfx::upload(ws->meta.ptr, ws->staging.ptr, L.o_up, ws->stream);
+    ws->last_h2d = image_bytes + L.o_up;
+    u32* d_err = reinterpret_cast<u32*>(qb + o_err);
+    bfx::desc_fill_kernel<<<batch_count, 512, 0, ws->stream>>>(q, g.owner, g.tile_off, g.T, tiles, tstride,
+                                                               ws->params.batches, d_err);
+    BFX_CUDA(cudaGetLastError());
+    u32 err = 0;
+    BFX_CUDA(cudaMemcpyAsync(&err, d_err, 4, cudaMemcpyDeviceToHost, ws->stream));
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    if (err) {
+      ws->nb = 0;
+      throw std::invalid_argument("terminal owner tile not selected");
+    }
+  });
+}
+
+int bfx_fetch_prepared_description(bfx_workspace* ws, uint32_t batch, uint32_t counts[5], uint32_t* source_offsets,
+                                   uint32_t* sources, uint32_t* target_offsets, uint32_t* targets,
+                                   uint32_t* union_tiles, uint32_t* tile_lane_masks,
+                                   bfx_batch_vertex_range* selected_vertex_ranges) {
+  return bfx::guarded([&] {
+    bfx::require(ws && counts, "null argument");
+    bfx::require(ws->nb > 0, "no prepared batches");
+    if (batch >= ws->nb) throw std::out_of_range("batch index");
+    BFX_CUDA(cudaSetDevice(ws->graph->device));
+    const bfx::DBatch& B = ws->batches[batch];
+    counts[0] = B.W;
+    counts[1] = B.valid;
+    counts[2] = B.src_count;
+    counts[3] = B.tgt_count;
+    counts[4] = B.range_count;
+    if (!(source_offsets && sources && target_offsets && targets && union_tiles && tile_lane_masks &&
+          selected_vertex_ranges)) {
+      return;  // counts only
+    }
+    const std::uint32_t T = ws->graph->g.T;
+    std::vector<uint4> ranges(B.range_count);
+    std::vector<uint2> table(T);
+    BFX_CUDA(cudaMemcpyAsync(source_offsets, B.src_off, (B.W + 1) * 4, cudaMemcpyDeviceToHost, ws->stream));
+    if (B.src_count)
+      BFX_CUDA(cudaMemcpyAsync(sources, B.src, size_t{B.src_count} * 4, cudaMemcpyDeviceToHost, ws->stream));
+    BFX_CUDA(cudaMemcpyAsync(target_offsets, B.tgt_off, (B.W + 1) * 4, cudaMemcpyDeviceToHost, ws->stream));
+    if (B.tgt_count)
+      BFX_CUDA(cudaMemcpyAsync(targets, B.tgt, size_t{B.tgt_count} * 4, cudaMemcpyDeviceToHost, ws->stream));
+    if (B.range_count)
+      BFX_CUDA(cudaMemcpyAsync(ranges.data(), B.ranges, size_t{B.range_count} * 16, cudaMemcpyDeviceToHost,
+                               ws->stream));
+    BFX_CUDA(cudaMemcpyAsync(table.data(), B.tiles, size_t{T} * 8, cudaMemcpyDeviceToHost, ws->stream));
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    for (std::uint32_t i = 0; i < B.range_count; ++i) {
+      union_tiles[i] = ranges[i].x;
+      selected_vertex_ranges[i] = bfx_batch_vertex_range{ranges[i].y, ranges[i].z, ranges[i].w};
+    }
+    for (std::uint32_t t = 0; t < T; ++t) tile_lane_masks[t] = table[t].x;
   });
 }
 

@@ -42,6 +42,7 @@ struct DGraph {
   const u32* eid_src;  // [E] source vertex of each stable edge id
   const uint2* lrun;   // [V] own-tile run of each CSR row {first CSR index, count} (rows are sorted by
                        // destination tile, so a vertex's edges into its own tile are contiguous)
+  const u32* tile_off; // [T+1] first vertex of each tile
 };
 
 struct DBatch {
@@ -243,7 +244,9 @@ struct bfx_workspace {
   std::uint64_t src_total{0};
   std::vector<bfx::DBatch> batches;
   bfx::DeviceBuffer meta;   // DBatch[], DCtl[], DRun, unit_base, src_base, uploaded descriptions
-  bfx::DeviceBuffer arena;  // labels, masks, queues, c2g, tile tables
+  bfx::DeviceBuffer arena;  // labels, masks, queues, c2g, row tables
+  bfx::DeviceBuffer tile_tables;  // per batch dense {lane mask, compact bias} over all tiles
+  bfx::DeviceBuffer qimage;       // device-side preparation: the uploaded query and lane image
   bfx::PinnedBuffer staging;
   bfx::PinnedBuffer status_host;
   size_t meta_bytes{0};

@@ -109,6 +109,38 @@ int bfx_plan_batch_info(const bfx_plan *plan, uint32_t batch, uint32_t *query_in
 /* All descriptions as one contiguous array (borrowed). */
 int bfx_plan_descriptions(const bfx_plan *plan, const bfx_batch_description **out);
 
+/* ---- device-side batch description preparation ----------------------------
+ * Replaces prepare_batch_device_description (src/batch_layout.cpp:1056-1296)
+ * run on the host per batch: the caller gives only each batch's lane ->
+ * query assignment (lanes 0..lane_count-1 valid, the rest padding) and the
+ * queries' canonical terminals and strictly increasing selected tiles; the
+ * dense tile lane masks, one vertex range per union tile with its compact
+ * offset, and the lane terminal slices are built on the device, into the
+ * workspace, with one small readback of the union sizes.  The result is the
+ * same prepared set bfx_prepare_batches makes from the host descriptions of
+ * the same assignment (ready for bfx_execute).  Errors as
+ * bfx_prepare_batches (a terminal whose owner tile its lane does not select
+ * is rejected with BFX_ERR_INVALID_ARGUMENT). */
+typedef struct bfx_batch_lanes {
+  uint32_t lane_width;                 /* 1, 8, 16 or 32 */
+  uint32_t lane_count;                 /* 1..lane_width */
+  const uint32_t *query_index_by_lane; /* [lane_count] indices into the query array */
+} bfx_batch_lanes;
+
+int bfx_prepare_batches_from_queries(bfx_workspace *ws, uint32_t batch_count, const bfx_batch_lanes *batches,
+                                     uint32_t query_count, const bfx_route_query *queries);
+
+/* The prepared description of batch `batch` as the device holds it (either
+ * prepare path), in bfx_batch_description's arrays: counts = {lane_width,
+ * valid_lane_mask, source count, target count, union tile count}; with every
+ * array non-NULL also source_offsets[W+1], sources, target_offsets[W+1],
+ * targets, union_tiles[R], tile_lane_masks[tile_count] and
+ * selected_vertex_ranges[R]. */
+int bfx_fetch_prepared_description(bfx_workspace *ws, uint32_t batch, uint32_t counts[5],
+                                   uint32_t *source_offsets, uint32_t *sources, uint32_t *target_offsets,
+                                   uint32_t *targets, uint32_t *union_tiles, uint32_t *tile_lane_masks,
+                                   bfx_batch_vertex_range *selected_vertex_ranges);
+
 /* Seeded synthetic spatial workloads (bfx's own generator; the reference's
  * FPGA artifacts are not available).  PRNG: xoshiro256** seeded by
  * splitmix64.  Vertex i of tile (tx, ty) sits at
