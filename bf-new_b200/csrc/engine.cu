@@ -1690,7 +1690,6 @@ int bfx_fetch_prepared_description(bfx_workspace* ws, uint32_t batch, uint32_t c
     }
     const std::uint32_t T = ws->graph->g.T;
     std::vector<uint4> ranges(B.range_count);
-    std::vector<uint2> table(T);
     BFX_CUDA(cudaMemcpyAsync(source_offsets, B.src_off, (B.W + 1) * 4, cudaMemcpyDeviceToHost, ws->stream));
     if (B.src_count)
       BFX_CUDA(cudaMemcpyAsync(sources, B.src, size_t{B.src_count} * 4, cudaMemcpyDeviceToHost, ws->stream));
@@ -1700,13 +1699,15 @@ int bfx_fetch_prepared_description(bfx_workspace* ws, uint32_t batch, uint32_t c
     if (B.range_count)
       BFX_CUDA(cudaMemcpyAsync(ranges.data(), B.ranges, size_t{B.range_count} * 16, cudaMemcpyDeviceToHost,
                                ws->stream));
-    BFX_CUDA(cudaMemcpyAsync(table.data(), B.tiles, size_t{T} * 8, cudaMemcpyDeviceToHost, ws->stream));
     BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    // dense masks from the prepared ranges (the tile table itself is
+    // completed by the launch's init)
+    std::fill(tile_lane_masks, tile_lane_masks + T, 0U);
     for (std::uint32_t i = 0; i < B.range_count; ++i) {
       union_tiles[i] = ranges[i].x;
       selected_vertex_ranges[i] = bfx_batch_vertex_range{ranges[i].y, ranges[i].z, ranges[i].w};
+      if (ranges[i].x < T) tile_lane_masks[ranges[i].x] = ranges[i].w;
     }
-    for (std::uint32_t t = 0; t < T; ++t) tile_lane_masks[t] = table[t].x;
   });
 }
 
