@@ -410,12 +410,11 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
     # ---- end-to-end timing through the C ABI from host buffers (e2e): each
     # step prepares the set (host descriptions, or on the device from the
     # lane -> query assignment), relaxes it and fetches the statuses
-    lanes = [(d.lane_width, [int(x) for x in d.query_index_by_lane[:bin(d.valid_lane_mask).count("1")]])
-             for d in descs]
+    lanes = bfx.QueryLanes.from_descriptions(descs, wl.queries)
 
     def prepare():
         if args.prepare == "device":
-            ws.prepare_from_queries(lanes, wl.queries)
+            ws.prepare_from_queries(lanes)
         else:
             ws.prepare(descs)
         if engines_chosen is None and args.step is not None:

@@ -436,6 +436,27 @@ class BatchDescription:
         return int((self.ranges[:, 1].astype(np.int64) - self.ranges[:, 0]).sum())
 
 
+class QueryLanes:
+    """A batch set as lane -> query assignments over a query list -- the input
+    of device-side description preparation -- with its C image built once."""
+
+    def __init__(self, lanes: Sequence[tuple[int, Sequence[int]]], queries: Sequence["RouteQuery"]):
+        self.queries = list(queries)
+        self.query_count = len(self.queries)
+        self.queries_c = (RouteQueryC * self.query_count)(*[q.c() for q in self.queries])
+        self._idx = [np.ascontiguousarray(np.asarray(ix, np.uint32)) for _, ix in lanes]
+        self.count = len(self._idx)
+        self.batches_c = (BatchLanesC * self.count)(*[BatchLanesC(w, len(a), _ptr(a))
+                                                      for (w, _), a in zip(lanes, self._idx)])
+
+    @classmethod
+    def from_descriptions(cls, descriptions: Sequence["BatchDescription"], queries: Sequence["RouteQuery"]):
+        """The assignment a plan's descriptions carry (valid lanes first)."""
+        lanes = [(d.lane_width, [int(x) for x in d.query_index_by_lane[:bin(d.valid_lane_mask).count("1")]])
+                 for d in descriptions]
+        return cls(lanes, queries)
+
+
 class BatchPlan:
     """make_overlapping_batch_plan + prepare_batch_device_description (libbfx)."""
 
@@ -540,15 +561,15 @@ class Workspace:
         _check(load().bfx_prepare_batches(self._h, u32(len(batches)), arr))
         self.batch_count = len(batches)
 
-    def prepare_from_queries(self, lanes: Sequence[tuple[int, Sequence[int]]], queries: Sequence["RouteQuery"]):
+    def prepare_from_queries(self, lanes, queries: Sequence["RouteQuery"] | None = None):
         """bfx_prepare_batches_from_queries: batches given as (lane width, query
-        indices of the valid lanes); descriptions are built on the device."""
-        qc = (RouteQueryC * len(queries))(*[q.c() for q in queries])
-        idx = [np.ascontiguousarray(np.asarray(ix, np.uint32)) for _, ix in lanes]
-        bc = (BatchLanesC * len(lanes))(*[BatchLanesC(w, len(ix), _ptr(a)) for (w, ix), a in zip(lanes, idx)])
-        self._keep = (qc, idx, list(queries))
-        _check(load().bfx_prepare_batches_from_queries(self._h, u32(len(lanes)), bc, u32(len(queries)), qc))
-        self.batch_count = len(lanes)
+        indices of the valid lanes) over `queries`, or a prebuilt QueryLanes;
+        descriptions are built on the device."""
+        image = lanes if isinstance(lanes, QueryLanes) else QueryLanes(lanes, queries)
+        self._keep = image
+        _check(load().bfx_prepare_batches_from_queries(self._h, u32(image.count), image.batches_c, u32(image.query_count),
+                                                       image.queries_c))
+        self.batch_count = image.count
 
     def prepared_description(self, batch: int) -> "BatchDescription":
         """The prepared description of a batch, read back from the device."""
