@@ -344,6 +344,13 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
         if args.step is not None:
             deltas = [float("inf") if args.step == 0 else args.step * mean_w] * len(descs)
             ws.set_batch_deltas(deltas)
+    # the layout and per-batch mappings the tuner left (it may switch between
+    # the chunked and the tiled layout)
+    layout_names = {v: k for k, v in layout_ids.items()}
+    tuned_layout, tuned_mappings = ws.frontier_mapping(len(descs))
+    frontier_used = layout_names[tuned_layout]
+    if frontier_used == "tiled":
+        eff_regs = 128
     opts = bfx.GpuRunOptions(engine=engine_id)
     opts_instr = bfx.GpuRunOptions(engine=engine_id, instrumentation=1)
 
@@ -468,7 +475,7 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
             plain_total_s += s3.elapsed_time(e3) / 1000 / len(sample_q) * len(members)
             plain_sampled += len(sample_q)
         plain_by_layout[lname] = len(wl.queries) / plain_total_s
-    ws.set_frontier_layout(layout_ids[args.frontier])
+    ws.set_frontier_layout(tuned_layout)
 
     nq = (len(wl.queries) if shard else queries_here * world)
     ms_per_step = dev_ms / steps
@@ -491,7 +498,10 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
     achieved = alg_bytes / (kernel_avg / 1000) / 1e9
     engines_for_step = engines_chosen or [2 if engine_id == bfx.ENGINE_FRONTIER_PUSH else engine_id] * len(descs)
     step = step_label(engines_for_step, deltas, mean_w)
-    traffic, traffic_source, random_ceiling = traffic_estimate(wl.name, work["relaxations"], kernel_avg, step)
+    if frontier_used == "chunked":
+        traffic, traffic_source, random_ceiling = traffic_estimate(wl.name, work["relaxations"], kernel_avg, step)
+    else:  # the committed traffic captures are of the chunked kernel
+        traffic, traffic_source, random_ceiling = None, f"no capture of the {frontier_used} kernel is scaled", None
     line = {
         "metric": METRICS[wl.name], "value": value, "unit": "queries/s", "n_gpus": world, "steps": steps,
         "warmup": warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -504,7 +514,10 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
                                       wl.policy.maximum_union_inflation_numerator,
                                       wl.policy.maximum_union_inflation_denominator],
                    "near_far_step": step,
-                   "frontier_layout": args.frontier, "registers": eff_regs, "flat_items": args.items,
+                   "frontier_layout": frontier_used,
+                   "tile_visit_batches": (sum(1 for m in tuned_mappings if m == bfx.MAPPING_TILE_VISITS)
+                                          if frontier_used == "tiled" else 0),
+                   "registers": eff_regs, "flat_items": args.items,
                    "returning_min": args.amin, "edge_major": args.edge_major, "chunk_pairs": args.pairs,
                    "engines_chosen": None if engines_chosen is None else
                    {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
@@ -521,8 +534,9 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
                          "before both timed regions"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "traffic_source": traffic_source, "peak_source": peak_src,
-                     "random_sector_ceiling": random_ceiling, "kernel": "persistent_kernel (%s frontier, %d registers%s)" % (
-                         args.frontier, eff_regs,
+                     "random_sector_ceiling": random_ceiling, "kernel": "%s (%s frontier, %d registers%s)" % (
+                         "persistent_tiled_kernel" if frontier_used == "tiled" else "persistent_kernel",
+                         frontier_used, eff_regs,
                          ", mixed engines" if engines_chosen and any(e != 2 for e in engines_chosen) else ""),
                      "kernel_ms": kernel_avg, "execute_ms": float(np.mean(execute_ms)),
                      "algorithmic_bytes_per_launch": alg_bytes, "work": work, "engine_work": engine_work},

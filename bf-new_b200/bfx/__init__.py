@@ -35,6 +35,7 @@ ENGINE_JACOBI_PULL, ENGINE_DENSE_CHAOTIC_PUSH, ENGINE_FRONTIER_PUSH = 0, 1, 2
 ENGINE_AUTO = 0xFFFFFFFF
 CONTROL_PERSISTENT, CONTROL_CHUNKED, CONTROL_PER_ROUND = 0, 1, 2
 FRONTIER_GROUPS, FRONTIER_FLAT, FRONTIER_CHUNKED, FRONTIER_TILED = 0, 1, 2, 3
+MAPPING_CHUNKS, MAPPING_TILE_VISITS = 0, 1
 STOP_NONE, STOP_CONVERGED, STOP_MAXIMUM_ROUNDS, STOP_QUEUE_OVERFLOW, STOP_INVALID, STOP_FAILURE = range(6)
 INF_BITS = 0x7F800000
 NO_EDGE = 0xFFFFFFFF
@@ -656,6 +657,19 @@ class Workspace:
         """FRONTIER_GROUPS (sub-warp groups per entry), FRONTIER_FLAT (flat work list),
         FRONTIER_CHUNKED (32-vertex chunks) or FRONTIER_TILED (tile visits in shared memory)."""
         _check(load().bfx_set_frontier_layout(self._h, u32(layout)))
+
+    def set_batch_mappings(self, mappings: Sequence[int]):
+        """Tiled layout: per-batch dense-round mapping (MAPPING_TILE_VISITS or MAPPING_CHUNKS)."""
+        arr = (u32 * len(mappings))(*mappings)
+        _check(load().bfx_set_batch_mappings(self._h, u32(len(mappings)), arr))
+
+    def frontier_mapping(self, count: int | None = None) -> tuple[int, list[int]]:
+        """(frontier layout, per-batch mappings of the first `count` batches)."""
+        n = self.batch_count if count is None else count
+        layout = u32()
+        arr = (u32 * max(n, 1))()
+        _check(load().bfx_get_frontier_mapping(self._h, C.byref(layout), u32(n), arr))
+        return layout.value, list(arr[:n])
 
     def set_tile_passes(self, passes: int):
         """Tiled layout: local relaxation passes per staged visit."""

@@ -13,9 +13,16 @@
 //     magnitudes of the union vertex and tile counts.
 //  3. In context again: the per-batch engines are kept only if the whole set
 //     runs faster with them than all-frontier with the phase-1 step.
-// The set is left prepared with its per-batch engines and steps, so an
-// execute with engine == BFX_ENGINE_AUTO runs each batch on its own engine
-// inside one launch.
+//  4. The work mapping (a workspace in the chunked or tiled frontier layout,
+//     persistent control): in context, the other of the two layouts at the
+//     chosen steps, kept if the whole set runs faster; under the tiled
+//     layout, per batch shape, dense rounds as tile visits or as chunk-slot
+//     warp items (timed alone, visits only where 1.1x faster; cached by
+//     signature), the per-batch mix kept only if the whole set runs faster
+//     than all-visits.
+// The set is left prepared with its per-batch engines, steps and mappings, so
+// an execute with engine == BFX_ENGINE_AUTO runs each batch on its own engine
+// and mapping inside one launch.
 #include "bfx.h"
 #include "bfx_host.h"
 #include "bfx_internal.hpp"
@@ -42,6 +49,7 @@ constexpr float kPlain = __builtin_inff();
 
 std::mutex g_tune_mutex;
 std::map<Signature, Choice> g_tune_cache;
+std::map<Signature, std::uint32_t> g_mapping_cache;  // tiled layout: BFX_MAPPING_* per batch shape
 
 Signature signature(const bfx_batch_description& d) {
   std::uint64_t U = 0;
@@ -172,6 +180,65 @@ extern "C" int bfx_autotune(bfx_workspace* ws, uint32_t count, const bfx_batch_d
     }
     bfx::check(bfx_set_batch_engines(ws, count, engines.data()));
     bfx::check(bfx_set_batch_deltas(ws, count, deltas.data()));
+
+    // Phase 4: the work mapping.
+    std::uint32_t layout = 0;
+    bfx::check(bfx_get_frontier_mapping(ws, &layout, 0, nullptr));
+    if ((layout == BFX_FRONTIER_CHUNKED || layout == BFX_FRONTIER_TILED) &&
+        o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE && (o.block_size == 256 || o.block_size == 384)) {
+      bfx_gpu_run_options oa = o;
+      oa.engine = BFX_ENGINE_AUTO;
+      bfx::check(bfx_set_batch_mappings(ws, 0, nullptr));
+      const float t_here = bfx::time_set(ws, oa, trials);
+      const std::uint32_t other = layout == BFX_FRONTIER_CHUNKED ? BFX_FRONTIER_TILED : BFX_FRONTIER_CHUNKED;
+      bfx::check(bfx_set_frontier_layout(ws, other));
+      const float t_other = bfx::time_set(ws, oa, trials);
+      if (t_other < t_here) {
+        layout = other;
+      } else {
+        bfx::check(bfx_set_frontier_layout(ws, layout));
+      }
+      if (layout == BFX_FRONTIER_TILED) {
+        const float t_visits = std::min(t_here, t_other);
+        std::vector<std::uint32_t> mappings(count, BFX_MAPPING_TILE_VISITS);
+        bool any_chunks = false;
+        for (std::uint32_t b = 0; b < count; ++b) {
+          if (engines[b] != BFX_ENGINE_FRONTIER_PUSH) continue;
+          const bfx::Signature sig = bfx::signature(batches[b]);
+          {
+            std::lock_guard<std::mutex> lock(bfx::g_tune_mutex);
+            const auto it = bfx::g_mapping_cache.find(sig);
+            if (it != bfx::g_mapping_cache.end()) {
+              mappings[b] = it->second;
+              any_chunks |= it->second == BFX_MAPPING_CHUNKS;
+              continue;
+            }
+          }
+          bfx::check(bfx_prepare_batches(ws, 1, &batches[b]));
+          bfx::check(bfx_set_batch_deltas(ws, 1, &deltas[b]));
+          bfx_gpu_run_options of = o;
+          of.engine = BFX_ENGINE_FRONTIER_PUSH;
+          const std::uint32_t visit = BFX_MAPPING_TILE_VISITS, chunks = BFX_MAPPING_CHUNKS;
+          bfx::check(bfx_set_batch_mappings(ws, 1, &visit));
+          const float tv = bfx::time_set(ws, of, trials);
+          bfx::check(bfx_set_batch_mappings(ws, 1, &chunks));
+          const float tc = bfx::time_set(ws, of, trials);
+          mappings[b] = tv * 1.1f <= tc ? BFX_MAPPING_TILE_VISITS : BFX_MAPPING_CHUNKS;
+          any_chunks |= mappings[b] == BFX_MAPPING_CHUNKS;
+          ++n_measured;
+          std::lock_guard<std::mutex> lock(bfx::g_tune_mutex);
+          bfx::g_mapping_cache[sig] = mappings[b];
+        }
+        bfx::check(bfx_prepare_batches(ws, count, batches));
+        bfx::check(bfx_set_batch_engines(ws, count, engines.data()));
+        bfx::check(bfx_set_batch_deltas(ws, count, deltas.data()));
+        bfx::check(bfx_set_batch_mappings(ws, 0, nullptr));
+        if (any_chunks) {
+          bfx::check(bfx_set_batch_mappings(ws, count, mappings.data()));
+          if (bfx::time_set(ws, oa, trials) >= t_visits) bfx::check(bfx_set_batch_mappings(ws, 0, nullptr));
+        }
+      }
+    }
     if (measured) *measured = n_measured;
   });
 }
@@ -180,6 +247,7 @@ extern "C" int bfx_autotune_reset(void) {
   return bfx::guarded([&] {
     std::lock_guard<std::mutex> lock(bfx::g_tune_mutex);
     bfx::g_tune_cache.clear();
+    bfx::g_mapping_cache.clear();
   });
 }
 

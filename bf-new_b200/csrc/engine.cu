@@ -1784,6 +1784,22 @@ const void* persistent_entry(bool count, std::uint32_t registers, std::uint32_t 
                : reinterpret_cast<const void*>(persistent_kernel<false, 2, 2>);
 }
 
+// A per-batch launch parameter array (engines, steps, mappings) on the
+// device.  Uploaded only when it differs from the last upload, after the
+// workspace stream drained, so a launch still in flight never sees a
+// half-written array and no staging buffer is rewritten under an
+// asynchronous copy.
+const std::uint32_t* upload_batch_words(bfx_workspace* ws, DeviceBuffer& dev, std::vector<std::uint32_t>& uploaded,
+                                        const std::vector<std::uint32_t>& words) {
+  if (dev.ptr == nullptr || uploaded != words) {
+    BFX_CUDA(cudaStreamSynchronize(ws->stream));
+    dev.reserve(words.size() * 4, ws->graph->device);
+    BFX_CUDA(cudaMemcpy(dev.ptr, words.data(), words.size() * 4, cudaMemcpyHostToDevice));
+    uploaded = words;
+  }
+  return static_cast<const std::uint32_t*>(dev.ptr);
+}
+
 void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   require(ws->nb > 0, "no prepared batches");
   validate_options(o, true);
@@ -1807,6 +1823,10 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
     if (p.flat == 3u) {
       p.tshift = ws->graph->tile_shift;
       for (const DBatch& b : ws->batches) p.tile_wmax = std::max(p.tile_wmax, b.W);
+      if (!ws->batch_mappings.empty()) {
+        require(ws->batch_mappings.size() == ws->nb, "per-batch mappings do not match the prepared batches");
+        p.mappings = upload_batch_words(ws, ws->mappings_dev, ws->mappings_uploaded, ws->batch_mappings);
+      }
     }
   }
   p.round_trace = nullptr;
@@ -1821,24 +1841,16 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   }
   if (!ws->batch_deltas.empty()) {
     require(ws->batch_deltas.size() == ws->nb, "per-batch deltas do not match the prepared batches");
-    ws->deltas_dev.reserve(ws->nb * 4, ws->graph->device);
-    ws->deltas_host.reserve(ws->nb * 4 + 256);
-    std::memcpy(ws->deltas_host.ptr, ws->batch_deltas.data(), ws->nb * 4);
-    BFX_CUDA(cudaMemcpyAsync(ws->deltas_dev.ptr, ws->deltas_host.ptr, ws->nb * 4, cudaMemcpyHostToDevice,
-                             ws->stream));
-    p.deltas = static_cast<const std::uint32_t*>(ws->deltas_dev.ptr);
+    std::vector<std::uint32_t> bits(ws->nb);
+    std::memcpy(bits.data(), ws->batch_deltas.data(), ws->nb * 4);
+    p.deltas = upload_batch_words(ws, ws->deltas_dev, ws->deltas_uploaded, bits);
   }
   if (o.engine == BFX_ENGINE_AUTO) {
     // Per-batch engines chosen by bfx_autotune / bfx_set_batch_engines
     // (frontier push where none was chosen).
     std::vector<std::uint32_t> eng(ws->nb, BFX_ENGINE_FRONTIER_PUSH);
     if (ws->batch_engines.size() == ws->nb) eng = ws->batch_engines;
-    ws->engines_dev.reserve(ws->nb * 4, ws->graph->device);
-    ws->status_host.reserve(ws->nb * 4 + 256);
-    std::memcpy(ws->status_host.ptr, eng.data(), ws->nb * 4);
-    BFX_CUDA(cudaMemcpyAsync(ws->engines_dev.ptr, ws->status_host.ptr, ws->nb * 4, cudaMemcpyHostToDevice,
-                             ws->stream));
-    p.engines = static_cast<const std::uint32_t*>(ws->engines_dev.ptr);
+    p.engines = upload_batch_words(ws, ws->engines_dev, ws->engines_uploaded, eng);
     p.engine = BFX_ENGINE_FRONTIER_PUSH;
   }
   const int block = static_cast<int>(o.block_size);
@@ -2024,6 +2036,28 @@ int bfx_set_tile_stage_min(bfx_workspace* ws, uint32_t lane_edges) {
   return bfx::guarded([&] {
     bfx::require(ws != nullptr, "null argument");
     ws->tile_stage_min = lane_edges;
+  });
+}
+
+int bfx_set_batch_mappings(bfx_workspace* ws, uint32_t count, const uint32_t* mappings) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null workspace");
+    bfx::require(count == 0 || mappings != nullptr, "null mappings");
+    for (std::uint32_t i = 0; i < count; ++i) {
+      bfx::require(mappings[i] == BFX_MAPPING_CHUNKS || mappings[i] == BFX_MAPPING_TILE_VISITS, "invalid mapping");
+    }
+    ws->batch_mappings.assign(mappings, mappings + count);
+  });
+}
+
+int bfx_get_frontier_mapping(bfx_workspace* ws, uint32_t* layout, uint32_t count, uint32_t* mappings) {
+  return bfx::guarded([&] {
+    bfx::require(ws && layout, "null argument");
+    *layout = ws->frontier_layout;
+    for (std::uint32_t i = 0; i < count; ++i) {
+      bfx::require(mappings != nullptr, "null mappings");
+      mappings[i] = i < ws->batch_mappings.size() ? ws->batch_mappings[i] : BFX_MAPPING_TILE_VISITS;
+    }
   });
 }
 
@@ -2284,19 +2318,21 @@ int bfx_run_query(bfx_workspace* ws, uint32_t source_count, const uint32_t* sour
     d.range_count = selected_tile_count;
     d.selected_vertex_ranges = ranges.data();
     // The plain per-query engine runs the options' engine as given: per-batch
-    // engines and near/far steps of the workspace's batch set do not apply
-    // (they are kept for that set).
+    // engines, near/far steps and mappings of the workspace's batch set do
+    // not apply (they are kept for that set).
     struct Keep {
       bfx_workspace* ws;
-      std::vector<std::uint32_t> engines;
+      std::vector<std::uint32_t> engines, mappings;
       std::vector<float> deltas;
       explicit Keep(bfx_workspace* w) : ws(w) {
         engines.swap(w->batch_engines);
         deltas.swap(w->batch_deltas);
+        mappings.swap(w->batch_mappings);
       }
       ~Keep() {
         ws->batch_engines.swap(engines);
         ws->batch_deltas.swap(deltas);
+        ws->batch_mappings.swap(mappings);
       }
     } keep(ws);
     int rc = bfx_run_batches(ws, 1, &d, options, status);

@@ -159,6 +159,7 @@ struct LaunchParams {
   u32 tile_wmax;         // tiled layout: widest batch of the launch (sizes the staged label rows)
   u32 tile_iters;        // tiled layout: local relaxation passes per visit before the rest waits a round
   u32 tshift;            // tiled layout: a dense round visits units of 2^tshift compact vertices (the tile size)
+  const u32* mappings;   // tiled layout, [nb] or null (every batch visits tiles): BFX_MAPPING_* per batch
 };
 
 constexpr u32 kRoundTraceCap = 65536;
@@ -281,6 +282,8 @@ struct bfx_workspace {
   bfx::DeviceBuffer adjoint;     // per-edge exact accumulators, upstream values, result
   std::vector<std::uint32_t> batch_engines;  // per-batch engine for BFX_ENGINE_AUTO launches
   std::vector<float> batch_deltas;           // per-batch near/far steps (empty: plain frontier)
+  std::vector<std::uint32_t> batch_mappings; // tiled layout: per-batch dense-round mapping (empty: tile visits)
+  bfx::DeviceBuffer mappings_dev;
   std::uint32_t frontier_layout = 2;         // BFX_FRONTIER_CHUNKED (default) / _FLAT / _GROUPS
   std::uint32_t relax_atomic = 0;            // flat frontier relaxation: 0 pre-read + min, 1 returning min
   std::uint32_t edge_major = 0;              // flat frontier work order (see bfx_set_flat_order)
@@ -290,8 +293,8 @@ struct bfx_workspace {
   std::uint32_t tile_stage_min = 1024;       // tiled layout: lane-edge work from which a visit stages its labels
   std::uint32_t tile_iters = 32;             // tiled layout: local passes per visit
   bfx::DeviceBuffer deltas_dev;
-  bfx::PinnedBuffer deltas_host;
   bfx::DeviceBuffer engines_dev;
+  std::vector<std::uint32_t> deltas_uploaded, engines_uploaded, mappings_uploaded;  // contents of the *_dev arrays
   bfx::DeviceBuffer round_trace;  // instrumentation 2 only
 };
 

@@ -365,13 +365,19 @@ __device__ void tile_visit(const LaunchParams& p, const FrontierView& B, u32 uni
 }
 
 // Work of round r in two prefixes: block items (one tile visit per unit of a
-// frontier batch in a dense near round) and warp items (everything else, as
-// the chunked layout counts them: one queued chunk per sparse near item, 32
-// far entries per split item, Jacobi / dense warp items).
+// frontier batch in a dense near round, for batches mapped to tile visits)
+// and warp items (everything else, as the chunked layout counts them: one
+// queued chunk per sparse near item, every chunk slot of a dense round of a
+// batch mapped to chunks, 32 far entries per split item, Jacobi / dense warp
+// items).
+__device__ __forceinline__ bool visits_tiles(const LaunchParams& p, u32 b) {
+  return p.mappings == nullptr || p.mappings[b] == BFX_MAPPING_TILE_VISITS;
+}
+
 __device__ u32 round_work_tiled(const LaunchParams& p, u32 r, u32* prefix_block, u32* prefix_warp) {
   const u32 ridx = r % 3u;
   block_prefix(prefix_block, p.nb, [&](u32 b) -> u32 {
-    if (engine_of(p, b) != BFX_ENGINE_FRONTIER_PUSH) return 0u;
+    if (engine_of(p, b) != BFX_ENGINE_FRONTIER_PUSH || !visits_tiles(p, b)) return 0u;
     const DBatch& B = p.batches[b];
     const u32 n = min(dev::ld_cg(&p.ctl[b].count[ridx]), B.U);
     return n != 0u && chunk_dense(n, B.U, 5u) ? chunk_count(B.U, p.tshift) : 0u;
@@ -381,7 +387,9 @@ __device__ u32 round_work_tiled(const LaunchParams& p, u32 r, u32* prefix_block,
     if (engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH) {
       const DCtl& C = p.ctl[b];
       const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
-      if (n != 0u) return chunk_dense(n, B.U, 5u) ? 0u : n;
+      // dense rounds of a batch mapped to chunks: every chunk slot, in index
+      // order, as the chunked layout runs them
+      if (n != 0u) return chunk_dense(n, B.U, 5u) ? (visits_tiles(p, b) ? 0u : chunk_count(B.U, 5u)) : n;
       const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
       return (f + 31u) >> 5;
     }

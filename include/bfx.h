@@ -282,12 +282,19 @@ int bfx_resident_graph_set_weights(bfx_resident_graph *graph, const float *weigh
  * it is at least 1.5x faster on the batch alone (cached per lane width, valid
  * lanes, magnitude of union vertices and tiles), and keeps those engines only
  * if the whole set runs faster with them (best of `trials` device timings
- * each).  Leaves the
- * workspace prepared with all `count` batches and their engines and steps, so
- * bfx_execute with options->engine == BFX_ENGINE_AUTO relaxes each batch with
- * its own engine in one launch.  engines_out[count]; deltas_out[count] (may be
- * NULL) = chosen steps (+inf = plain); *measured (may be NULL) = batches that
- * were timed rather than found in the cache. */
+ * each).  Then the work mapping, when the workspace is in the chunked or the
+ * tiled frontier layout with persistent control and blocks of 256 or 384
+ * threads: the other of the two layouts is timed on the whole set and kept
+ * if faster (the workspace's layout may change), and under the tiled layout
+ * each batch shape's dense rounds are mapped to tile visits or chunk-slot
+ * warp items (timed alone, visits where 1.1x faster, cached per shape), the
+ * per-batch mix kept only if the whole set runs faster (bfx_get_frontier_mapping
+ * reports the outcome).  Leaves the workspace prepared with all `count`
+ * batches and their engines, steps and mappings, so bfx_execute with
+ * options->engine == BFX_ENGINE_AUTO relaxes each batch with its own engine
+ * in one launch.  engines_out[count]; deltas_out[count] (may be NULL) =
+ * chosen steps (+inf = plain); *measured (may be NULL) = batches that were
+ * timed rather than found in the cache. */
 int bfx_autotune(bfx_workspace *ws, uint32_t count, const bfx_batch_description *batches,
                  const bfx_gpu_run_options *base, uint32_t trials, uint32_t *engines_out, float *deltas_out,
                  uint32_t *measured);
@@ -331,6 +338,16 @@ int bfx_set_tile_stage_min(bfx_workspace *ws, uint32_t lane_edges);
  * default 32); lanes still pending after them are relaxed in the next round
  * (bfx extension; results unchanged). */
 int bfx_set_tile_passes(bfx_workspace *ws, uint32_t passes);
+/* Tiled layout, per batch (bfx extension; results unchanged): dense rounds
+ * as tile visits (BFX_MAPPING_TILE_VISITS, the default) or as chunk-slot
+ * warp items like the chunked layout (BFX_MAPPING_CHUNKS).  count 0 clears
+ * the setting; otherwise count must equal the prepared batch count at
+ * execute time.  bfx_autotune sets these when it keeps the tiled layout. */
+enum { BFX_MAPPING_CHUNKS = 0, BFX_MAPPING_TILE_VISITS = 1 };
+int bfx_set_batch_mappings(bfx_workspace *ws, uint32_t count, const uint32_t *mappings);
+/* The workspace's frontier layout and, for the first `count` batches, their
+ * mappings (BFX_MAPPING_TILE_VISITS where none was set). */
+int bfx_get_frontier_mapping(bfx_workspace *ws, uint32_t *layout, uint32_t count, uint32_t *mappings);
 /* Register budget of the persistent relaxation kernel (a bfx tuning option,
  * results unchanged): 40 registers per thread (three 512-thread blocks per
  * SM), 64 (two 512-thread blocks per SM: no spills in the group layout, few

@@ -136,3 +136,47 @@ def test_host_poll_modes_fall_back_to_chunked(gpu, c1):
     d = bfx.make_description(c1.layout, c1.queries, 8)
     st, labels, _ = run_tiled(c1.layout, [d], 0, control=bfx.CONTROL_CHUNKED)
     check_batches(c1.layout, [d], [c1.queries], st, labels, Oracle.from_layout(c1.layout))
+
+
+@pytest.mark.parametrize("step", [None, 3.0])
+def test_per_batch_mappings_bit_exact(gpu, c2_regional, step):
+    """One tiled launch with dense rounds mapped per batch: alternating tile
+    visits and chunk-slot warp items."""
+    layout, descs, lanes = c2_regional
+    res = bfx.ResidentDeviceGraph.upload_once(layout)
+    ws = bfx.Workspace(res)
+    ws.set_frontier_layout(bfx.FRONTIER_TILED)
+    ws.set_tile_stage_min(0)
+    ws.prepare(descs)
+    if step is not None:
+        ws.set_batch_deltas([step] * len(descs))
+    mappings = [bfx.MAPPING_TILE_VISITS if b % 2 else bfx.MAPPING_CHUNKS for b in range(len(descs))]
+    ws.set_batch_mappings(mappings)
+    assert ws.frontier_mapping(len(descs)) == (bfx.FRONTIER_TILED, mappings)
+    ws.execute(bfx.GpuRunOptions(instrumentation=1))
+    st = ws.fetch_statuses()
+    labels = [ws.download_labels(b, d.lane_width) for b, d in enumerate(descs)]
+    check_batches(layout, descs, lanes, st, labels, Oracle.from_layout(layout))
+    ws.close()
+    res.close()
+
+
+@pytest.mark.parametrize("start", [bfx.FRONTIER_CHUNKED, bfx.FRONTIER_TILED], ids=["from_chunked", "from_tiled"])
+def test_autotuner_chooses_layout_and_mappings(gpu, c2_regional, start):
+    """bfx_autotune's mapping phase: whichever of the chunked and tiled layouts
+    it keeps, and whatever per-batch mappings, the AUTO launch is bit-exact."""
+    layout, descs, lanes = c2_regional
+    res = bfx.ResidentDeviceGraph.upload_once(layout)
+    ws = bfx.Workspace(res)
+    bfx.load().bfx_autotune_reset()
+    ws.set_frontier_layout(start)
+    engines, measured = ws.autotune(descs)
+    kept, mappings = ws.frontier_mapping(len(descs))
+    assert kept in (bfx.FRONTIER_CHUNKED, bfx.FRONTIER_TILED)
+    assert set(mappings) <= {bfx.MAPPING_CHUNKS, bfx.MAPPING_TILE_VISITS}
+    ws.execute(bfx.GpuRunOptions(engine=bfx.ENGINE_AUTO))
+    st = ws.fetch_statuses()
+    labels = [ws.download_labels(b, d.lane_width) for b, d in enumerate(descs)]
+    check_batches(layout, descs, lanes, st, labels, Oracle.from_layout(layout))
+    ws.close()
+    res.close()
