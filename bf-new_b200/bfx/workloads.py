@@ -224,11 +224,16 @@ BENCH_DESCRIPTIONS = {
 }
 
 
-def bench_workload(name: str, rank: int = 0, query_count: int | None = None, threads: int = 0) -> BenchWorkload:
-    """The exact graph, query set and planner policy that bench.py times."""
+def bench_workload(name: str, rank: int = 0, query_count: int | None = None, threads: int = 0,
+                   keep_input: bool = False) -> BenchWorkload:
+    """The exact graph, query set and planner policy that bench.py times.  The
+    input graph (edge records, vertex metadata: 4.7 GB on c3) is dropped once
+    the layout is built unless `keep_input`."""
     spec, grid = bench_graph_spec(name)
     g, order, _ = synth_graph(**spec)
     layout = build_device_graph_layout(g, order, threads)
+    if not keep_input:
+        g = None
     queries, classes = bench_queries(name, layout, grid, rank, query_count)
     if name in ("c2", "c5"):
         policy = BatchPlannerPolicy(32, 1, 8, 2, 1, narrow_lanes=True)
