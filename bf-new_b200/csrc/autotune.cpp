@@ -6,7 +6,10 @@
 //  1. In context: the whole set on frontier push with one near/far step for
 //     every batch -- plain, and 1/2, 1, 2, 4, 8, 32, 128 mean edge weights -- as it
 //     will run, in one launch; the fastest step wins.  (A batch timed alone
-//     favours few rounds; in one launch with others the work matters.)
+//     favours few rounds; in one launch with others the work matters.)  The
+//     step and the phase-4 layout are cached per set class (graph, magnitudes
+//     of the batch count per lane width and of the union size), so a later
+//     query set of the same class skips both searches.
 //  2. Per batch shape: Jacobi pull or dense chaotic push replaces frontier
 //     push only where it is at least 1.5x faster on the batch alone.  Cached
 //     by batch signature -- lane width, valid lanes, and the binary
@@ -51,6 +54,18 @@ std::mutex g_tune_mutex;
 std::map<Signature, Choice> g_tune_cache;
 std::map<Signature, std::uint32_t> g_mapping_cache;  // tiled layout: BFX_MAPPING_* per batch shape
 
+// A set's class: the graph (edge count and mean weight bits), and the binary
+// magnitudes of the batch count, of the batch counts per lane width and of
+// the total union vertices.  Two query sets of one workload fall into one
+// class, so the second reuses the first's in-context choices.
+using SetKey = std::tuple<std::uint64_t, std::uint32_t, std::uint32_t, std::uint32_t, std::uint32_t, std::uint32_t,
+                          std::uint32_t, std::uint32_t, std::uint32_t>;
+struct SetChoice {
+  float step;           // phase 1
+  std::uint32_t layout; // phase 4 (frontier layout kept)
+};
+std::map<SetKey, SetChoice> g_set_cache;
+
 Signature signature(const bfx_batch_description& d) {
   std::uint64_t U = 0;
   for (std::uint32_t i = 0; i < d.range_count; ++i) U += d.selected_vertex_ranges[i].end - d.selected_vertex_ranges[i].begin;
@@ -61,6 +76,24 @@ Signature signature(const bfx_batch_description& d) {
 
 void check(int rc) {
   if (rc != BFX_OK) throw Error(rc, bfx_last_error());
+}
+
+SetKey set_key(const double stats[2], std::uint32_t count, const bfx_batch_description* batches,
+               std::uint32_t layout) {
+  const auto log2u = [](std::uint64_t x) { return x ? 64U - static_cast<std::uint32_t>(std::countl_zero(x)) : 0U; };
+  std::uint64_t by_width[4] = {0, 0, 0, 0}, union_vertices = 0;
+  for (std::uint32_t b = 0; b < count; ++b) {
+    const bfx_batch_description& d = batches[b];
+    by_width[d.lane_width == 1 ? 0 : d.lane_width == 8 ? 1 : d.lane_width == 16 ? 2 : 3] += 1;
+    for (std::uint32_t i = 0; i < d.range_count; ++i) {
+      union_vertices += d.selected_vertex_ranges[i].end - d.selected_vertex_ranges[i].begin;
+    }
+  }
+  const float mean = static_cast<float>(stats[0]);
+  std::uint32_t mean_bits;
+  std::memcpy(&mean_bits, &mean, 4);
+  return {static_cast<std::uint64_t>(stats[1]) << 32 | mean_bits, log2u(count), log2u(by_width[0]),
+          log2u(by_width[1]), log2u(by_width[2]), log2u(by_width[3]), log2u(union_vertices), layout, 0U};
 }
 
 }  // namespace
@@ -100,18 +133,39 @@ extern "C" int bfx_autotune(bfx_workspace* ws, uint32_t count, const bfx_batch_d
     o.instrumentation = 0;
 
     // Phase 1, in context: every batch on frontier push with one step, the
-    // whole set relaxed together as it will run; keep the fastest step.
+    // whole set relaxed together as it will run; keep the fastest step.  A
+    // set of a class tuned before reuses that class's step (timed once).
+    std::uint32_t layout0 = 0;
+    bfx::check(bfx_get_frontier_mapping(ws, &layout0, 0, nullptr));
+    const bfx::SetKey key = bfx::set_key(stats, count, batches, layout0);
+    bool set_cached = false;
+    bfx::SetChoice set_choice{kPlain, layout0};
+    {
+      std::lock_guard<std::mutex> lock(bfx::g_tune_mutex);
+      const auto it = bfx::g_set_cache.find(key);
+      if (it != bfx::g_set_cache.end()) {
+        set_cached = true;
+        set_choice = it->second;
+      }
+    }
     const float steps[] = {kPlain, 0.5f * w, 1.0f * w, 2.0f * w, 4.0f * w, 8.0f * w, 32.0f * w, 128.0f * w};
     bfx::check(bfx_prepare_batches(ws, count, batches));
     o.engine = BFX_ENGINE_FRONTIER_PUSH;
     float best_step = kPlain, best_set = 0.0f;
-    for (std::size_t i = 0; i < sizeof(steps) / sizeof(steps[0]); ++i) {
-      const std::vector<float> d(count, steps[i]);
+    if (set_cached) {
+      best_step = set_choice.step;
+      const std::vector<float> d(count, best_step);
       bfx::check(bfx_set_batch_deltas(ws, count, d.data()));
-      const float t = bfx::time_set(ws, o, trials);
-      if (i == 0 || t < best_set) {
-        best_set = t;
-        best_step = steps[i];
+      best_set = bfx::time_set(ws, o, trials);
+    } else {
+      for (std::size_t i = 0; i < sizeof(steps) / sizeof(steps[0]); ++i) {
+        const std::vector<float> d(count, steps[i]);
+        bfx::check(bfx_set_batch_deltas(ws, count, d.data()));
+        const float t = bfx::time_set(ws, o, trials);
+        if (i == 0 || t < best_set) {
+          best_set = t;
+          best_step = steps[i];
+        }
       }
     }
 
@@ -189,17 +243,25 @@ extern "C" int bfx_autotune(bfx_workspace* ws, uint32_t count, const bfx_batch_d
       bfx_gpu_run_options oa = o;
       oa.engine = BFX_ENGINE_AUTO;
       bfx::check(bfx_set_batch_mappings(ws, 0, nullptr));
-      const float t_here = bfx::time_set(ws, oa, trials);
-      const std::uint32_t other = layout == BFX_FRONTIER_CHUNKED ? BFX_FRONTIER_TILED : BFX_FRONTIER_CHUNKED;
-      bfx::check(bfx_set_frontier_layout(ws, other));
-      const float t_other = bfx::time_set(ws, oa, trials);
-      if (t_other < t_here) {
-        layout = other;
-      } else {
+      float t_visits = 0.0f;
+      if (set_cached) {
+        // the class's layout, timed once (the baseline of the mapping mix)
+        layout = set_choice.layout;
         bfx::check(bfx_set_frontier_layout(ws, layout));
+        if (layout == BFX_FRONTIER_TILED) t_visits = bfx::time_set(ws, oa, trials);
+      } else {
+        const float t_here = bfx::time_set(ws, oa, trials);
+        const std::uint32_t other = layout == BFX_FRONTIER_CHUNKED ? BFX_FRONTIER_TILED : BFX_FRONTIER_CHUNKED;
+        bfx::check(bfx_set_frontier_layout(ws, other));
+        const float t_other = bfx::time_set(ws, oa, trials);
+        if (t_other < t_here) {
+          layout = other;
+        } else {
+          bfx::check(bfx_set_frontier_layout(ws, layout));
+        }
+        t_visits = std::min(t_here, t_other);
       }
       if (layout == BFX_FRONTIER_TILED) {
-        const float t_visits = std::min(t_here, t_other);
         std::vector<std::uint32_t> mappings(count, BFX_MAPPING_TILE_VISITS);
         bool any_chunks = false;
         for (std::uint32_t b = 0; b < count; ++b) {
@@ -239,6 +301,10 @@ extern "C" int bfx_autotune(bfx_workspace* ws, uint32_t count, const bfx_batch_d
         }
       }
     }
+    {
+      std::lock_guard<std::mutex> lock(bfx::g_tune_mutex);
+      bfx::g_set_cache[key] = bfx::SetChoice{best_step, layout};
+    }
     if (measured) *measured = n_measured;
   });
 }
@@ -248,6 +314,7 @@ extern "C" int bfx_autotune_reset(void) {
     std::lock_guard<std::mutex> lock(bfx::g_tune_mutex);
     bfx::g_tune_cache.clear();
     bfx::g_mapping_cache.clear();
+    bfx::g_set_cache.clear();
   });
 }
 
