@@ -6,6 +6,7 @@
 #pragma once
 
 #include "bfx.h"
+#include "bfx_internal.hpp"
 
 #include <algorithm>
 #include <cstdint>
@@ -38,35 +39,51 @@ struct RegionIndex {
   }
 };
 
+// Built per source tile in parallel: a tile's vertices are one contiguous
+// span (the layout orders vertices by tile), and their CSR runs name the
+// destination tiles; the (destination tile, edge count) pairs of a tile are
+// merged in a small sorted list.
 inline RegionIndex make_region_index(const bfx_device_graph_layout32& g) {
   RegionIndex r;
   r.T = g.tile_count;
   r.vertex_counts.assign(r.T, 0U);
   for (std::uint32_t v = 0; v < g.vertex_count; ++v) ++r.vertex_counts[g.owner_tiles[v]];
+  std::vector<std::uint32_t> first(r.T + 1, 0U);
+  for (std::uint32_t t = 0; t < r.T; ++t) first[t + 1] = first[t] + static_cast<std::uint32_t>(r.vertex_counts[t]);
   std::vector<std::vector<std::pair<std::uint32_t, std::uint64_t>>> per(r.T);
-  for (std::uint32_t v = 0; v < g.vertex_count; ++v) {
-    const std::uint32_t st = g.owner_tiles[v];
-    for (std::uint32_t run = g.csr_row_run_offsets[v]; run < g.csr_row_run_offsets[v + 1]; ++run) {
-      per[st].emplace_back(g.csr_run_destination_tiles[run],
+  parallel_for(r.T, 0, [&](std::uint64_t tb, std::uint64_t te) {
+    std::vector<std::pair<std::uint32_t, std::uint64_t>> lst;
+    for (std::uint64_t t = tb; t < te; ++t) {
+      lst.clear();
+      for (std::uint32_t v = first[t]; v < first[t + 1]; ++v) {
+        for (std::uint32_t run = g.csr_row_run_offsets[v]; run < g.csr_row_run_offsets[v + 1]; ++run) {
+          lst.emplace_back(g.csr_run_destination_tiles[run],
                            g.csr_run_edge_offsets[run + 1] - g.csr_run_edge_offsets[run]);
-    }
-  }
-  r.adj_offsets.assign(r.T + 1, 0U);
-  for (std::uint32_t t = 0; t < r.T; ++t) {
-    auto& lst = per[t];
-    std::sort(lst.begin(), lst.end());
-    std::vector<std::pair<std::uint32_t, std::uint64_t>> merged;
-    for (const auto& p : lst) {
-      if (!merged.empty() && merged.back().first == p.first) {
-        merged.back().second += p.second;
-      } else {
-        merged.push_back(p);
+        }
+      }
+      std::sort(lst.begin(), lst.end());
+      auto& merged = per[t];
+      for (const auto& q : lst) {
+        if (!merged.empty() && merged.back().first == q.first) {
+          merged.back().second += q.second;
+        } else {
+          merged.push_back(q);
+        }
       }
     }
-    r.adj_offsets[t + 1] = r.adj_offsets[t] + static_cast<std::uint32_t>(merged.size());
-    for (const auto& p : merged) {
-      r.adj_tiles.push_back(p.first);
-      r.adj_edges.push_back(p.second);
+  });
+  r.adj_offsets.assign(r.T + 1, 0U);
+  for (std::uint32_t t = 0; t < r.T; ++t) {
+    r.adj_offsets[t + 1] = r.adj_offsets[t] + static_cast<std::uint32_t>(per[t].size());
+  }
+  r.adj_tiles.resize(r.adj_offsets[r.T]);
+  r.adj_edges.resize(r.adj_offsets[r.T]);
+  for (std::uint32_t t = 0; t < r.T; ++t) {
+    std::uint32_t k = r.adj_offsets[t];
+    for (const auto& q : per[t]) {
+      r.adj_tiles[k] = q.first;
+      r.adj_edges[k] = q.second;
+      ++k;
     }
   }
   return r;
