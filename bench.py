@@ -318,6 +318,8 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
     ws.set_relax_atomic(args.amin)
     ws.set_flat_order(args.edge_major)
     ws.set_chunk_pairs(args.pairs)
+    if args.pack is not None:
+        ws.set_chunk_pack(args.pack)
     engine_id = {"auto": bfx.ENGINE_AUTO, "frontier": bfx.ENGINE_FRONTIER_PUSH, "jacobi": bfx.ENGINE_JACOBI_PULL,
                  "dense": bfx.ENGINE_DENSE_CHAOTIC_PUSH}[args.engine]
     mean_w = float(np.mean(wl.layout.arrays["csr_weights"]))
@@ -519,6 +521,7 @@ def measure(wl, args, *, rank, world, dist, device, steps, warmup, shard=False, 
                                           if frontier_used == "tiled" else 0),
                    "registers": eff_regs, "flat_items": args.items,
                    "returning_min": args.amin, "edge_major": args.edge_major, "chunk_pairs": args.pairs,
+                   "chunk_pack": ws.chunk_pack(),
                    "engines_chosen": None if engines_chosen is None else
                    {name: engines_chosen.count(e) for e, name in ((0, "jacobi"), (1, "dense"), (2, "frontier"))},
                    "control": "persistent_cooperative",
@@ -606,6 +609,8 @@ def main():
                     help="flat/chunked work order: 1 = entry, edge, lane")
     ap.add_argument("--pairs", type=int, default=0, choices=[0, 1],
                     help="chunked frontier: 1 = one (vertex, lane) pair per thread")
+    ap.add_argument("--pack", type=int, default=None, choices=[1, 2, 4, 8],
+                    help="chunked frontier: chunk slots per warp item (default: the library's)")
     ap.add_argument("--step", type=float, default=None,
                     help="with --engine frontier: near/far threshold step in mean edge weights (0 = plain frontier)")
     ap.add_argument("--tune-policy", action="store_true",

@@ -641,6 +641,15 @@ class Workspace:
         """Chunked layout: 0 work list, 1 (vertex, lane) pair per thread (persistent control)."""
         _check(load().bfx_set_chunk_pairs(self._h, u32(mode)))
 
+    def set_chunk_pack(self, pack: int):
+        """Chunk slots per warp item of the chunked layout (1, 2, 4 or 8)."""
+        _check(load().bfx_set_chunk_pack(self._h, u32(pack)))
+
+    def chunk_pack(self) -> int:
+        out = u32()
+        _check(load().bfx_get_chunk_pack(self._h, C.byref(out)))
+        return int(out.value)
+
     def set_flat_order(self, edge_major: int):
         """Flat/chunked work order: 0 entry-lane-edge, 1 entry-edge-lane."""
         _check(load().bfx_set_flat_order(self._h, u32(edge_major)))

@@ -1,15 +1,16 @@
 // Per-batch engine autotuner (a bfx component; the reference's engine
 // shootout, src/engine_shootout.cpp, only catalogues configurations).
 //
-// Three phases, all timed on the device with the library's own CUDA events
+// Five phases, all timed on the device with the library's own CUDA events
 // around the relaxation launch (best of `trials`):
 //  1. In context: the whole set on frontier push with one near/far step for
 //     every batch -- plain, and 1/2, 1, 2, 4, 8, 32, 128 mean edge weights -- as it
 //     will run, in one launch; the fastest step wins.  (A batch timed alone
 //     favours few rounds; in one launch with others the work matters.)  The
-//     step and the phase-4 layout are cached per set class (graph, magnitudes
-//     of the batch count per lane width and of the union size), so a later
-//     query set of the same class skips both searches.
+//     step, the phase-4 layout and the phase-5 pack are cached per set
+//     class (graph, magnitudes of the batch count per lane width and of the
+//     union size), so a later query set of the same class skips those
+//     searches.
 //  2. Per batch shape: Jacobi pull or dense chaotic push replaces frontier
 //     push only where it is at least 1.5x faster on the batch alone.  Cached
 //     by batch signature -- lane width, valid lanes, and the binary
@@ -23,6 +24,9 @@
 //     warp items (timed alone, visits only where 1.1x faster; cached by
 //     signature), the per-batch mix kept only if the whole set runs faster
 //     than all-visits.
+//  5. With either of those layouts: in context, 2, 4 or 8 chunk slots per
+//     warp item, the fastest kept (cached per set class with the step and
+//     the layout).
 // The set is left prepared with its per-batch engines, steps and mappings, so
 // an execute with engine == BFX_ENGINE_AUTO runs each batch on its own engine
 // and mapping inside one launch.
@@ -63,6 +67,7 @@ using SetKey = std::tuple<std::uint64_t, std::uint32_t, std::uint32_t, std::uint
 struct SetChoice {
   float step;           // phase 1
   std::uint32_t layout; // phase 4 (frontier layout kept)
+  std::uint32_t pack;   // phase 5 (chunk slots per warp item)
 };
 std::map<SetKey, SetChoice> g_set_cache;
 
@@ -92,8 +97,11 @@ SetKey set_key(const double stats[2], std::uint32_t count, const bfx_batch_descr
   const float mean = static_cast<float>(stats[0]);
   std::uint32_t mean_bits;
   std::memcpy(&mean_bits, &mean, 4);
+  // the chunked and tiled layouts are one family: phase 4 chooses between
+  // them whichever the search starts from
+  const std::uint32_t family = layout == BFX_FRONTIER_TILED ? static_cast<std::uint32_t>(BFX_FRONTIER_CHUNKED) : layout;
   return {static_cast<std::uint64_t>(stats[1]) << 32 | mean_bits, log2u(count), log2u(by_width[0]),
-          log2u(by_width[1]), log2u(by_width[2]), log2u(by_width[3]), log2u(union_vertices), layout, 0U};
+          log2u(by_width[1]), log2u(by_width[2]), log2u(by_width[3]), log2u(union_vertices), family, 0U};
 }
 
 }  // namespace
@@ -139,7 +147,7 @@ extern "C" int bfx_autotune(bfx_workspace* ws, uint32_t count, const bfx_batch_d
     bfx::check(bfx_get_frontier_mapping(ws, &layout0, 0, nullptr));
     const bfx::SetKey key = bfx::set_key(stats, count, batches, layout0);
     bool set_cached = false;
-    bfx::SetChoice set_choice{kPlain, layout0};
+    bfx::SetChoice set_choice{kPlain, layout0, 4U};
     {
       std::lock_guard<std::mutex> lock(bfx::g_tune_mutex);
       const auto it = bfx::g_set_cache.find(key);
@@ -236,8 +244,9 @@ extern "C" int bfx_autotune(bfx_workspace* ws, uint32_t count, const bfx_batch_d
     bfx::check(bfx_set_batch_deltas(ws, count, deltas.data()));
 
     // Phase 4: the work mapping.
-    std::uint32_t layout = 0;
+    std::uint32_t layout = 0, pack = 0;
     bfx::check(bfx_get_frontier_mapping(ws, &layout, 0, nullptr));
+    bfx::check(bfx_get_chunk_pack(ws, &pack));
     if ((layout == BFX_FRONTIER_CHUNKED || layout == BFX_FRONTIER_TILED) &&
         o.control_mode == BFX_CONTROL_PERSISTENT_COOPERATIVE && (o.block_size == 256 || o.block_size == 384)) {
       bfx_gpu_run_options oa = o;
@@ -300,10 +309,28 @@ extern "C" int bfx_autotune(bfx_workspace* ws, uint32_t count, const bfx_batch_d
           if (bfx::time_set(ws, oa, trials) >= t_visits) bfx::check(bfx_set_batch_mappings(ws, 0, nullptr));
         }
       }
+      // Phase 5, in context: chunk slots per warp item, 2, 4 or 8 (the
+      // class's choice when cached).
+      if (set_cached) {
+        pack = set_choice.pack;
+        bfx::check(bfx_set_chunk_pack(ws, pack));
+      } else {
+        float t_best = bfx::time_set(ws, oa, trials);
+        for (const std::uint32_t k : {2U, 4U, 8U}) {
+          if (k == pack) continue;
+          bfx::check(bfx_set_chunk_pack(ws, k));
+          const float t = bfx::time_set(ws, oa, trials);
+          if (t < t_best) {
+            t_best = t;
+            pack = k;
+          }
+        }
+        bfx::check(bfx_set_chunk_pack(ws, pack));
+      }
     }
     {
       std::lock_guard<std::mutex> lock(bfx::g_tune_mutex);
-      bfx::g_set_cache[key] = bfx::SetChoice{best_step, layout};
+      bfx::g_set_cache[key] = bfx::SetChoice{best_step, layout, pack};
     }
     if (measured) *measured = n_measured;
   });

@@ -87,16 +87,76 @@ __device__ __forceinline__ u32 lane_of_position(const u32* offsets, u32 W, u32 p
   return lo;
 }
 
-// Block-wide exclusive scan of per-batch values into smem prefix[0..nb].
+// Values of per-batch work that a round may pack: the chunk slots of a
+// chunked near round carry this flag; their warp items are the slots
+// divided by the round's pack (round_pack).
+constexpr u32 kPackable = 0x80000000u;
+
+// Chunk slots per warp item of the current round, set by block_prefix.
+__shared__ u32 s_round_pack;
+
+// Block-wide exclusive scan of per-batch work items into smem
+// prefix[0..nb].  Each value is computed once (four batches per iteration,
+// so their loads are in flight together) and parked in prefix[b].  Values
+// flagged kPackable are chunk slots: the round's pack is the largest power
+// of two up to `kmax` that still leaves at least two warp items per warp of
+// the grid (slots / pack + the other items), so packing never starves the
+// grid of items on a small frontier; the flagged slots then become
+// ceil(slots / pack) items.  The second pass replaces each value by its
+// exclusive sum.  Every block computes the same result from the same
+// counters.
 template <typename F>
-__device__ void block_prefix(u32* prefix, u32 nb, F value) {
+__device__ void block_prefix(u32* prefix, u32 nb, F value, u32 kmax = 1u) {
   __shared__ u32 s_warp[33];
+  __shared__ u64 s_tot[2][32];
   const u32 per = (nb + blockDim.x - 1) / blockDim.x;
   const u32 begin = threadIdx.x * per;
+  const u32 warp = threadIdx.x >> 5;
+  u64 slots = 0, other = 0;
+#pragma unroll 4
+  for (u32 i = 0; i < per; ++i) {
+    const u32 b = begin + i;
+    if (b < nb) {
+      const u32 x = value(b);
+      prefix[b] = x;
+      if (x & kPackable) {
+        slots += x & ~kPackable;
+      } else {
+        other += x;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    slots += __shfl_down_sync(0xFFFFFFFFu, slots, o);
+    other += __shfl_down_sync(0xFFFFFFFFu, other, o);
+  }
+  if (lane_id() == 0) {
+    s_tot[0][warp] = slots;
+    s_tot[1][warp] = other;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    u64 S = 0, O = 0;
+    for (u32 w = 0; w < (blockDim.x >> 5); ++w) {
+      S += s_tot[0][w];
+      O += s_tot[1][w];
+    }
+    const u64 want = 2ull * gridDim.x * (blockDim.x >> 5);
+    u32 k = kmax;
+    while (k > 1u && S / k + O < want) k >>= 1;
+    s_round_pack = k;
+  }
+  __syncthreads();
+  const u32 k = s_round_pack;
   u32 local = 0;
   for (u32 i = 0; i < per; ++i) {
     const u32 b = begin + i;
-    if (b < nb) local += value(b);
+    if (b < nb) {
+      u32 x = prefix[b];
+      if (x & kPackable) x = ((x & ~kPackable) + k - 1u) / k;
+      prefix[b] = x;
+      local += x;
+    }
   }
   // inclusive warp scan
   u32 x = local;
@@ -104,7 +164,6 @@ __device__ void block_prefix(u32* prefix, u32 nb, F value) {
     const u32 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
     if (lane_id() >= o) x += y;
   }
-  const u32 warp = threadIdx.x >> 5;
   if (lane_id() == 31) s_warp[warp] = x;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -122,8 +181,9 @@ __device__ void block_prefix(u32* prefix, u32 nb, F value) {
   for (u32 i = 0; i < per; ++i) {
     const u32 b = begin + i;
     if (b < nb) {
+      const u32 y = prefix[b];
       prefix[b] = run;
-      run += value(b);
+      run += y;
     }
   }
   if (threadIdx.x == 0) prefix[nb] = s_warp[32];
@@ -371,22 +431,37 @@ __device__ __forceinline__ u32 batch_exec(const LaunchParams& p, u32 b, u32 ridx
   return p.per_lane ? ch : (ch != 0u ? p.batches[b].valid : 0u);
 }
 
+// Far pile size of the batch's current generation: the three pile counters
+// and the generation are read together (one dependent step, not two).
+__device__ __forceinline__ u32 current_far_count(const DCtl& C, u32 r) {
+  const u32 g = dev::ld_cg(&C.gen[r & 1u]) % 3u;
+  const u32 f0 = dev::ld_cg(&C.fcount[0]), f1 = dev::ld_cg(&C.fcount[1]), f2 = dev::ld_cg(&C.fcount[2]);
+  return g == 0u ? f0 : (g == 1u ? f1 : f2);
+}
+
 __device__ u32 round_work(const LaunchParams& p, u32 r, u32* prefix) {
   const u32 ridx = r % 3u;
   block_prefix(prefix, p.nb, [&](u32 b) {
     const DBatch& B = p.batches[b];
-    if (engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH) {
-      const DCtl& C = p.ctl[b];
-      const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
-      if (n != 0u) {  // warp items: one chunk (chunked), flat_entries_per_item(n) entries (flat), 4 or 1 entries
-        if (p.flat >= 2u) return chunk_items(n, B.U, 5u);
+    const DCtl& C = p.ctl[b];
+    // every counter the batch's item count can depend on, loaded up front
+    const u32 eng = engine_of(p, b);
+    const u32 count = dev::ld_cg(&C.count[ridx]);
+    const u32 changed = dev::ld_cg(&C.changed[ridx]);
+    const u32 far = current_far_count(C, r);
+    const u32 U = B.U;
+    if (eng == BFX_ENGINE_FRONTIER_PUSH) {
+      const u32 n = min(count, U);
+      if (n != 0u) {  // warp items: a pack of chunks (chunked), flat_entries_per_item(n) entries (flat), 4 or 1 entries
+        if (p.flat >= 2u) return chunk_slots(n, U) | kPackable;
         return p.flat ? (n + flat_entries_per_item(n) - 1u) / flat_entries_per_item(n) : (B.W <= 8u ? (n + 3u) >> 2 : n);
       }
-      const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
-      return (f + 31u) >> 5;  // split round: 32 far entries per warp item
+      const u32 f = min(far, U);
+      return (f + kSplitPerItem - 1u) / kSplitPerItem;  // split round: kSplitPerItem far entries per warp item
     }
-    return batch_exec(p, b, ridx) != 0u ? (((B.U << B.shift) + 31u) >> 5) : 0u;
-  });
+    const u32 exec = eng == BFX_ENGINE_JACOBI_PULL || !p.per_lane ? (changed != 0u ? B.valid : 0u) : changed;
+    return exec != 0u ? (((U << B.shift) + 31u) >> 5) : 0u;
+  }, p.flat >= 2u ? p.cpack : 1u);
   return prefix[p.nb];
 }
 
@@ -405,6 +480,7 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
   __shared__ u32 s_next_item;
   const u32 ridx = r % 3u, widx = (r + 1u) % 3u;
   const u32 total = prefix[p.nb];
+  const u32 pack = s_round_pack;  // chunk slots per warp item of this round (round_work)
   Stages st{{0u, 0u}, 0xFFFFFFFFu};
   u32 staged_batch = 0xFFFFFFFFu;
   if (threadIdx.x == 0u) s_next_item = 0u;
@@ -456,15 +532,10 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
       }
       if (n != 0u) {
         if (kChunked) {
-          u32 chunk = kNoChunk;  // sparse round: the item's queue word names the chunk
-          if (chunk_dense(n, V.U, 5u)) {
-            // dense round: the item is chunk slot `item`; clear bit, no work
-            // (every lane reads the same word, so the skip is warp-uniform)
-            const u32 word = dev::ld_cg(V.cmask_r + (item >> 5));
-            if (((word >> (item & 31u)) & 1u) == 0u) continue;
-            chunk = item;
-          }
-          frontier_flat<kCount, kItems, true, kPairs>(p, V, C, item, n, 32u, tau, st, wk, chunk);
+          // a pack of queue words (sparse round) or of chunk slots in index
+          // order (dense round)
+          frontier_flat<kCount, kItems, true, kPairs>(p, V, C, item, n, 32u, tau, st, wk, chunk_dense(n, V.U, 5u),
+                                                      pack);
         } else if (p.flat) {
           frontier_flat<kCount, kItems, false>(p, V, C, item, n, flat_entries_per_item(n), tau, st, wk);
         } else if (B.W <= 8u) {
@@ -486,20 +557,26 @@ __device__ void round_body(const LaunchParams& p, u32 r, const u32* prefix, Work
   stages_flush(st);
 }
 
-// Bookkeeping at the start of round r, done by one thread: rounds counter
-// per batch, clear the rotating slot that round r+1 will write.
+// Bookkeeping at the start of round r, done by block 0 (threads striding
+// over the batches): rounds counter per batch, clear the rotating slot that
+// round r+1 will write.  A batch's counters are loaded together before any
+// of them is used.
 __device__ void round_bookkeeping(const LaunchParams& p, u32 r) {
   const u32 ridx = r % 3u, zidx = (r + 2u) % 3u;
+#pragma unroll 4
   for (u32 b = threadIdx.x; b < p.nb; b += blockDim.x) {
     DCtl& C = p.ctl[b];
     bool work;
-    if (engine_of(p, b) == BFX_ENGINE_FRONTIER_PUSH) {
+    const u32 eng = engine_of(p, b);
+    const u32 g = dev::ld_cg(&C.gen[r & 1u]);
+    const u32 tau = dev::ld_cg(&C.tau[r & 1u]);
+    const u32 count = dev::ld_cg(&C.count[ridx]);
+    const u32 far = current_far_count(C, r);
+    if (eng == BFX_ENGINE_FRONTIER_PUSH) {
       // near round, split round (near frontier empty, far pile not), or idle;
       // generation and threshold of round r+1 go to the other parity slot.
-      const u32 g = dev::ld_cg(&C.gen[r & 1u]);
-      const u32 tau = dev::ld_cg(&C.tau[r & 1u]);
-      const bool near = dev::ld_cg(&C.count[ridx]) != 0u;
-      const bool split = !near && dev::ld_cg(&C.fcount[g % 3u]) != 0u;
+      const bool near = count != 0u;
+      const bool split = !near && far != 0u;
       work = near || split;
       if (split) {
         C.fcount[(g + 2u) % 3u] = 0u;  // idle since two splits ago; the next split writes it
@@ -1813,6 +1890,7 @@ void execute(bfx_workspace* ws, const bfx_gpu_run_options& o) {
   p.deltas = nullptr;
   p.flat = ws->frontier_layout == BFX_FRONTIER_FLAT ? 1u : (ws->frontier_layout == BFX_FRONTIER_CHUNKED ? 2u : 0u);
   p.cshift = 5u;
+  p.cpack = ws->chunk_pack;
   p.tile_stage_min = ws->tile_stage_min;
   p.tile_iters = ws->tile_iters;
   p.tile_wmax = 1u;
@@ -1987,6 +2065,21 @@ int bfx_set_register_budget(bfx_workspace* ws, uint32_t registers) {
     bfx::require(registers == 0u || registers == 40u || registers == 64u || registers == 80u,
                  "register budget must be 0 (automatic), 40, 64 or 80");
     ws->register_budget = registers;
+  });
+}
+
+int bfx_set_chunk_pack(bfx_workspace* ws, uint32_t pack) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr, "null argument");
+    bfx::require(pack == 1u || pack == 2u || pack == 4u || pack == 8u, "chunk pack must be 1, 2, 4 or 8");
+    ws->chunk_pack = pack;
+  });
+}
+
+int bfx_get_chunk_pack(bfx_workspace* ws, uint32_t* pack) {
+  return bfx::guarded([&] {
+    bfx::require(ws != nullptr && pack != nullptr, "null argument");
+    *pack = ws->chunk_pack;
   });
 }
 

@@ -154,7 +154,8 @@ struct LaunchParams {
   u32 amin;              // flat frontier: 1 = returning min per relaxation, 0 = pre-read + min on success
   u32 edge_major;        // flat frontier work order: 1 = entry, edge, lane; 0 = entry, lane, edge
   u32 cshift;            // chunked / tiled layouts: a claim unit is 2^cshift consecutive compact vertices
-                         // (5 for the chunked layout; the tile size for the tiled one)
+                         // (5: 32-vertex chunks)
+  u32 cpack;             // chunked / tiled layouts: chunk slots per warp item (1, 2, 4 or 8)
   u32 tile_stage_min;    // tiled layout: lane-edge work below which a block visit relaxes in place (no staging)
   u32 tile_wmax;         // tiled layout: widest batch of the launch (sizes the staged label rows)
   u32 tile_iters;        // tiled layout: local relaxation passes per visit before the rest waits a round
@@ -288,6 +289,7 @@ struct bfx_workspace {
   std::uint32_t relax_atomic = 0;            // flat frontier relaxation: 0 pre-read + min, 1 returning min
   std::uint32_t edge_major = 0;              // flat frontier work order (see bfx_set_flat_order)
   std::uint32_t chunk_pairs = 0;             // chunked frontier pair mode (see bfx_set_chunk_pairs)
+  std::uint32_t chunk_pack = 4;              // chunk slots per warp item (see bfx_set_chunk_pack)
   std::uint32_t flat_items = 2;              // flat layout: work items per thread per iteration (2..4)
   std::uint32_t register_budget = 0;         // persistent kernel registers per thread: 0 automatic, 40, 64, 80
   std::uint32_t tile_stage_min = 1024;       // tiled layout: lane-edge work from which a visit stages its labels

@@ -289,92 +289,144 @@ __device__ __forceinline__ void frontier_group(const LaunchParams& p, const Fron
 // so the threshold advances (split_threshold) and every parked (vertex, lane) of the
 // current far pile is re-examined: lanes whose label is now below the new
 // threshold join the next round's near frontier, the rest move to the next
-// pile.  One thread per far entry; claims are warp-aggregated.  The batch
-// runs no near round in the same round, so the far masks it reads are
-// stable and are cleared with plain stores.
+// pile.  The batch runs no near round in the same round, so the far masks it
+// reads are stable and are cleared with plain stores.
+//
+// A warp item covers kSplitPerItem (256) pile entries, eight per thread: the
+// eight entries' pile words, far masks and bounds are loaded together, and
+// the entries that stay parked whole (bound not below the new threshold) --
+// usually most of the pile -- are appended to the next pile with one counter
+// atomic for the item and plain stores, so a pile of millions of entries
+// does not serialise on its counter.  The other entries re-read their parked
+// labels; their claims are warp-aggregated through the stages.
+constexpr u32 kSplitPer = 8u;
+constexpr u32 kSplitPerItem = 32u * kSplitPer;
+
 template <bool kCount, bool kChunked>
 __device__ __forceinline__ void split_group(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
                                             u32 tau_next, Stages& st, Work& wk) {
   const u32 lane = lane_id();
-  const u32 entry = item * 32u + lane;
-  u32 near = 0u, far = 0u, v = 0u, cv = 0u, fd = 0xFFFFFFFFu;
-  bool claim_far = false;  // the entry is re-parked unread (its far mask stays set)
-  if (entry < count) {
-    const u64 q = dev::ld_cg(B.pile + entry);
-    v = static_cast<u32>(q);
-    cv = static_cast<u32>(q >> 32);
-    u32 bits = 0u, bound = 0xFFFFFFFFu;
-    if (cv < B.U) {
-      bits = dev::ld_cg(B.fmask + cv) & B.valid;
-      bound = dev::ld_cg(B.fbound + cv);
-    } else {
-      atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
-    }
-    // Every parked label of the vertex is at least `bound` (each far
-    // improvement lowers it; a split stores the exact minimum of the lanes
-    // it re-parks).  When the bound is finite and not below the new
-    // threshold, all lanes stay parked: the entry moves to the next pile
-    // unread and its far mask stays set.
-    const bool stays = bits != 0u && bound < dev::kInfBits && bound >= tau_next;
-    if (stays) {
-      far = bits;
-      fd = bound;
-    } else if (cv < B.U) {
-      B.fmask[cv] = 0u;
-    }
-    // Parked lanes are re-read eight at a time: the eight label loads are
-    // issued back to back, so an entry with k far lanes waits ceil(k / 8)
-    // memory latencies instead of k.
-    u64* const row = B.dist + (static_cast<u64>(cv) << B.shift);
-    for (u32 rest = stays ? 0u : bits; rest != 0u;) {
-      u32 ls[8], ds[8];
+  const u32 below = (1u << lane) - 1u;
+  u64 q[kSplitPer];
+  u32 bits[kSplitPer], bound[kSplitPer];
 #pragma unroll
-      for (u32 i = 0; i < 8u; ++i) {
-        ls[i] = rest != 0u ? static_cast<u32>(__ffs(rest)) - 1u : 32u;
-        rest &= rest - 1u;
+  for (u32 j = 0; j < kSplitPer; ++j) {
+    const u32 entry = item * kSplitPerItem + j * 32u + lane;
+    q[j] = entry < count ? dev::ld_cg(B.pile + entry) : ~u64{0};
+  }
+#pragma unroll
+  for (u32 j = 0; j < kSplitPer; ++j) {
+    bits[j] = 0u;
+    bound[j] = 0xFFFFFFFFu;
+    const u32 cv = static_cast<u32>(q[j] >> 32);
+    if (q[j] != ~u64{0}) {
+      if (cv < B.U) {
+        bits[j] = dev::ld_cg(B.fmask + cv) & B.valid;
+        bound[j] = dev::ld_cg(B.fbound + cv);
+      } else {
+        atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
+        q[j] = ~u64{0};
       }
+    }
+  }
+  // Every parked label of a vertex is at least its bound (each far
+  // improvement lowers it; a split stores the exact minimum of the lanes it
+  // re-parks).  When the bound is finite and not below the new threshold,
+  // all lanes stay parked: the entry moves to the next pile unread and its
+  // far mask stays set.
+  u32 stay_mask = 0u, nstay = 0u, stay_rank[kSplitPer];
 #pragma unroll
-      for (u32 i = 0; i < 8u; ++i) ds[i] = ls[i] < 32u ? dev::hi(dev::ld_cg(row + ls[i])) : 0u;
+  for (u32 j = 0; j < kSplitPer; ++j) {
+    const bool stays = q[j] != ~u64{0} && bits[j] != 0u && bound[j] < dev::kInfBits && bound[j] >= tau_next;
+    const u32 bal = __ballot_sync(0xFFFFFFFFu, stays);
+    stay_rank[j] = nstay + static_cast<u32>(__popc(bal & below));
+    nstay += static_cast<u32>(__popc(bal));
+    if (stays) {
+      stay_mask |= 1u << j;
+      st.fd = min(st.fd, bound[j]);
+    }
+  }
+  if (nstay != 0u) {  // warp-uniform
+    const StageQueue sq = s_stage_queue[kFar][threadIdx.x >> 5];
+    u32 pos = 0u;
+    if (lane == 0u) pos = atomicAdd(sq.counter, nstay);
+    pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
 #pragma unroll
-      for (u32 i = 0; i < 8u; ++i) {
-        if (ls[i] < 32u) {
-          if (ds[i] < tau_next) {
-            near |= 1u << ls[i];
-          } else {
-            far |= 1u << ls[i];
-            fd = min(fd, ds[i]);
-          }
+    for (u32 j = 0; j < kSplitPer; ++j) {
+      if ((stay_mask >> j) & 1u) {
+        if (pos + stay_rank[j] < sq.cap) {
+          sq.queue[pos + stay_rank[j]] = q[j];
+        } else {
+          atomicOr(sq.err, static_cast<u32>(BFX_DEVICE_ERROR_QUEUE_OVERFLOW));
         }
       }
     }
-    // the bound of the lanes that stay parked (none: cleared)
-    if (!stays && cv < B.U) B.fbound[cv] = far != 0u ? fd : 0xFFFFFFFFu;
-    if (kCount) {
-      wk.c[0] += 1;
-      wk.c[11] += 1;
-      if (!stays) wk.c[12] += static_cast<u32>(__popc(bits));
-    }
-    claim_far = stays;
   }
-  // far lanes stay parked (next pile); near lanes join the next round
-  bool fclaim = claim_far, claim = false;
-  if (far != 0u && !claim_far) fclaim = atomicOr(B.fmask + cv, far) == 0u;
-  u64 qword = queue_word(v, cv);  // queue word: {vertex, compact index}, or the chunk (chunked layout)
-  if (near != 0u) {
-    if (kChunked) {
-      dev::red_or(B.mask_w + cv, near);
-      const u32 chunk = cv >> p.cshift;
-      const u32 bit = 1u << (chunk & 31u);
-      claim = (atomicOr(B.cmask_w + (chunk >> 5), bit) & bit) == 0u;
-      qword = chunk;
-    } else {
-      claim = atomicOr(B.mask_w + cv, near) == 0u;
+  if (kCount) {
+#pragma unroll
+    for (u32 j = 0; j < kSplitPer; ++j) {
+      if (q[j] != ~u64{0}) {
+        wk.c[0] += 1;
+        wk.c[11] += 1;
+        if (!((stay_mask >> j) & 1u)) wk.c[12] += static_cast<u32>(__popc(bits[j]));
+      }
     }
   }
-  st.fd = min(st.fd, fd);
-  stage_push(st, kFar, fclaim, queue_word(v, cv));
-  if (kCount && claim) wk.c[4] += 1;
-  stage_push(st, kNear, claim, qword);
+  // The other entries: their parked lanes are re-read eight at a time (the
+  // eight label loads issued back to back).
+#pragma unroll 1
+  for (u32 j = 0; j < kSplitPer; ++j) {
+    const bool go = q[j] != ~u64{0} && !((stay_mask >> j) & 1u);
+    if (!__any_sync(0xFFFFFFFFu, go)) continue;
+    const u32 v = static_cast<u32>(q[j]), cv = static_cast<u32>(q[j] >> 32);
+    u32 near = 0u, far = 0u, fd = 0xFFFFFFFFu;
+    if (go) {
+      B.fmask[cv] = 0u;
+      u64* const row = B.dist + (static_cast<u64>(cv) << B.shift);
+      for (u32 rest = bits[j]; rest != 0u;) {
+        u32 ls[8], ds[8];
+#pragma unroll
+        for (u32 i = 0; i < 8u; ++i) {
+          ls[i] = rest != 0u ? static_cast<u32>(__ffs(rest)) - 1u : 32u;
+          rest &= rest - 1u;
+        }
+#pragma unroll
+        for (u32 i = 0; i < 8u; ++i) ds[i] = ls[i] < 32u ? dev::hi(dev::ld_cg(row + ls[i])) : 0u;
+#pragma unroll
+        for (u32 i = 0; i < 8u; ++i) {
+          if (ls[i] < 32u) {
+            if (ds[i] < tau_next) {
+              near |= 1u << ls[i];
+            } else {
+              far |= 1u << ls[i];
+              fd = min(fd, ds[i]);
+            }
+          }
+        }
+      }
+      // the bound of the lanes that stay parked (none: cleared)
+      B.fbound[cv] = far != 0u ? fd : 0xFFFFFFFFu;
+    }
+    // far lanes stay parked (next pile); near lanes join the next round
+    bool fclaim = false, claim = false;
+    if (far != 0u) fclaim = atomicOr(B.fmask + cv, far) == 0u;
+    u64 qword = queue_word(v, cv);  // queue word: {vertex, compact index}, or the chunk (chunked layout)
+    if (near != 0u) {
+      if (kChunked) {
+        dev::red_or(B.mask_w + cv, near);
+        const u32 chunk = cv >> p.cshift;
+        const u32 bit = 1u << (chunk & 31u);
+        claim = (atomicOr(B.cmask_w + (chunk >> 5), bit) & bit) == 0u;
+        qword = chunk;
+      } else {
+        claim = atomicOr(B.mask_w + cv, near) == 0u;
+      }
+    }
+    st.fd = min(st.fd, fd);
+    stage_push(st, kFar, fclaim, queue_word(v, cv));
+    if (kCount && claim) wk.c[4] += 1;
+    stage_push(st, kNear, claim, qword);
+  }
 }
 
 // Entries per flat warp item for a batch frontier of n entries: 32 from 2,048
@@ -445,77 +497,41 @@ __device__ __forceinline__ FlatItem flat_decode(u32 w, u32 total, u32 incl, u32 
   return it;
 }
 
-// kChunked: the item is one queued 32-vertex chunk (compact indices
-// 32 c .. 32 c + 31) instead of `epi` queued vertices; successes set the
-// pending lane with a non-returning OR and claim the target's chunk through
-// the chunk bitmap.  The chunk is the item's queue word, or `chunk_in`
-// when the caller enumerates chunk slots (dense rounds, chunk_items); the
-// pending lanes and the compact row table {row begin, out-degree} of its 32
-// vertices are read together.
-// kPairs (chunked only): the warp walks the item's (entry, lane) pairs, one
+// kChunked: the item is a pack of `pack` (the round's pack, at most
+// LaunchParams::cpack and kPackMax) chunk slots -- in a sparse round consecutive queue words,
+// each naming a queued 32-vertex chunk (compact indices 32 c .. 32 c + 31);
+// in a dense round consecutive chunk slots in index order, of which only
+// those whose bit is set in the chunk bitmap are read.  The pending lanes
+// and the compact row table {row begin, out-degree} of each chunk's 32
+// vertices are read together (the next chunk's loads are issued before the
+// current one is compacted), and the vertices with pending lanes are
+// compacted into a per-warp ring in shared memory, so a work list covers up
+// to 32 active vertices of several chunks instead of the few a single chunk
+// holds.  Successes set the pending lane with a non-returning OR and claim
+// the target's chunk through the chunk bitmap.
+// kPairs (chunked only): the warp walks the group's (entry, lane) pairs, one
 // per thread, each over its entry's out-edges -- no per-edge decode.
 constexpr u32 kNoChunk = 0xFFFFFFFFu;
+constexpr u32 kPackMax = 8u;              // chunk slots per warp item, at most
+__shared__ uint4 s_pack[16][64];          // per warp: ring of {compact index, pending lanes, row begin, degree}
 
 // Chunked near round of a batch with n queued chunks: sparse rounds walk
 // the queue (claim order); once at least half of the batch's chunk slots are
 // pending, the items are all chunk slots in index order and a warp skips the
 // slots whose bit is clear.  Concurrent warps then relax neighbouring
 // chunks, whose target labels (intra-tile edges) are shared in the L2.
-// cshift: the claim unit is 2^cshift compact vertices (5: the chunked layout's
-// 32-vertex chunks; the tile size in the tiled layout).
+// cshift: the claim unit is 2^cshift compact vertices (5: 32-vertex chunks).
+// chunk_slots: the round's slots (queue words or chunk slots), of which a
+// warp item takes the round's pack.
 __device__ __forceinline__ u32 chunk_count(u32 U, u32 cshift) { return (U + (1u << cshift) - 1u) >> cshift; }
 __device__ __forceinline__ bool chunk_dense(u32 n, u32 U, u32 cshift) { return 2u * n >= chunk_count(U, cshift); }
-__device__ __forceinline__ u32 chunk_items(u32 n, u32 U, u32 cshift) {
-  return chunk_dense(n, U, cshift) ? chunk_count(U, cshift) : n;
-}
+__device__ __forceinline__ u32 chunk_slots(u32 n, u32 U) { return chunk_dense(n, U, 5u) ? chunk_count(U, 5u) : n; }
 
 template <bool kCount, u32 kItems, bool kChunked, bool kPairs = false>
 __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const FrontierView& B, DCtl& C, u32 item, u32 count,
-                                              u32 epi, u32 tau_bits, Stages& st, Work& wk, u32 chunk_in = kNoChunk) {
+                                              u32 epi, u32 tau_bits, Stages& st, Work& wk, bool dense = false,
+                                              u32 pack = 1u) {
   const u32 lane = lane_id();
-  const u32 entry = item * epi + lane;  // epi entries per item (a power of two <= 32)
-  u32 v = 0u, cv = 0u, m = 0u, rb = 0u, deg = 0u;
-  if (kChunked) {
-    const u32 chunk = chunk_in != kNoChunk ? chunk_in : static_cast<u32>(dev::ld_cg(B.queue_r + item));
-    if (chunk < (B.U + 31u) >> 5) {
-      cv = (chunk << 5) + lane;
-      if (cv < B.U) {
-        m = dev::ld_cg(B.mask_r + cv) & B.valid;
-        const uint2 row = __ldg(B.crow + cv);
-        if (m != 0u) {
-          rb = row.x;
-          deg = row.y;
-          B.mask_r[cv] = 0u;
-          if (kCount) {
-            wk.c[0] += 1;
-            wk.c[1] += deg;
-            wk.c[2] += __popc(m);
-          }
-        }
-      }
-      if (lane == 0u) atomicAnd(B.cmask_r + (chunk >> 5), ~(1u << (chunk & 31u)));
-    } else if (lane == 0u) {
-      atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
-    }
-  } else if (lane < epi && entry < count) {
-    const u64 q = dev::ld_cg(B.queue_r + entry);
-    v = static_cast<u32>(q);
-    cv = static_cast<u32>(q >> 32);
-    if (v < p.g.V && cv < B.U) {
-      m = dev::ld_cg(B.mask_r + cv) & B.valid;
-      rb = __ldg(p.g.csr_off + v);
-      deg = __ldg(p.g.csr_off + v + 1u) - rb;
-      B.mask_r[cv] = 0u;
-    } else {
-      atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
-      v = cv = 0u;
-    }
-    if (kCount) {
-      wk.c[0] += 1;
-      wk.c[1] += deg;
-      wk.c[2] += __popc(m);
-    }
-  }
   // Claims of the previous step: their pending-word and far-mask ORs stay
   // in flight while the next step decodes its items and issues its first
   // loads.  p_old / f_old == 0: the OR claimed the vertex (or its chunk).
@@ -627,68 +643,174 @@ __device__ __forceinline__ void frontier_flat(const LaunchParams& p, const Front
       }
     }
   };
-  if (kPairs) {
-    // Pair mode: each thread takes one (entry, lane) pair of the item and
-    // walks that entry's edges kItems per step; one source read per pair,
-    // no per-edge decode.
-    const u32 k = static_cast<u32>(__popc(m));
-    u32 kincl = k;
-    for (u32 o = 1; o < 32u; o <<= 1) {
-      const u32 y = __shfl_up_sync(0xFFFFFFFFu, kincl, o);
-      if (lane >= o) kincl += y;
-    }
-    const u32 kexcl = kincl - k;
-    const u32 pairs = __shfl_sync(0xFFFFFFFFu, kincl, 31);
-    for (u32 pbase = 0; pbase < pairs; pbase += 32u) {
-      const u32 pi = pbase + lane;
-      u32 e = 0u;
-      for (u32 s = 16u; s > 0u; s >>= 1) {
-        if (__shfl_sync(0xFFFFFFFFu, kincl, static_cast<int>(e + s - 1u)) <= pi) e += s;
+  // The work list of one group of up to 32 entries, one per thread
+  // (m == 0: no entry).
+  auto relax_entries = [&](const u32 cv, const u32 m, const u32 rb, const u32 deg) {
+    if (kPairs) {
+      // Pair mode: each thread takes one (entry, lane) pair of the item and
+      // walks that entry's edges kItems per step; one source read per pair,
+      // no per-edge decode.
+      const u32 k = static_cast<u32>(__popc(m));
+      u32 kincl = k;
+      for (u32 o = 1; o < 32u; o <<= 1) {
+        const u32 y = __shfl_up_sync(0xFFFFFFFFu, kincl, o);
+        if (lane >= o) kincl += y;
       }
-      const u32 ecv = __shfl_sync(0xFFFFFFFFu, cv, static_cast<int>(e));
-      const u32 em = __shfl_sync(0xFFFFFFFFu, m, static_cast<int>(e));
-      const u32 erb = __shfl_sync(0xFFFFFFFFu, rb, static_cast<int>(e));
-      const u32 edeg = __shfl_sync(0xFFFFFFFFu, deg, static_cast<int>(e));
-      const u32 eexcl = __shfl_sync(0xFFFFFFFFu, kexcl, static_cast<int>(e));
-      const bool plive = pi < pairs;
-      u32 pql = 0u, psrc = dev::kInfBits;
-      if (plive) {
-        u32 mm = em;
-        for (u32 t = 0; t < pi - eexcl; ++t) mm &= mm - 1u;
-        pql = __ffs(mm) - 1u;
-        psrc = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(ecv) << B.shift) + pql)));
+      const u32 kexcl = kincl - k;
+      const u32 pairs = __shfl_sync(0xFFFFFFFFu, kincl, 31);
+      for (u32 pbase = 0; pbase < pairs; pbase += 32u) {
+        const u32 pi = pbase + lane;
+        u32 e = 0u;
+        for (u32 s = 16u; s > 0u; s >>= 1) {
+          if (__shfl_sync(0xFFFFFFFFu, kincl, static_cast<int>(e + s - 1u)) <= pi) e += s;
+        }
+        const u32 ecv = __shfl_sync(0xFFFFFFFFu, cv, static_cast<int>(e));
+        const u32 em = __shfl_sync(0xFFFFFFFFu, m, static_cast<int>(e));
+        const u32 erb = __shfl_sync(0xFFFFFFFFu, rb, static_cast<int>(e));
+        const u32 edeg = __shfl_sync(0xFFFFFFFFu, deg, static_cast<int>(e));
+        const u32 eexcl = __shfl_sync(0xFFFFFFFFu, kexcl, static_cast<int>(e));
+        const bool plive = pi < pairs;
+        u32 pql = 0u, psrc = dev::kInfBits;
+        if (plive) {
+          u32 mm = em;
+          for (u32 t = 0; t < pi - eexcl; ++t) mm &= mm - 1u;
+          pql = __ffs(mm) - 1u;
+          psrc = dev::hi(dev::ld_cg(B.dist + ((static_cast<u64>(ecv) << B.shift) + pql)));
+        }
+        const u32 steps = __reduce_max_sync(0xFFFFFFFFu, plive ? edeg : 0u);
+        for (u32 s = 0; s < steps; s += kItems) {
+          FlatItem it[kItems];
+          u32 src[kItems];
+  #pragma unroll
+          for (u32 u = 0; u < kItems; ++u) {
+            it[u] = FlatItem{plive && s + u < edeg, pql, erb + s + u, ecv};
+            src[u] = psrc;
+          }
+          step(it, src, false);
+        }
       }
-      const u32 steps = __reduce_max_sync(0xFFFFFFFFu, plive ? edeg : 0u);
-      for (u32 s = 0; s < steps; s += kItems) {
+    } else {
+      const u32 work = static_cast<u32>(__popc(m)) * deg;
+      u32 incl = work;
+      for (u32 o = 1; o < 32u; o <<= 1) {
+        const u32 y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const u32 excl = incl - work;
+      const u32 total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+      for (u32 base = 0; base < total; base += 32u * kItems) {
         FlatItem it[kItems];
         u32 src[kItems];
-#pragma unroll
+  #pragma unroll
         for (u32 u = 0; u < kItems; ++u) {
-          it[u] = FlatItem{plive && s + u < edeg, pql, erb + s + u, ecv};
-          src[u] = psrc;
+          it[u] = flat_decode(base + 32u * u + lane, total, incl, excl, cv, m, rb, deg, p.edge_major != 0u);
+          src[u] = dev::kInfBits;
         }
-        step(it, src, false);
+        step(it, src, true);
       }
+    }
+  };
+  if (kChunked) {
+    // Pack: lane j < pack holds slot j's chunk (kNoChunk: none).
+    const u32 K = pack;
+    const u32 nchunks = chunk_count(B.U, 5u);
+    const u32 s0 = item * K;
+    u32 my_chunk = kNoChunk;
+    if (lane < K) {
+      const u32 s = s0 + lane;
+      if (dense) {
+        if (s < nchunks && ((dev::ld_cg(B.cmask_r + (s >> 5)) >> (s & 31u)) & 1u) != 0u) my_chunk = s;
+      } else if (s < count) {
+        my_chunk = static_cast<u32>(dev::ld_cg(B.queue_r + s));
+        if (my_chunk >= nchunks) {
+          atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
+          my_chunk = kNoChunk;
+        }
+      }
+    }
+    u32 rest = __ballot_sync(0xFFFFFFFFu, my_chunk != kNoChunk);
+    if (rest == 0u) return;  // warp-uniform: no slot of the pack is pending
+    // the read slot's chunk bits are cleared for the round after next (a
+    // dense pack's slots share one bitmap word: K divides 32)
+    if (dense) {
+      if (lane == 0u) atomicAnd(B.cmask_r + (s0 >> 5), ~(rest << (s0 & 31u)));
+    } else if (my_chunk != kNoChunk) {
+      atomicAnd(B.cmask_r + (my_chunk >> 5), ~(1u << (my_chunk & 31u)));
+    }
+    // One chunk's pending lanes and rows per thread (vertex 32 c + lane).
+    auto load_chunk = [&](u32 j, u32& ccv, u32& cm, uint2& crow) {
+      const u32 chunk = __shfl_sync(0xFFFFFFFFu, my_chunk, static_cast<int>(j));
+      ccv = (chunk << 5) + lane;
+      cm = 0u;
+      crow = make_uint2(0u, 0u);
+      if (ccv < B.U) {
+        cm = dev::ld_cg(B.mask_r + ccv) & B.valid;
+        crow = __ldg(B.crow + ccv);
+      }
+    };
+    uint4* const ring = s_pack[threadIdx.x >> 5];
+    const u32 below = (1u << lane) - 1u;
+    u32 head = 0u, held = 0u;  // ring: entries [head, head + held) wait for a group (warp-uniform)
+    u32 ncv, nm;
+    uint2 nrow;
+    load_chunk(static_cast<u32>(__ffs(rest)) - 1u, ncv, nm, nrow);
+    rest &= rest - 1u;
+    bool loaded = true;  // ncv / nm / nrow hold a chunk not yet compacted
+    for (;;) {
+      while (loaded && held < 32u) {
+        const u32 ccv = ncv, cm = nm;
+        const uint2 crow = nrow;
+        loaded = rest != 0u;
+        if (loaded) {  // the next chunk's loads go out before this one is compacted
+          load_chunk(static_cast<u32>(__ffs(rest)) - 1u, ncv, nm, nrow);
+          rest &= rest - 1u;
+        }
+        const bool act = cm != 0u;
+        if (act) {
+          B.mask_r[ccv] = 0u;
+          if (kCount) {
+            wk.c[0] += 1;
+            wk.c[1] += crow.y;
+            wk.c[2] += __popc(cm);
+          }
+        }
+        const u32 bal = __ballot_sync(0xFFFFFFFFu, act);
+        if (act) ring[(head + held + static_cast<u32>(__popc(bal & below))) & 63u] = make_uint4(ccv, cm, crow.x, crow.y);
+        held += static_cast<u32>(__popc(bal));
+      }
+      if (held == 0u) break;
+      __syncwarp();
+      const u32 take = min(held, 32u);
+      uint4 e = make_uint4(0u, 0u, 0u, 0u);
+      if (lane < take) e = ring[(head + lane) & 63u];
+      __syncwarp();
+      head += take;
+      held -= take;
+      relax_entries(e.x, e.y, e.z, e.w);
     }
   } else {
-    const u32 work = static_cast<u32>(__popc(m)) * deg;
-    u32 incl = work;
-    for (u32 o = 1; o < 32u; o <<= 1) {
-      const u32 y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= o) incl += y;
-    }
-    const u32 excl = incl - work;
-    const u32 total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-    for (u32 base = 0; base < total; base += 32u * kItems) {
-      FlatItem it[kItems];
-      u32 src[kItems];
-#pragma unroll
-      for (u32 u = 0; u < kItems; ++u) {
-        it[u] = flat_decode(base + 32u * u + lane, total, incl, excl, cv, m, rb, deg, p.edge_major != 0u);
-        src[u] = dev::kInfBits;
+    const u32 entry = item * epi + lane;  // epi entries per item (a power of two <= 32)
+    u32 cv = 0u, m = 0u, rb = 0u, deg = 0u;
+    if (lane < epi && entry < count) {
+      const u64 q = dev::ld_cg(B.queue_r + entry);
+      const u32 v = static_cast<u32>(q);
+      cv = static_cast<u32>(q >> 32);
+      if (v < p.g.V && cv < B.U) {
+        m = dev::ld_cg(B.mask_r + cv) & B.valid;
+        rb = __ldg(p.g.csr_off + v);
+        deg = __ldg(p.g.csr_off + v + 1u) - rb;
+        B.mask_r[cv] = 0u;
+      } else {
+        atomicOr(&C.error_bits, static_cast<u32>(BFX_DEVICE_ERROR_INVALID_CONTROLLER_STATE));
+        cv = 0u;
       }
-      step(it, src, true);
+      if (kCount) {
+        wk.c[0] += 1;
+        wk.c[1] += deg;
+        wk.c[2] += __popc(m);
+      }
     }
+    relax_entries(cv, m, rb, deg);
   }
 #pragma unroll
   for (u32 u = 0; u < kItems; ++u) {

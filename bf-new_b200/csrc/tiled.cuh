@@ -366,10 +366,10 @@ __device__ void tile_visit(const LaunchParams& p, const FrontierView& B, u32 uni
 
 // Work of round r in two prefixes: block items (one tile visit per unit of a
 // frontier batch in a dense near round, for batches mapped to tile visits)
-// and warp items (everything else, as the chunked layout counts them: one
-// queued chunk per sparse near item, every chunk slot of a dense round of a
-// batch mapped to chunks, 32 far entries per split item, Jacobi / dense warp
-// items).
+// and warp items (everything else, as the chunked layout counts them: a
+// pack of queued chunks per sparse near item, a pack of chunk slots of a
+// dense round of a batch mapped to chunks, 256 far entries per split item,
+// Jacobi / dense warp items).
 __device__ __forceinline__ bool visits_tiles(const LaunchParams& p, u32 b) {
   return p.mappings == nullptr || p.mappings[b] == BFX_MAPPING_TILE_VISITS;
 }
@@ -389,12 +389,14 @@ __device__ u32 round_work_tiled(const LaunchParams& p, u32 r, u32* prefix_block,
       const u32 n = min(dev::ld_cg(&C.count[ridx]), B.U);
       // dense rounds of a batch mapped to chunks: every chunk slot, in index
       // order, as the chunked layout runs them
-      if (n != 0u) return chunk_dense(n, B.U, 5u) ? (visits_tiles(p, b) ? 0u : chunk_count(B.U, 5u)) : n;
+      if (n != 0u) {
+        return chunk_dense(n, B.U, 5u) && visits_tiles(p, b) ? 0u : (chunk_slots(n, B.U) | kPackable);
+      }
       const u32 f = min(dev::ld_cg(&C.fcount[dev::ld_cg(&C.gen[r & 1u]) % 3u]), B.U);
-      return (f + 31u) >> 5;
+      return (f + kSplitPerItem - 1u) / kSplitPerItem;
     }
     return batch_exec(p, b, ridx) != 0u ? (((B.U << B.shift) + 31u) >> 5) : 0u;
-  });
+  }, p.cpack);
   return prefix_block[p.nb] + prefix_warp[p.nb];
 }
 

@@ -289,7 +289,11 @@ int bfx_resident_graph_set_weights(bfx_resident_graph *graph, const float *weigh
  * each batch shape's dense rounds are mapped to tile visits or chunk-slot
  * warp items (timed alone, visits where 1.1x faster, cached per shape), the
  * per-batch mix kept only if the whole set runs faster (bfx_get_frontier_mapping
- * reports the outcome).  Leaves the workspace prepared with all `count`
+ * reports the outcome); last, 2, 4 and 8 chunk slots per warp item are timed
+ * on the whole set and the fastest kept (bfx_get_chunk_pack reports it).  The
+ * step, layout and pack are cached per set class (graph, magnitudes of the
+ * batch counts per lane width and of the union size) and reused for a later
+ * set of the class.  Leaves the workspace prepared with all `count`
  * batches and their engines, steps and mappings, so bfx_execute with
  * options->engine == BFX_ENGINE_AUTO relaxes each batch with its own engine
  * in one launch.  engines_out[count]; deltas_out[count] (may be NULL) =
@@ -375,6 +379,14 @@ int bfx_set_flat_order(bfx_workspace *ws, uint32_t edge_major);
  * (vertex, lane) pair per thread walking the vertex's out-edges (no per-edge
  * decode; idle threads where degrees differ).  Host-poll modes use 0. */
 int bfx_set_chunk_pairs(bfx_workspace *ws, uint32_t mode);
+/* Chunked layout (and the tiled layout's warp items): chunk slots per warp
+ * item -- 1, 2, 4 (default) or 8 queue words of a sparse round, or as many
+ * consecutive chunk slots of a dense round.  The vertices with pending lanes
+ * of the item's chunks are compacted into work lists of up to 32 vertices,
+ * so a warp step carries more lane-edge relaxations when few vertices of
+ * each chunk are pending. */
+int bfx_set_chunk_pack(bfx_workspace *ws, uint32_t pack);
+int bfx_get_chunk_pack(bfx_workspace *ws, uint32_t *pack);
 /* {mean edge weight, edge count} of the workspace's resident graph. */
 int bfx_workspace_graph_stats(bfx_workspace *ws, double out[2]);
 

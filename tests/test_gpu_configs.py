@@ -37,13 +37,15 @@ THREADS = max(1, min(32, os.cpu_count() or 1))
 LAYOUTS = {"chunked": bfx.FRONTIER_CHUNKED, "tiled": bfx.FRONTIER_TILED}
 
 
-def tuned_launch(resident, wl, layout="chunked"):
+def tuned_launch(resident, wl, layout="chunked", pack=None):
     """Plan, autotune (engines and near/far steps per batch) and run the set
     in one launch, as the benchmark does."""
     plan = bfx.make_overlapping_batch_plan(wl.layout, wl.queries, wl.policy)
     descs = plan.descriptions()
     ws = bfx.Workspace(resident)
     ws.set_frontier_layout(LAYOUTS[layout])
+    if pack is not None:
+        ws.set_chunk_pack(pack)
     engines, _ = ws.autotune(descs)
     ws.execute(bfx.GpuRunOptions(engine=bfx.ENGINE_AUTO))
     statuses = ws.fetch_statuses()
@@ -95,10 +97,10 @@ def c2_graph(gpu):
     resident.close()
 
 
-@pytest.mark.parametrize("layout", ["chunked", "tiled"])
-def test_c2_every_lane_bit_exact(c2_graph, layout):
+@pytest.mark.parametrize("layout,pack", [("chunked", None), ("tiled", None), ("chunked", 1), ("chunked", 8)])
+def test_c2_every_lane_bit_exact(c2_graph, layout, pack):
     wl, resident, orc = c2_graph
-    ws, descs, engines, statuses = tuned_launch(resident, wl, layout)
+    ws, descs, engines, statuses = tuned_launch(resident, wl, layout, pack)
     assert_statuses(statuses)
     picks = [(b, l) for b, d in enumerate(descs) for l in valid_lanes(d)]
     assert len(picks) == len(wl.queries) == 256

@@ -297,6 +297,10 @@ def test_flat_frontier_layout_bit_exact(gpu, c1, step, control, layout_kind, reg
     walked 32 per step) gives the oracle's labels on full-graph W=8, regional
     multi-batch W in {1, 8, 16, 32}, plain and near/far, with the counting
     (instr 1) and the production (instr 0) kernel instantiations."""
+    run_layout_case(c1, layout_kind, step, control, regs, items, amin, order, pairs, instr)
+
+
+def run_layout_case(c1, layout_kind, step, control, regs, items, amin, order, pairs, instr, pack=1):
     layout = c1.layout
     d = bfx.make_description(layout, c1.queries, 8)
     layout2, grid = workloads.build_graph("c2", scale_tiles=(32, 32))
@@ -314,6 +318,7 @@ def test_flat_frontier_layout_bit_exact(gpu, c1, step, control, layout_kind, reg
         ws.set_relax_atomic(amin)
         ws.set_flat_order(order)
         ws.set_chunk_pairs(pairs)
+        ws.set_chunk_pack(pack)
         ws.prepare(descs)
         if step is not None:
             ws.set_batch_deltas([step] * len(descs))
@@ -323,6 +328,28 @@ def test_flat_frontier_layout_bit_exact(gpu, c1, step, control, layout_kind, reg
         check_batches(lay, descs, lanes, st, labels, Oracle.from_layout(lay))
         ws.close()
         res.close()
+
+
+@pytest.mark.parametrize("pack", [2, 4, 8])
+@pytest.mark.parametrize("regs,items,order,pairs,instr", [(80, 2, 0, 0, 0), (80, 2, 0, 0, 1), (80, 4, 0, 0, 0),
+                                                          (80, 2, 1, 0, 1), (64, 2, 0, 1, 1), (64, 2, 0, 0, 0)])
+@pytest.mark.parametrize("step", [None, 3.0])
+@pytest.mark.parametrize("control", [bfx.CONTROL_PERSISTENT, bfx.CONTROL_PER_ROUND], ids=["persistent", "per_round"])
+def test_chunk_pack_bit_exact(gpu, c1, step, control, regs, items, order, pairs, instr, pack):
+    """Chunked layout with 2, 4 or 8 chunk slots per warp item (the pending
+    vertices of several chunks compacted into one work list): the oracle's
+    labels on the same full-graph and regional multi-batch sets."""
+    run_layout_case(c1, bfx.FRONTIER_CHUNKED, step, control, regs, items, 0, order, pairs, instr, pack)
+
+
+def test_chunk_pack_rejects_other_values(gpu, c1):
+    res = bfx.ResidentDeviceGraph.upload_once(c1.layout)
+    ws = bfx.Workspace(res)
+    for bad in (0, 3, 16):
+        with pytest.raises(ValueError):
+            ws.set_chunk_pack(bad)
+    ws.close()
+    res.close()
 
 
 def test_plain_query_after_autotune_ignores_batch_settings(gpu):

@@ -138,15 +138,17 @@ def test_host_poll_modes_fall_back_to_chunked(gpu, c1):
     check_batches(c1.layout, [d], [c1.queries], st, labels, Oracle.from_layout(c1.layout))
 
 
+@pytest.mark.parametrize("pack", [1, 4])
 @pytest.mark.parametrize("step", [None, 3.0])
-def test_per_batch_mappings_bit_exact(gpu, c2_regional, step):
+def test_per_batch_mappings_bit_exact(gpu, c2_regional, step, pack):
     """One tiled launch with dense rounds mapped per batch: alternating tile
-    visits and chunk-slot warp items."""
+    visits and chunk-slot warp items (1 or 4 chunk slots per warp item)."""
     layout, descs, lanes = c2_regional
     res = bfx.ResidentDeviceGraph.upload_once(layout)
     ws = bfx.Workspace(res)
     ws.set_frontier_layout(bfx.FRONTIER_TILED)
     ws.set_tile_stage_min(0)
+    ws.set_chunk_pack(pack)
     ws.prepare(descs)
     if step is not None:
         ws.set_batch_deltas([step] * len(descs))

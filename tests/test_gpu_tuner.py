@@ -1,7 +1,7 @@
 """The autotuner's set-class cache: a second query set of the same workload
 class (same graph, same magnitudes of batch counts per lane width and of the
-union size) reuses the first set's near/far step and layout instead of
-searching again, and its launch stays bit-exact."""
+union size) reuses the first set's near/far step, layout and chunk pack
+instead of searching again, and its launch stays bit-exact."""
 import pytest
 
 import bfx
@@ -30,9 +30,13 @@ def test_second_set_of_a_class_reuses_the_step_and_stays_exact(gpu):
     bfx.load().bfx_autotune_reset()
     e1, _ = ws.autotune(d1)
     steps1 = {x for e, x in zip(e1, ws.tuned_deltas) if e == bfx.ENGINE_FRONTIER_PUSH}
+    pack1 = ws.chunk_pack()
+    assert pack1 in (2, 4, 8)
+    ws.set_chunk_pack(1)  # the cached class pack replaces it
     e2, _ = ws.autotune(d2)
     steps2 = {x for e, x in zip(e2, ws.tuned_deltas) if e == bfx.ENGINE_FRONTIER_PUSH}
     assert len(steps1) == 1 and steps2 <= steps1  # the cached class step
+    assert ws.chunk_pack() == pack1
     ws.execute(bfx.GpuRunOptions(engine=bfx.ENGINE_AUTO))
     st = ws.fetch_statuses()
     labels = [ws.download_labels(b, d.lane_width) for b, d in enumerate(d2)]
