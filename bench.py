@@ -71,31 +71,35 @@ def traffic_estimate(workload: str, relaxations: int, kernel_ms: float, step: st
                      path: Path | None = None):
     """DRAM traffic of one relaxation launch, scaled by relaxations from one
     ncu capture per workload class (profiles/frontier_push_traffic.txt:
-    `workload bytes relaxations step summary` lines; c2 from the c2 capture,
-    c3 and c5 from the c3-shaped capture), and the launch's DRAM rate against
-    the random-sector ceiling (`ceiling bytes_per_s summary`).  The near/far
-    step changes the relaxations per sector, so a capture is scaled only to a
-    launch run at its own step (`step` = the launch's steps, e.g. "1" or
-    "plain"; None accepts any).  Returns (bytes or None, source text or None,
+    `workload bytes relaxations step summary` lines, one per captured step;
+    c2 from the c2 captures, c3 and c5 from the c3-shaped ones), and the
+    launch's DRAM rate against the random-sector ceiling (`ceiling
+    bytes_per_s summary`).  The near/far step changes the relaxations per
+    sector, so only a capture at the launch's own step is scaled (`step` =
+    the launch's steps, e.g. "1" or "plain"; None takes the first line).  Returns (bytes or None, source text or None,
     ceiling dict or None)."""
     path = path or REPO / "profiles" / "frontier_push_traffic.txt"
     if not path.exists():
         return None, None, None
-    captured, ceiling = {}, None
+    captured, ceiling = {}, None  # workload -> {step: (bytes, relaxations, summary)}
     for line in path.read_text().splitlines():
         parts = line.split()
         if line.startswith("#"):
             continue
         if len(parts) == 5:
-            captured[parts[0]] = (int(parts[1]), int(parts[2]), parts[3], parts[4])
+            captured.setdefault(parts[0], {})[parts[3]] = (int(parts[1]), int(parts[2]), parts[4])
         elif len(parts) == 3 and parts[0] == "ceiling":
             ceiling = (int(parts[1]), parts[2])
     key = "c2" if workload == "c2" else "c3small"
     if key not in captured or not relaxations:
         return None, None, None
-    b, rl, cstep, src = captured[key]
-    if step is not None and step != cstep:
-        return None, f"{src}: captured at step {cstep}, launch ran at step {step}; not scaled", None
+    by_step = captured[key]
+    if step is not None and step not in by_step:
+        src = next(iter(by_step.values()))[2]
+        return None, (f"{src}: captured at step {', '.join(sorted(by_step))}, launch ran at step {step}; "
+                      "not scaled"), None
+    cstep = step if step is not None else next(iter(by_step))
+    b, rl, src = by_step[cstep]
     traffic = int(b / rl * relaxations)
     source = f"{src} (step {cstep}): {b / rl:.1f} bytes per relaxation x {relaxations:,} relaxations"
     random_ceiling = None

@@ -20,21 +20,22 @@ def test_traffic_estimate_scales_the_committed_captures():
     for a launch at the capture's near/far step; the DRAM rate is reported
     against the random-sector ceiling."""
     bench = load_bench()
-    rows = {}
+    rows = []
     for line in (REPO / "profiles" / "frontier_push_traffic.txt").read_text().splitlines():
         parts = line.split()
         if parts and not line.startswith("#") and len(parts) == 5:
-            rows[parts[0]] = (int(parts[1]), int(parts[2]), parts[3])
-    for workload, key in (("c2", "c2"), ("c3", "c3small"), ("c5", "c3small")):
-        b, rl, step = rows[key]
-        t, src, ceil = bench.traffic_estimate(workload, 2 * rl, 10.0, step)
-        assert t == pytest.approx(2 * b, rel=1e-9)
-        assert src.endswith(f"{2 * rl:,} relaxations")
-        assert ceil["dram_gbs"] == pytest.approx(2 * b / 0.010 / 1e9)
-        assert 0 < ceil["frac"] and ceil["peak_gbs"] > 0
-        # another step: not scaled, and the source says why
-        t, src, ceil = bench.traffic_estimate(workload, 2 * rl, 10.0, "another")
-        assert t is None and ceil is None and "not scaled" in src
+            rows.append((parts[0], int(parts[1]), int(parts[2]), parts[3]))
+    assert {r[0] for r in rows} == {"c2", "c3small"}
+    for name, b, rl, step in rows:
+        for workload in (("c2",) if name == "c2" else ("c3", "c5")):
+            t, src, ceil = bench.traffic_estimate(workload, 2 * rl, 10.0, step)
+            assert t == pytest.approx(2 * b, rel=1e-9)
+            assert f"(step {step})" in src and src.endswith(f"{2 * rl:,} relaxations")
+            assert ceil["dram_gbs"] == pytest.approx(2 * b / 0.010 / 1e9)
+            assert 0 < ceil["frac"] and ceil["peak_gbs"] > 0
+            # a step without a capture: not scaled, and the source says why
+            t, src, ceil = bench.traffic_estimate(workload, 2 * rl, 10.0, "another")
+            assert t is None and ceil is None and "not scaled" in src
     assert bench.traffic_estimate("c2", 0, 10.0) == (None, None, None)
 
 
