@@ -21,9 +21,10 @@
 //   * the frontier is a queue of 32-vertex chunks by default (frontier.cuh:
 //     chunk bitmaps per round slot, pending lanes set with non-returning ORs,
 //     near and far claims staged per warp and (round, batch)); a warp item
-//     is one chunk whose (lane, edge) work is walked as a flat list, two
-//     items per thread in flight, and dense rounds take the chunk slots in
-//     index order; the vertex-queue flat layout and the sub-warp group
+//     is a pack of up to 8 chunks whose pending vertices are compacted into
+//     work lists of up to 32 vertices, each walked as a flat (lane, edge)
+//     list, two items per thread in flight, and dense rounds take the chunk
+//     slots in index order; the vertex-queue flat layout and the sub-warp group
 //     layout remain options; improvements use a non-returning 64-bit min
 //     after a coherent pre-read;
 //   * persistent mode runs all rounds of all batches in one cooperative
