@@ -456,7 +456,8 @@ int bfx_run_query(bfx_workspace *ws, uint32_t source_count, const uint32_t *sour
  *  - every GPU that loads libbfx.so holds the 32 MiB array until exit;
  *  - the first call on a device resolves the array's device address once
  *    (cudaGetSymbolAddress) and keeps it for the process, so resetting the
- *    device (cudaDeviceReset) between calls is not supported;
+ *    device (cudaDeviceReset) between calls is not supported, and that first
+ *    call should be made before any stream capture begins;
  *  - all calls on a device share the array and leave their data in it (each
  *    call re-initialises what it reads); calls that overlap on the GPU --
  *    from several host threads at once -- race and must be serialised by the
