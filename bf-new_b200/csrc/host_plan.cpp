@@ -14,8 +14,10 @@
 // the region estimates follow SelectedRegionIndex (src/selected_region_index.cpp).
 //
 // Our implementation evaluates the expensive union-edge tie-breakers only for
-// candidates that tie on the first three keys, and keeps the union as a tile
-// bitmap, which yields the same plan in far less time on 256+ query sets.
+// candidates that tie on the first three keys, keeps the union as a tile
+// bitmap and, with a positive minimum Jaccard, meets only the candidates that
+// share a tile with the union (a tile -> queries index), which yields the
+// same plan in far less time on 256+ query sets.
 //
 // Descriptions follow prepare_batch_device_description
 // (src/batch_layout.cpp:1056-1296) with device-materialized run masks: lane
@@ -196,6 +198,35 @@ std::unique_ptr<HostPlan> build_plan(const bfx_device_graph_layout32& g, const s
   u32 assigned_count = 0;
   std::size_t anchor_cursor = 0;
 
+  // With a positive minimum Jaccard only a query that shares a tile with the
+  // batch's union can join it, so the candidates of a growing batch are
+  // found through a tile -> queries index, and each one's overlap with the
+  // union is counted as tiles join the union (shared[c] = |tiles(c) & U|)
+  // instead of rescanning every query's tiles for every lane.  The choice
+  // does not depend on the order candidates are met in (the last
+  // tie-breaker is the unique query id), so the plan is the same.
+  const bool indexed = policy.minimum_jaccard_numerator > 0;
+  std::vector<u32> tile_q_off, tile_q, shared, touched;
+  if (indexed) {
+    tile_q_off.assign(T + 1U, 0U);
+    for (u32 c = 0; c < nq; ++c) {
+      for (u32 t : F[c].selected_tiles) ++tile_q_off[t + 1U];
+    }
+    for (u32 t = 0; t < T; ++t) tile_q_off[t + 1U] += tile_q_off[t];
+    tile_q.resize(tile_q_off[T]);
+    std::vector<u32> fill(tile_q_off.begin(), tile_q_off.end() - 1);
+    for (u32 c = 0; c < nq; ++c) {
+      for (u32 t : F[c].selected_tiles) tile_q[fill[t]++] = c;
+    }
+    shared.assign(nq, 0U);
+  }
+  const auto union_gains = [&](u32 t) {  // tile t joins the union
+    for (u32 k = tile_q_off[t]; k < tile_q_off[t + 1U]; ++k) {
+      const u32 c = tile_q[k];
+      if (shared[c]++ == 0U) touched.push_back(c);
+    }
+  };
+
   struct Cand {
     u32 idx;
     Fraction jac;
@@ -216,15 +247,26 @@ std::unique_ptr<HostPlan> build_plan(const bfx_device_graph_layout32& g, const s
     std::vector<u32> U = anchor.selected_tiles;
     std::vector<u32> US = anchor.source_tiles, UT = anchor.target_tiles;
     for (u32 t : U) in_union[t] = 1U;
+    if (indexed) {
+      for (u32 c : touched) shared[c] = 0U;
+      touched.clear();
+      for (u32 t : U) union_gains(t);
+    }
     u64 lane_tiles = anchor.selected_tiles.size();
 
     while (b.feature_by_lane.size() < W) {
       std::vector<Cand> top;
-      for (u32 c = 0; c < nq; ++c) {
+      const u32 ncand = indexed ? static_cast<u32>(touched.size()) : nq;
+      for (u32 ci = 0; ci < ncand; ++ci) {
+        const u32 c = indexed ? touched[ci] : ci;
         if (assigned[c]) continue;
         const Feature& f = F[c];
         u64 inter = 0;
-        for (u32 t : f.selected_tiles) inter += in_union[t];
+        if (indexed) {
+          inter = shared[c];
+        } else {
+          for (u32 t : f.selected_tiles) inter += in_union[t];
+        }
         const u64 usize = U.size() + f.selected_tiles.size() - inter;
         Cand cd;
         cd.idx = c;
@@ -277,7 +319,10 @@ std::unique_ptr<HostPlan> build_plan(const bfx_device_graph_layout32& g, const s
       ++assigned_count;
       lane_tiles += s.selected_tiles.size();
       U = set_union(U, s.selected_tiles);
-      for (u32 t : s.selected_tiles) in_union[t] = 1U;
+      for (u32 t : s.selected_tiles) {
+        if (indexed && !in_union[t]) union_gains(t);
+        in_union[t] = 1U;
+      }
       US = set_union(US, s.source_tiles);
       UT = set_union(UT, s.target_tiles);
     }

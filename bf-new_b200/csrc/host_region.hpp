@@ -41,8 +41,11 @@ struct RegionIndex {
 
 // Built per source tile in parallel: a tile's vertices are one contiguous
 // span (the layout orders vertices by tile), and their CSR runs name the
-// destination tiles; the (destination tile, edge count) pairs of a tile are
-// merged in a small sorted list.
+// destination tiles.  A tile's runs reach few distinct tiles (its own and
+// its neighbours), so their edge counts are accumulated by a linear search
+// of the short list of tiles seen so far and the list is sorted once; a
+// tile that reaches more than kLinear tiles falls back to sorting all its
+// (destination tile, edge count) pairs.
 inline RegionIndex make_region_index(const bfx_device_graph_layout32& g) {
   RegionIndex r;
   r.T = g.tile_count;
@@ -51,9 +54,40 @@ inline RegionIndex make_region_index(const bfx_device_graph_layout32& g) {
   std::vector<std::uint32_t> first(r.T + 1, 0U);
   for (std::uint32_t t = 0; t < r.T; ++t) first[t + 1] = first[t] + static_cast<std::uint32_t>(r.vertex_counts[t]);
   std::vector<std::vector<std::pair<std::uint32_t, std::uint64_t>>> per(r.T);
+  constexpr std::size_t kLinear = 64;
   parallel_for(r.T, 0, [&](std::uint64_t tb, std::uint64_t te) {
     std::vector<std::pair<std::uint32_t, std::uint64_t>> lst;
     for (std::uint64_t t = tb; t < te; ++t) {
+      auto& merged = per[t];
+      bool wide = false;
+      std::size_t hint = 0;
+      for (std::uint32_t v = first[t]; v < first[t + 1] && !wide; ++v) {
+        for (std::uint32_t run = g.csr_row_run_offsets[v]; run < g.csr_row_run_offsets[v + 1]; ++run) {
+          const std::uint32_t dt = g.csr_run_destination_tiles[run];
+          const std::uint64_t n = g.csr_run_edge_offsets[run + 1] - g.csr_run_edge_offsets[run];
+          if (hint < merged.size() && merged[hint].first == dt) {
+            merged[hint].second += n;
+            continue;
+          }
+          std::size_t i = 0;
+          while (i < merged.size() && merged[i].first != dt) ++i;
+          if (i == merged.size()) {
+            if (merged.size() == kLinear) {
+              wide = true;
+              break;
+            }
+            merged.emplace_back(dt, 0U);
+          }
+          merged[i].second += n;
+          hint = i;
+        }
+      }
+      if (!wide) {
+        std::sort(merged.begin(), merged.end());
+        continue;
+      }
+      // many destination tiles: all pairs of the tile, sorted and merged
+      merged.clear();
       lst.clear();
       for (std::uint32_t v = first[t]; v < first[t + 1]; ++v) {
         for (std::uint32_t run = g.csr_row_run_offsets[v]; run < g.csr_row_run_offsets[v + 1]; ++run) {
@@ -62,7 +96,6 @@ inline RegionIndex make_region_index(const bfx_device_graph_layout32& g) {
         }
       }
       std::sort(lst.begin(), lst.end());
-      auto& merged = per[t];
       for (const auto& q : lst) {
         if (!merged.empty() && merged.back().first == q.first) {
           merged.back().second += q.second;
