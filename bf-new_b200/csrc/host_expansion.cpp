@@ -324,6 +324,8 @@ std::unique_ptr<ExpansionResult> run(const bfx_device_graph_layout32& g, const b
                                      const bfx_route_query* queries, const bfx_expansion_options& o, Runner runner,
                                      void* user) {
   const Geometry geo = make_geometry(g, tg);
+  require(g.csr_row_run_offsets && g.csr_run_edge_offsets && g.csr_run_destination_tiles,
+          "planner needs owner tiles and CSR runs");
   const RegionIndex region = make_region_index(g);
   Counter count(region);
   std::vector<u32> full(geo.T);
@@ -369,10 +371,9 @@ std::unique_ptr<ExpansionResult> run(const bfx_device_graph_layout32& g, const b
       r.selected_tile_count = static_cast<u32>(s.tiles.size());
       r.selected_tiles = s.tiles.data();
     }
-    bfx_plan* plan = nullptr;
-    int rc = bfx_plan_build(&g, tg.tile_vertex_offsets, static_cast<u32>(rq.size()), rq.data(), &o.planner_policy,
-                            &plan);
-    if (rc != BFX_OK) throw Error(rc, bfx_last_error());
+    // every pass is planned against the loop's one region index
+    bfx_plan* plan = plan_build_with_region(g, tg.tile_vertex_offsets, static_cast<u32>(rq.size()), rq.data(),
+                                            o.planner_policy, region);
     std::unique_ptr<bfx_plan, int (*)(bfx_plan*)> plan_owner(plan, bfx_plan_destroy);
     u32 nb = 0;
     bfx_plan_batch_count(plan, &nb);

@@ -123,7 +123,8 @@ struct HostPlan {
 namespace {
 
 std::unique_ptr<HostPlan> build_plan(const bfx_device_graph_layout32& g, const std::vector<u32>& tile_offsets,
-                                     u32 nq, const bfx_route_query* queries, const bfx_planner_policy& policy) {
+                                     u32 nq, const bfx_route_query* queries, const bfx_planner_policy& policy,
+                                     const RegionIndex* shared_region = nullptr) {
   const u32 W = policy.lane_width;
   require(W == 1 || W == 8 || W == 16 || W == 32, "batch planner policy is invalid");
   require(policy.minimum_jaccard_denominator != 0 &&
@@ -134,7 +135,9 @@ std::unique_ptr<HostPlan> build_plan(const bfx_device_graph_layout32& g, const s
           "batch planner policy is invalid");
   require(nq > 0, "batch planning requires at least one query");
   const u32 T = g.tile_count;
-  const RegionIndex region = make_region_index(g);
+  RegionIndex own;
+  if (shared_region == nullptr) own = make_region_index(g);
+  const RegionIndex& region = shared_region != nullptr ? *shared_region : own;
 
   auto plan = std::make_unique<HostPlan>();
   auto& F = plan->features;
@@ -410,6 +413,19 @@ const HostPlan& plan_ref(const bfx_plan* p) {
 }
 
 }  // namespace
+}  // namespace bfx
+
+namespace bfx {
+
+bfx_plan* plan_build_with_region(const bfx_device_graph_layout32& g, const std::uint32_t* tile_vertex_offsets,
+                                 std::uint32_t query_count, const bfx_route_query* queries,
+                                 const bfx_planner_policy& policy, const RegionIndex& region) {
+  require(tile_vertex_offsets && queries, "null argument");
+  require(region.T == g.tile_count, "region index does not match the graph");
+  std::vector<std::uint32_t> offsets(tile_vertex_offsets, tile_vertex_offsets + g.tile_count + 1U);
+  return reinterpret_cast<bfx_plan*>(build_plan(g, offsets, query_count, queries, policy, &region).release());
+}
+
 }  // namespace bfx
 
 extern "C" {

@@ -6,6 +6,7 @@
 #pragma once
 
 #include "bfx.h"
+#include "bfx_host.h"
 #include "bfx_internal.hpp"
 
 #include <algorithm>
@@ -121,5 +122,12 @@ inline RegionIndex make_region_index(const bfx_device_graph_layout32& g) {
   }
   return r;
 }
+
+// bfx_plan_build with a region index the caller already holds for the same
+// graph (the expansion loop plans every pass against one index).  Throws on
+// invalid input like bfx_plan_build reports it.
+bfx_plan* plan_build_with_region(const bfx_device_graph_layout32& g, const std::uint32_t* tile_vertex_offsets,
+                                 std::uint32_t query_count, const bfx_route_query* queries,
+                                 const bfx_planner_policy& policy, const RegionIndex& region);
 
 }  // namespace bfx
